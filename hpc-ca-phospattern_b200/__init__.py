@@ -1,0 +1,153 @@
+"""B200 calcium_sparks time step -- Python host bindings of libcsparks_cuda.so.
+
+The product is the C ABI of include/csparks.h (libcsparks_cuda.so, built in-tree by
+build.py) and the C command-line driver bin/calcium_sparks.  This module is the thin
+ctypes layer the tests and bench.py drive it through.  There is no CPU path: loading
+fails loudly when the CUDA library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcsparks_cuda.so")
+_lib = None
+
+
+class CspError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run build.py (or __graft_entry__.build())")
+        lib = C.CDLL(LIB_PATH)
+        abi.declare(lib)
+        _lib = lib
+    return _lib
+
+
+def _status(lib, h):
+    buf = C.create_string_buffer(512)
+    lib.csp_status(h, buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+class Simulation:
+    """One handle of libcsparks_cuda.so over n realisations.
+
+    specs: list of model descriptions (synth.py format); options: list of dicts for
+    abi.make_options (one per realisation, or one shared).
+    """
+
+    def __init__(self, specs, options):
+        self.lib = load()
+        if isinstance(specs, dict):
+            specs = [specs]
+        if isinstance(options, dict):
+            options = [options] * len(specs)
+        n = len(specs)
+        self._keep = []
+        models = (abi.csp_model * n)()
+        opts = (abi.csp_options * n)()
+        for i, (s, o) in enumerate(zip(specs, options)):
+            m, k1 = abi.make_model(s)
+            op, k2 = abi.make_options(**o)
+            models[i] = m
+            opts[i] = op
+            self._keep += [k1, k2, m, op]
+        self._keep += [models, opts]
+        h = C.c_void_p()
+        rc = self.lib.csp_create(models, opts, n, C.byref(h))
+        if rc != 0:
+            raise CspError(rc, _status(self.lib, None))
+        self.h = h
+        self.n = n
+        self.specs = specs
+
+    def _check(self, rc):
+        if rc != 0:
+            raise CspError(rc, _status(self.lib, self.h))
+
+    def info(self, r=0):
+        inf = abi.csp_info()
+        self._check(self.lib.csp_get_info(self.h, r, C.byref(inf)))
+        return inf
+
+    def shape(self, r=0):
+        inf = self.info(r)
+        return (inf.num_species, inf.n[0], inf.n[1], inf.n[2])
+
+    def state(self, r=0):
+        u = np.empty(self.shape(r), dtype=np.float64)
+        self._check(self.lib.csp_download_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
+        return u
+
+    def set_state(self, u, r=0):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.shape != self.shape(r):
+            raise ValueError(f"state shape {u.shape} != {self.shape(r)}")
+        self._check(self.lib.csp_upload_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def advance(self, nsteps):
+        flags = np.zeros(self.n, dtype=np.int32)
+        self._check(self.lib.csp_advance(self.h, int(nsteps), flags.ctypes.data_as(C.POINTER(C.c_int32))))
+        return flags
+
+    def last_ms(self):
+        ms = C.c_float()
+        self._check(self.lib.csp_last_advance_ms(self.h, C.byref(ms)))
+        return ms.value
+
+    def channels(self, boundary, r=0):
+        n = self.info(r).num_channels[boundary]
+        st = np.zeros(n, dtype=np.int32)
+        self._check(self.lib.csp_get_channel_states(self.h, r, boundary, st.ctypes.data_as(C.POINTER(C.c_int32))))
+        return st
+
+    def set_channels(self, boundary, states, r=0):
+        st = np.ascontiguousarray(states, dtype=np.int32)
+        self._check(self.lib.csp_set_channel_states(self.h, r, boundary, st.ctypes.data_as(C.POINTER(C.c_int32))))
+
+    def outputs(self, r=0):
+        inf = self.info(r)
+        nd = len(self.specs[r]["domains"])
+        ns = inf.num_species
+        mn = np.zeros(nd * ns)
+        mx = np.zeros(nd * ns)
+        tot = np.zeros(nd * ns)
+        nch = sum(inf.num_channels[b] for b in range(abi.MAX_BOUNDARIES))
+        op = np.zeros(max(nch, 1), dtype=np.int32)
+        P = C.POINTER
+        self._check(self.lib.csp_reduce_outputs(self.h, r, mn.ctypes.data_as(P(C.c_double)),
+                                                mx.ctypes.data_as(P(C.c_double)),
+                                                tot.ctypes.data_as(P(C.c_double)),
+                                                op.ctypes.data_as(P(C.c_int32))))
+        return mn.reshape(nd, ns), mx.reshape(nd, ns), tot.reshape(nd, ns), op[:nch]
+
+    def set_kernel(self, which):
+        self._check(self.lib.csp_set_kernel(self.h, int(which)))
+
+    def stream(self):
+        s = C.c_void_p()
+        self._check(self.lib.csp_get_stream(self.h, C.byref(s)))
+        return s.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.csp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

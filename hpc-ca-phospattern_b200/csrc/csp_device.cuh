@@ -1,0 +1,228 @@
+// csp_device.cuh -- device-side data layout and per-voxel arithmetic shared by the
+// voxel kernels (direct and TMA-staged) and the boundary kernel.
+//
+// HBM layout of one realisation: for every species two FP32 buffers (the reference's
+// u1 / du pair, species.h:52-53, become a double buffer: a step reads the current
+// buffer and writes the other one) and one uint8 domain-id field.  Every field is
+// [nx][P] with P = ny*nz rounded up to a multiple of 128 elements, so each x-plane
+// starts on a 512-byte boundary (float) / 128-byte boundary (uint8) and can be moved by
+// 16-byte aligned bulk copies.  Within a plane the index is p = y*nz + z (z fastest,
+// species.c:1513).
+#pragma once
+#include <cstdint>
+
+#include "../../include/csparks.h"
+
+namespace csp {
+
+constexpr int ND = CSP_MAX_DOMAINS;
+constexpr int NS = CSP_MAX_SPECIES;
+constexpr int NB = CSP_MAX_BUFFERS;
+constexpr int PLANE_ALIGN = 128;
+
+enum FluxKind : int { FLUX_NONE = 0, FLUX_RYR = 1, FLUX_P_RYR = 2, FLUX_SERCA = 3 };
+
+// Constant description of one realisation (device resident, read-only in kernels).
+struct RealDesc {
+  int nx, ny, nz, P, plane;          // plane = ny*nz
+  int ns, nd, ndiff, nbuf;
+  int reaction_substep, stochastic_substep;
+  int dirichlet;
+  int substeps[NS];                  // per diffusive index
+  int diff_species[NS];
+  unsigned reaction_flag_mask;       // species flagged after a reaction step (species.c:1695-1699)
+  float dt_r;                        // dt * reaction_substep (species.c:1666)
+  float coef[NS][ND * ND];           // dt*substeps*sigma/h^2 tables (species.c:1545-1560)
+  float kon[NB * ND], koff[NB * ND], tot[NB * ND];   // [bi*nd + di] (species.c:249-253)
+  unsigned char bsp0[NB * ND], bsp1[NB * ND];
+  unsigned char fixed_mask[ND];      // bit s: species s is fixed in domain d
+  signed char dsi_of[NS];            // diffusive index of species s, or -1
+  signed char rtab[ND][NS];          // fast reaction table: buffer index bi with bsp0 = s in domain d, or -1
+  int react_fast;                    // every buffer binds species 0 and bound species are distinct per domain
+  float init[ND][NS];
+  float* u[2][NS];                   // the two buffers of every species
+  const unsigned char* dom;          // [nx][P]
+  long long total_steps;
+  double dt, h, tabort;
+  unsigned long long seed;           // Philox key of the realisation's channel draws
+  int has_channels;
+};
+
+// Mutable per-realisation progress (device).
+struct RealCtl {
+  long long step;                    // steps taken; the running step has time_ind = step+1
+  unsigned cur_mask[2];              // [step&1]: bit s = index of the current buffer of species s
+  int stopped;
+  int open_count[2];                 // open channels after the step, by (step+1)&1
+  double last_closed;                // abort rule bookkeeping
+};
+
+// One boundary pair (species voxels), with the law applied across it.
+struct FluxPair {
+  int r;                  // realisation
+  int species;            // flux species (species index)
+  int dsi;                // diffusive index of the flux species
+  int kind;               // FluxKind
+  int channel;            // global channel index (discrete boundaries) or -1
+  int boundary;           // boundary index within the realisation
+  int inner;              // inner boundary: the "from" voxel loses J
+  int param;              // index into the parameter blocks
+  long long v0, v1;       // padded linear indices x*P + p of from / to voxels
+  int local_channel;      // channel index within its boundary (RNG counter)
+  int pad;
+};
+
+// One voxel receiving flux: entries [begin, end) of the entry list, in pair order.
+struct FluxRow {
+  int r, species;
+  long long v;
+  int begin, end;
+  int apply;              // 0 if the voxel is reset by the fixed-value rules after the step
+  int pad;
+};
+
+struct FluxEntry {
+  int pair;
+  float sign;             // +1 "to" side, -1 "from" side (inner boundaries)
+  int owner;              // this entry writes the channel's new state
+  int pad;
+};
+
+struct FluxParams {
+  double p[10];           // RyR_model::params layout (boundaryfluxes.h:54) / SERCA params
+  double t_close;
+};
+
+// Species updated at step time_ind, and the subset flagged before the reaction runs
+// (diffusion and boundary fluxes flag their species, species.c:1542, 1746).
+__host__ __device__ inline void step_masks(const RealDesc& D, long long time_ind, unsigned& pre,
+                                           unsigned& updated, unsigned& diffusing_dsi) {
+  pre = 0;
+  diffusing_dsi = 0;
+  for (int d = 0; d < NS; d++) {
+    if (d >= D.ndiff) break;
+    if (time_ind % D.substeps[d] == 0) {
+      pre |= 1u << D.diff_species[d];
+      diffusing_dsi |= 1u << d;
+    }
+  }
+  updated = pre;
+  if (D.nbuf > 0 && time_ind % D.reaction_substep == 0) updated |= D.reaction_flag_mask;
+}
+
+// Register-array access with a run-time index, as a chain of selects (no local memory).
+template <int N>
+__device__ __forceinline__ float sel(const float (&a)[N], int i) {
+  float r = a[0];
+#pragma unroll
+  for (int s = 1; s < N; s++)
+    if (i == s) r = a[s];
+  return r;
+}
+
+template <int N>
+__device__ __forceinline__ void put(float (&a)[N], int i, float v) {
+#pragma unroll
+  for (int s = 0; s < N; s++)
+    if (i == s) a[s] = v;
+}
+
+template <int N>
+__device__ __forceinline__ void addto(float (&a)[N], int i, float v) {
+#pragma unroll
+  for (int s = 0; s < N; s++)
+    if (i == s) a[s] += v;
+}
+
+// Masked 7-point update of one species at one voxel (species.c:1572-1611 and the
+// face terms of species.c:1282-1498): out = u + sum_n c[d][d_n]*(u_n - u), with the
+// neighbours outside the box dropped (no flux).  Neighbour order: z-, z+, y-, y+, x-, x+.
+// valid bit k = neighbour k inside the box.
+__device__ __forceinline__ float stencil7(const float* __restrict__ c, float u, const float (&un)[6],
+                                          const unsigned char (&dn)[6], unsigned valid) {
+  float acc = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    float ck = (valid >> k & 1u) ? c[dn[k]] : 0.f;
+    float dk = (valid >> k & 1u) ? (un[k] - u) : 0.f;
+    acc = fmaf(ck, dk, acc);
+  }
+  return u + acc;
+}
+
+// Buffer reactions of one voxel (reaction_SIMD, kernel_generic.cpp:397-509): for each
+// buffer bi of the voxel's domain, J = k_on*(tot-b0)*b1 - k_off*b0 with the values at
+// step start; a species already updated this step accumulates, otherwise it is assigned
+// from its step-start value.
+template <int N>
+__device__ __forceinline__ void react(const RealDesc& D, int d, const float (&val)[N], float (&out)[N],
+                                      unsigned pre) {
+  for (int bi = 0; bi < NB; bi++) {
+    if (bi >= D.nbuf) break;
+    const int t = bi * D.nd + d;
+    const int s0 = D.bsp0[t], s1 = D.bsp1[t];
+    const float b0 = sel(val, s0), b1 = sel(val, s1);
+    const float J = D.kon[t] * (D.tot[t] - b0) * b1 - D.koff[t] * b0;
+    const float dJ = D.dt_r * J;
+    if (pre >> s0 & 1u) addto(out, s0, dJ); else put(out, s0, b0 + dJ);
+    if (pre >> s1 & 1u) addto(out, s1, -dJ); else put(out, s1, b1 - dJ);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) for the channel draws.
+__host__ __device__ inline void philox4x32(const unsigned (&ctr)[4], unsigned k0, unsigned k1, unsigned (&out)[4]) {
+  unsigned c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  for (int i = 0; i < 10; i++) {
+    unsigned long long p0 = 0xD2511F53ull * c0;
+    unsigned long long p1 = 0xCD9E8D57ull * c2;
+    unsigned hi0 = (unsigned)(p0 >> 32), lo0 = (unsigned)p0;
+    unsigned hi1 = (unsigned)(p1 >> 32), lo1 = (unsigned)p1;
+    c0 = hi1 ^ c1 ^ k0; c1 = lo1; c2 = hi0 ^ c3 ^ k1; c3 = lo0;
+    k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// Uniform in [0,1) with 53 bits for (seed, realisation; channel, boundary, step).
+__host__ __device__ inline double channel_uniform(unsigned long long seed, unsigned realisation, unsigned channel,
+                                                  unsigned boundary, long long step) {
+  const unsigned ctr[4] = {channel, boundary, (unsigned)step, (unsigned)((unsigned long long)step >> 32)};
+  unsigned r[4];
+  philox4x32(ctr, (unsigned)seed, realisation ^ (unsigned)(seed >> 32), r);
+  return ((double)(r[0] >> 5) * 67108864.0 + (double)(r[1] >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+// Flux laws in FP64 (boundaryfluxes.c:12-141).
+__host__ __device__ inline double serca_flux(double dt, double h, double u0, double u1, const double* params) {
+  const double Ca_sr = u1 / 1000, Ca_i = u0 / 1000;
+  const double k_p1 = 25900, k_p2 = 2540, k_p3 = 20.5, k_m1 = 16, k_m2 = 67200, k_m3 = 149;
+  const double kdcai = 0.9, kdcasr = 2.24, kdh1 = 1.09e-5, kdhi = 3.54e-3, kdhsr = 1.05e-8, kdh = 7.24e-5,
+               H_i = 1e-4, ATP = 5, ADP = 36.3e-3, P_i = 1;
+  const double T_Cai = Ca_i / kdcai, T_Casr = Ca_sr / kdcasr;
+  const double T_Cai2 = T_Cai * T_Cai, T_Casr2 = T_Casr * T_Casr;
+  const double T_H1 = H_i / kdh1, T_Hi = (H_i * H_i) / kdhi, T_Hsr = (H_i * H_i) / kdhsr, T_H = H_i / kdh;
+  const double a_p1 = k_p1 * ATP;
+  const double den_i = T_Cai2 + T_Cai2 * T_Hi + T_Hi * (1 + T_H1);
+  const double den_sr = T_Casr2 * T_H + T_H + T_Hsr * (1 + T_H);
+  const double a_p2 = k_p2 * T_Cai2 / den_i;
+  const double a_p3 = k_p3 * T_Hsr / den_sr;
+  const double a_m1 = k_m1 * T_Hi / den_i;
+  const double a_m2 = k_m2 * ADP * T_Casr2 * T_H / den_sr;
+  const double a_m3 = k_m3 * P_i;
+  const double s1 = a_p2 * a_p3 + a_m1 * a_p3 + a_m1 * a_m2;
+  const double s2 = a_p1 * a_p3 + a_m2 * a_p1 + a_m2 * a_m3;
+  const double s3 = a_p1 * a_p2 + a_m3 * a_m1 + a_m3 * a_p2;
+  const double v_cycle = (a_p1 * a_p2 * a_p3 - a_m1 * a_m2 * a_m3) / (s1 + s2 + s3);
+  const double Q = 1e-3 / 6e17;
+  const double J = h * h * (params[1] * (v_cycle * Q));
+  const double V = 1e-24 * h * h * h;
+  return dt * (J / V);
+}
+
+__host__ __device__ inline double ryr_flux(double dt, double h, double u0, double u1, const double* params) {
+  const double K_0 = exp(-2 * dt * 1e15 / (2 * 96485.) * params[6] / (1300. - 0.1) / (h * h * h));
+  return (u0 - u1) * (1 - K_0) / 2;
+}
+
+}  // namespace csp

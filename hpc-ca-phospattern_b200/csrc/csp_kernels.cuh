@@ -1,0 +1,340 @@
+// csp_kernels.cuh -- the step kernels.
+//
+//   k_voxels_direct   one thread per voxel: diffusion of every species due this step,
+//                     buffer reactions, fixed values (species.c:1501-1702, 1037-1121).
+//   k_voxels_staged   (csp_staged.cuh) the same arithmetic over x-marching tiles staged
+//                     in shared memory by bulk TMA copies.
+//   k_boundaries      channel gating + boundary flux scatter + step epilogue
+//                     (species.c:1704-1957, boundaryfluxes.c:295-359, species.c:3384-3488).
+//   k_reduce_*        per (domain, species) min / max / FP64 sum (species.c:2785-2880).
+#pragma once
+#include <cfloat>
+
+#include "csp_device.cuh"
+
+namespace csp {
+
+// Device error word bits.
+enum : int { ERR_BOUNDS = 1, ERR_TIMEOUT = 2 };
+
+// What a step does for one realisation (computed once per CTA / unit).
+struct StepInfo {
+  unsigned pre;        // species flagged before the reaction (diffusing ones, species.c:1542, 1746)
+  unsigned updated;    // species written this step (apply_du copies these, species.c:1080-1121)
+  int react;           // reaction step (species.c:1657)
+  int react_fast;      // the reaction can use the per-species table (see voxel_update)
+};
+
+__host__ __device__ inline StepInfo step_info(const RealDesc& D, long long time_ind) {
+  StepInfo si;
+  unsigned diffusing;
+  step_masks(D, time_ind, si.pre, si.updated, diffusing);
+  si.react = (D.nbuf > 0 && time_ind % D.reaction_substep == 0) ? 1 : 0;
+  si.react_fast = (si.react && D.react_fast && (si.pre & 1u)) ? 1 : 0;
+  return si;
+}
+
+// Arithmetic of one voxel given its 7-point neighbourhood.  Loads go through the caller:
+// ld(s, k) = species s at neighbour k (0..5 = z-, z+, y-, y+, x-, x+; 6 = the voxel),
+// ldd(k) = the domain id there.  The direct and the staged kernel share this function,
+// so both give bitwise equal fields.  N = species slots the caller carries (>= D.ns);
+// every species index below is a compile-time constant, so nothing leaves registers.
+//
+//  diffusion (species.c:1501-1650 with the faces of :1282-1498 and kernel_generic.cpp:
+//  512-600): out = u + sum_n c[d][d_n]*(u_n - u) over the in-box neighbours; when all six
+//  neighbours share the voxel's domain this is u + c[d][d]*sum_n (u_n - u), the
+//  reference's uniform-neighbourhood fast path (kernel_generic.cpp:529-533).
+//  reactions (species.c:1653-1702, kernel_generic.cpp:397-509): J = k_on*(tot-b)*Ca -
+//  k_off*b per buffer, with the step-start values.  When every buffer binds species 0,
+//  the bound species are distinct per domain and species 0 is already updated this step,
+//  the reference's assign-or-accumulate rule reduces to accumulation and the buffers are
+//  walked per bound species (table rtab); otherwise the general rule runs (react).
+//  fixed values (species.c:1037-1077): fixed (domain, species) pairs and, with -f, the
+//  outer faces of species 0 are reset to their initial values.
+template <int N, class LoadU, class LoadD>
+__device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& si, unsigned valid, bool on_face,
+                                             LoadU ld, LoadD ldd, float (&out)[N]) {
+  const int d = ldd(6);
+  float val[N];
+#pragma unroll
+  for (int s = 0; s < N; s++) {
+    val[s] = (si.updated >> s & 1u) ? ld(s, 6) : 0.f;
+    out[s] = val[s];
+  }
+  if (si.pre) {
+    int dn[6];
+    bool uniform = true;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      dn[k] = (valid >> k & 1u) ? ldd(k) : d;
+      uniform = uniform && dn[k] == d;
+    }
+#pragma unroll
+    for (int s = 0; s < N; s++) {
+      if (!(si.pre >> s & 1u)) continue;
+      const float u = val[s];
+      float un[6];
+#pragma unroll
+      for (int k = 0; k < 6; k++) un[k] = (valid >> k & 1u) ? ld(s, k) : u;
+      const float* c = &D.coef[D.dsi_of[s]][d * ND];
+      if (uniform) {
+        float a = un[0] - u;
+#pragma unroll
+        for (int k = 1; k < 6; k++) a += un[k] - u;
+        out[s] = fmaf(c[d], a, u);
+      } else {
+        float a = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; k++) a = fmaf(c[dn[k]], un[k] - u, a);
+        out[s] = u + a;
+      }
+    }
+  }
+  if (si.react) {
+    if (si.react_fast) {
+      const float ca = val[0];
+#pragma unroll
+      for (int s = 1; s < N; s++) {
+        const int bi = D.rtab[d][s];
+        if (bi < 0) continue;
+        const int t = bi * D.nd + d;
+        const float b = val[s];
+        const float J = D.kon[t] * (D.tot[t] - b) * ca - D.koff[t] * b;
+        const float dJ = D.dt_r * J;
+        out[s] += dJ;
+        out[0] -= dJ;
+      }
+    } else {
+      react<N>(D, d, val, out, si.pre);
+    }
+  }
+  const unsigned fm = D.fixed_mask[d];
+#pragma unroll
+  for (int s = 0; s < N; s++) {
+    if (fm >> s & 1u) out[s] = D.init[d][s];
+  }
+  if (D.dirichlet && on_face) out[0] = D.init[d][0];
+}
+
+// One thread per voxel; blockIdx.y = realisation.
+__global__ void __launch_bounds__(256) k_voxels_direct(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
+                                                        int* __restrict__ err) {
+  __shared__ StepInfo s_si;
+  __shared__ unsigned s_cur;
+  const int r = blockIdx.y;
+  const RealDesc& D = descs[r];
+  RealCtl& C = ctl[r];
+  if (C.stopped) return;
+  if (threadIdx.x == 0) {
+    const long long k = C.step;
+    s_si = step_info(D, k + 1);
+    s_cur = C.cur_mask[k & 1];
+    if (blockIdx.x == 0) C.cur_mask[(k + 1) & 1] = s_cur ^ s_si.updated;
+  }
+  __syncthreads();
+  const StepInfo si = s_si;
+  const unsigned cur = s_cur;
+  const int nz = D.nz, plane = D.plane;
+  const int nvox = D.nx * plane;
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nvox || si.updated == 0) return;
+  const int x = v / plane;
+  const int p = v - x * plane;
+  const int y = p / nz;
+  const int z = p - y * nz;
+  const long long idx = (long long)x * D.P + p;
+  const unsigned valid = (z > 0 ? 1u : 0u) | (z < nz - 1 ? 2u : 0u) | (y > 0 ? 4u : 0u) |
+                         (y < D.ny - 1 ? 8u : 0u) | (x > 0 ? 16u : 0u) | (x < D.nx - 1 ? 32u : 0u);
+  // out-of-box neighbours read the voxel itself, so every address stays inside the field
+  const long long off[6] = {(valid & 1u) ? -1ll : 0ll, (valid & 2u) ? 1ll : 0ll,
+                            (valid & 4u) ? -(long long)nz : 0ll, (valid & 8u) ? (long long)nz : 0ll,
+                            (valid & 16u) ? -(long long)D.P : 0ll, (valid & 32u) ? (long long)D.P : 0ll};
+  const bool on_face = valid != 63u;
+  auto ld = [&](int s, int kk) -> float {
+    const float* __restrict__ u = D.u[(cur >> s) & 1u][s];
+    return __ldg(u + idx + (kk < 6 ? off[kk] : 0));
+  };
+  auto ldd = [&](int kk) -> int { return __ldg(D.dom + idx + (kk < 6 ? off[kk] : 0)); };
+  float out[NS];
+  voxel_update<NS>(D, si, valid, on_face, ld, ldd, out);
+#pragma unroll
+  for (int s = 0; s < NS; s++) {
+    if (s < D.ns && (si.updated >> s & 1u)) D.u[((cur >> s) & 1u) ^ 1u][s][idx] = out[s];
+  }
+}
+
+// Channel gating of one channel at step time_ind (evaluate_RyR_stochastically,
+// boundaryfluxes.c:295-359), with the Philox stream of the realisation.
+__device__ __forceinline__ int gate(const FluxParams& fp, int state, double c0, double t, double dts,
+                                    unsigned long long seed, unsigned r, unsigned ch, unsigned boundary,
+                                    long long time_ind) {
+  const double* p = fp.p;
+  if (p[8] > 0) {
+    if (p[8] <= t + dts) return 0;
+    return state;
+  }
+  const double kc = fmax(fmin(pow(c0 / p[0], p[5]), p[1]), p[7]);
+  const double ko = fmax(fmin(pow(c0 / p[9], p[2]), p[3]), p[4]);
+  const double rv = channel_uniform(seed, r, ch, boundary, time_ind);
+  if (state == 0) return rv <= dts * ko ? 1 : 0;
+  if (state == 1) return rv <= dts * kc ? 0 : 1;
+  return state;
+}
+
+// One thread per flux row (a voxel receiving boundary flux).  Each row sums, in pair
+// order, the flux of every pair that touches it, with the channel states after this
+// step's gating; the owner entry of a channel stores its new state.  The last block
+// to finish runs the step epilogue for every realisation.
+__global__ void __launch_bounds__(256) k_boundaries(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
+                                                     const FluxRow* __restrict__ rows, int nrows,
+                                                     const FluxEntry* __restrict__ entries,
+                                                     const FluxPair* __restrict__ pairs,
+                                                     const FluxParams* __restrict__ params,
+                                                     unsigned char* __restrict__ states,  // [2][nch]
+                                                     int nch, int nreal,
+                                                     unsigned* __restrict__ ticket) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nrows) {
+    const FluxRow row = rows[i];
+    const RealDesc& D = descs[row.r];
+    const RealCtl& C = ctl[row.r];
+    if (!C.stopped) {
+      const long long k = C.step;
+      const long long ti = k + 1;
+      unsigned pre, updated, diffusing;
+      step_masks(D, ti, pre, updated, diffusing);
+      const unsigned cur = C.cur_mask[k & 1];
+      const bool stoch = (ti % D.stochastic_substep) == 0;
+      const double t = (double)ti * D.dt, dts = D.dt * D.stochastic_substep;
+      const float* __restrict__ uold = D.u[(cur >> row.species) & 1u][row.species];
+      const float* __restrict__ ca = D.u[cur & 1u][0];
+      double acc = 0.0;
+      bool any = false;
+      for (int e = row.begin; e < row.end; e++) {
+        const FluxEntry en = entries[e];
+        const FluxPair pr = pairs[en.pair];
+        const FluxParams& fp = params[pr.param];
+        if (pr.channel >= 0) {
+          int s_old = states[(k & 1) * (long long)nch + pr.channel];
+          int s_new = s_old;
+          if (stoch && pr.kind != FLUX_SERCA)
+            s_new = gate(fp, s_old, (double)__ldg(ca + pr.v1), t, dts, D.seed, (unsigned)row.r,
+                         (unsigned)pr.local_channel, (unsigned)pr.boundary, ti);
+          if (en.owner) {
+            states[((k + 1) & 1) * (long long)nch + pr.channel] = (unsigned char)s_new;
+            if (s_new == 1) atomicAdd(&ctl[row.r].open_count[(k + 1) & 1], 1);
+          }
+          if (s_new != 1) continue;
+        }
+        if (ti % D.substeps[pr.dsi] != 0) continue;
+        const double u0 = (double)__ldg(uold + pr.v0), u1 = (double)__ldg(uold + pr.v1);
+        const double J = pr.kind == FLUX_SERCA ? serca_flux(D.dt, D.h, u0, u1, fp.p) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
+        acc += (double)en.sign * J;
+        any = true;
+      }
+      if (any && row.apply && (updated >> row.species & 1u)) {
+        float* unew = D.u[((cur >> row.species) & 1u) ^ 1u][row.species];
+        unew[row.v] = (float)((double)unew[row.v] + acc);
+      }
+    }
+  }
+  // step epilogue, by the last block to finish
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int r = threadIdx.x; r < nreal; r += blockDim.x) {
+    RealCtl& C = ctl[r];
+    if (C.stopped) continue;
+    const RealDesc& D = descs[r];
+    const long long k = C.step;
+    const long long ti = k + 1;
+    const int open = C.open_count[(k + 1) & 1];
+    C.open_count[k & 1] = 0;
+    C.step = ti;
+    if (D.has_channels && D.tabort != 0) {
+      // abort rule (species.c:3476-3486) on the current openness
+      const double tt = (double)ti * D.dt;
+      if (open) {
+        C.last_closed = -1.0;
+      } else if (D.tabort >= 0) {
+        if (C.last_closed < 0) C.last_closed = tt;
+        if (tt - C.last_closed >= D.tabort) C.stopped = 1;
+      }
+    }
+    if (C.step >= D.total_steps) C.stopped = 1;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Output reductions: partial min / max / sum over a block for one species of one
+// realisation, then a fixed-order final pass (deterministic FP64 sums).
+__global__ void __launch_bounds__(256) k_reduce_partial(const RealDesc* __restrict__ descs,
+                                                         const RealCtl* __restrict__ ctl, int r, int s,
+                                                         double* __restrict__ part /*[nblk][3][ND]*/) {
+  const RealDesc& D = descs[r];
+  const unsigned cur = ctl[r].cur_mask[ctl[r].step & 1];
+  const float* __restrict__ u = D.u[(cur >> s) & 1u][s];
+  double mn[ND], mx[ND], sm[ND];
+#pragma unroll
+  for (int d = 0; d < ND; d++) { mn[d] = FLT_MAX; mx[d] = FLT_MIN; sm[d] = 0.0; }
+  const long long nvox = (long long)D.nx * D.plane;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(v / D.plane);
+    const long long idx = (long long)x * D.P + (v - (long long)x * D.plane);
+    const int d = D.dom[idx];
+    const double val = (double)u[idx];
+#pragma unroll
+    for (int dd = 0; dd < ND; dd++) {
+      if (dd == d) {
+        mn[dd] = val < mn[dd] ? val : mn[dd];
+        mx[dd] = val > mx[dd] ? val : mx[dd];
+        sm[dd] += val;
+      }
+    }
+  }
+  __shared__ double red[3][ND][256];
+#pragma unroll
+  for (int d = 0; d < ND; d++) { red[0][d][threadIdx.x] = mn[d]; red[1][d][threadIdx.x] = mx[d]; red[2][d][threadIdx.x] = sm[d]; }
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        double a = red[0][d][threadIdx.x + w];
+        if (a < red[0][d][threadIdx.x]) red[0][d][threadIdx.x] = a;
+        a = red[1][d][threadIdx.x + w];
+        if (a > red[1][d][threadIdx.x]) red[1][d][threadIdx.x] = a;
+        red[2][d][threadIdx.x] += red[2][d][threadIdx.x + w];
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < ND) {
+    const int d = threadIdx.x;
+    part[(blockIdx.x * 3 + 0) * ND + d] = red[0][d][0];
+    part[(blockIdx.x * 3 + 1) * ND + d] = red[1][d][0];
+    part[(blockIdx.x * 3 + 2) * ND + d] = red[2][d][0];
+  }
+}
+
+__global__ void k_reduce_final(const double* __restrict__ part, int nblk, double dV,
+                               double* __restrict__ out /*[3][ND]*/) {
+  const int d = threadIdx.x;
+  if (d >= ND) return;
+  double mn = FLT_MAX, mx = FLT_MIN, sm = 0.0;
+  for (int b = 0; b < nblk; b++) {
+    const double a = part[(b * 3 + 0) * ND + d], c = part[(b * 3 + 1) * ND + d];
+    mn = a < mn ? a : mn;
+    mx = c > mx ? c : mx;
+    sm += part[(b * 3 + 2) * ND + d];
+  }
+  out[0 * ND + d] = mn;
+  out[1 * ND + d] = mx;
+  out[2 * ND + d] = sm * dV;
+}
+
+}  // namespace csp

@@ -1,0 +1,821 @@
+// csp_runtime.cu -- libcsparks_cuda.so: the C ABI of include/csparks.h.
+//
+// Host side: derive every per-realisation constant from the model and options exactly
+// as the reference setup does (species.c:95-884, geometry.c:96-344,
+// boundaryfluxes.c:361-605), build the boundary-flux rows, allocate HBM, and drive the
+// step kernels (direct launches, or replay of a captured CUDA graph of STEPS_PER_GRAPH
+// steps: the kernels read the step index from device memory, so one graph serves
+// every cycle).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <vector>
+
+#include "csp_kernels.cuh"
+#include "csp_staged.cuh"
+
+using namespace csp;
+
+namespace {
+
+constexpr int STEPS_PER_GRAPH = 16;
+thread_local char g_create_error[512];
+
+struct HostReal {
+  RealDesc desc;                  // host copy (device pointers filled in)
+  csp_info info;
+  int nd;
+  double dV;
+  double volumes[ND];
+  std::vector<int> boundary_channel_base;   // per boundary: first global channel, or -1
+  std::vector<int> boundary_nch;
+  size_t field_elems;             // nx*P
+};
+
+}  // namespace
+
+struct csp_handle {
+  int n = 0;
+  std::vector<HostReal> real;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  // device memory
+  float* d_fields = nullptr;
+  unsigned char* d_dom = nullptr;
+  RealDesc* d_desc = nullptr;
+  RealCtl* d_ctl = nullptr;
+  FluxRow* d_rows = nullptr;
+  FluxEntry* d_entries = nullptr;
+  FluxPair* d_pairs = nullptr;
+  FluxParams* d_params = nullptr;
+  unsigned char* d_states = nullptr;
+  unsigned* d_ticket = nullptr;
+  int* d_err = nullptr;
+  double* d_red = nullptr;
+  double* d_red_out = nullptr;
+  int nrows = 0, nch = 0;
+  int max_plane_vox = 0;
+  long long max_vox = 0;
+  int kernel = 0;                 // 0 staged, 1 direct
+  StagedPlan plan;
+  cudaGraphExec_t graph = nullptr;
+  int graph_kernel = -1;
+  std::string msg;
+};
+
+static int fail(csp_handle* h, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (h) h->msg = buf; else snprintf(g_create_error, sizeof g_create_error, "%s", buf);
+  return code;
+}
+
+#define CUDA_TRY(h, call)                                                                     \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return fail(h, CSP_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+static int name_index(const char names[][CSP_NAME_LEN], int n, const char* s) {
+  for (int i = 0; i < n; i++)
+    if (strncmp(names[i], s, CSP_NAME_LEN) == 0) return i;
+  return -1;
+}
+
+static int boundary_index(const csp_model& m, const char* name) {
+  for (int i = 0; i < m.num_boundaries; i++)
+    if (strncmp(m.boundaries[i].name, name, CSP_NAME_LEN) == 0) return i;
+  return -1;
+}
+
+extern "C" void csp_options_default(csp_options* o) {
+  // arguments_construct, options.c:502-542
+  memset(o, 0, sizeof(*o));
+  o->h = 6.;
+  o->dt = -1.;
+  o->tstop = 10.;
+  o->dt_save = .5;
+  o->dt_update_react = -1.;
+  o->dt_update_stoch = -1.;
+  o->tabort = 0.;
+}
+
+namespace {
+
+// Per-realisation constants (species.c:181-313, 784-787; geometry.c:104-105).
+struct Derived {
+  int S, nx, ny, nz;
+  double h, dt;
+  int ndiff;
+  int diff_species[NS], substeps[NS];
+  double coef[NS][ND][ND];
+  int nbuf;
+  double kon[NB * ND], koff[NB * ND], tot[NB * ND];
+  unsigned char bsp0[NB * ND], bsp1[NB * ND];
+  unsigned reaction_flag_mask;
+  int reaction_substep, stochastic_substep;
+  long long total_steps;
+};
+
+int derive(const csp_model& m, const csp_options& o, Derived& dv, std::string& err) {
+  if (m.num_domains < 1 || m.num_domains > ND) { err = "num_domains out of range (max 5)"; return CSP_EINVAL; }
+  if (m.num_species < 1 || m.num_species > NS) { err = "num_species out of range (max 8)"; return CSP_EINVAL; }
+  if (m.num_boundaries < 0 || m.num_boundaries > CSP_MAX_BOUNDARIES) { err = "num_boundaries out of range"; return CSP_EINVAL; }
+  if (!m.voxels) { err = "voxels is NULL"; return CSP_EINVAL; }
+  if (!(o.h > 0)) { err = "resolution -h must be positive"; return CSP_EINVAL; }
+  for (int a = 0; a < 3; a++)
+    if (m.N[a] < 1) { err = "geometry size must be positive"; return CSP_EINVAL; }
+  int S = (int)std::fmax(1., std::floor(m.h_geom / o.h));
+  S &= 0xff;  // Geometry_t::subdivisions is a domain_id
+  if (S == 0) { err = "subdivisions overflow (h_geom/h >= 256)"; return CSP_EINVAL; }
+  dv.S = S;
+  dv.h = m.h_geom / S;
+  dv.nx = m.N[0] * S; dv.ny = m.N[1] * S; dv.nz = m.N[2] * S;
+  const int nd = m.num_domains;
+  double max_sigma = 0, max_sigma_species[NS] = {0};
+  bool is_diff[NS] = {false};
+  for (int d = 0; d < nd; d++) {
+    const csp_domain_species& ds = m.domain[d];
+    if (ds.num_diffusive < 0 || ds.num_diffusive > NS || ds.num_buffers < 0 || ds.num_buffers > NB) {
+      err = "per-domain species counts out of range"; return CSP_EINVAL;
+    }
+    for (int k = 0; k < ds.num_diffusive; k++) {
+      const int s = ds.diffusive[k];
+      if (s >= m.num_species) { err = "diffusive species index out of range"; return CSP_EINVAL; }
+      is_diff[s] = true;
+      max_sigma = std::fmax(max_sigma, ds.sigma[k]);
+      max_sigma_species[s] = std::fmax(ds.sigma[k], max_sigma_species[s]);
+    }
+  }
+  dv.dt = o.dt > 0 ? o.dt : 0.95 * (1. / 6) * dv.h * dv.h / max_sigma;  // species.c:265
+  if (!(dv.dt > 0) || !std::isfinite(dv.dt)) { err = "time step is not positive (no diffusive species and no -d?)"; return CSP_EINVAL; }
+  dv.ndiff = 0;
+  for (int s = 0; s < m.num_species; s++) {  // species.c:281-294
+    if (!is_diff[s]) continue;
+    const double sdt = std::fabs(max_sigma - max_sigma_species[s]) < 1e-12
+                           ? dv.dt : 0.95 * (1. / 6) * dv.h * dv.h / max_sigma_species[s];
+    dv.substeps[dv.ndiff] = ((int)std::fmax(1., std::floor(sdt / dv.dt))) & 0xff;
+    if (dv.substeps[dv.ndiff] == 0) { err = "species substeps overflow"; return CSP_EINVAL; }
+    dv.diff_species[dv.ndiff++] = s;
+  }
+  // coefficient tables, species.c:1545-1560: sigma[di][dsi] is indexed by the diffusive
+  // index dsi, i.e. a domain's diffusive list is expected to follow the global order.
+  for (int dsi = 0; dsi < dv.ndiff; dsi++) {
+    for (int a = 0; a < ND; a++)
+      for (int b = 0; b < ND; b++) dv.coef[dsi][a][b] = 0.0;
+    for (int di = 0; di < nd; di++) {
+      const csp_domain_species& A = m.domain[di];
+      if (!(dsi < A.num_diffusive && A.sigma[dsi] != 0)) continue;
+      for (int dn = 0; dn < di; dn++) {
+        const csp_domain_species& B = m.domain[dn];
+        if (m.domain_connections[di * nd + dn] && dsi < B.num_diffusive && B.sigma[dsi] != 0)
+          dv.coef[dsi][di][dn] = dv.coef[dsi][dn][di] =
+              dv.dt * 0.5 * (A.sigma[dsi] + B.sigma[dsi]) / (dv.h * dv.h) * dv.substeps[dsi];
+      }
+      dv.coef[dsi][di][di] = dv.dt * A.sigma[dsi] / (dv.h * dv.h) * dv.substeps[dsi];
+    }
+  }
+  // buffer tables (species.c:134-145, 216-241, 304-313)
+  memset(dv.kon, 0, sizeof dv.kon); memset(dv.koff, 0, sizeof dv.koff); memset(dv.tot, 0, sizeof dv.tot);
+  memset(dv.bsp0, 0, sizeof dv.bsp0); memset(dv.bsp1, 0, sizeof dv.bsp1);
+  bool is_buf[NS] = {false};
+  unsigned char bsp0_dom[ND][NS] = {{0}}, bsp1_dom[ND][NS] = {{0}};
+  for (int d = 0; d < nd; d++) {
+    const csp_domain_species& ds = m.domain[d];
+    for (int bi = 0; bi < ds.num_buffers; bi++) {
+      if (ds.bsp0[bi] >= m.num_species || ds.bsp1[bi] >= m.num_species) { err = "buffer species index out of range"; return CSP_EINVAL; }
+      dv.bsp0[bi * nd + d] = ds.bsp0[bi]; dv.bsp1[bi * nd + d] = ds.bsp1[bi];
+      dv.kon[bi * nd + d] = ds.k_on[bi]; dv.koff[bi * nd + d] = ds.k_off[bi]; dv.tot[bi * nd + d] = ds.tot[bi];
+      bsp0_dom[d][bi] = ds.bsp0[bi]; bsp1_dom[d][bi] = ds.bsp1[bi];
+      is_buf[ds.bsp0[bi]] = true;
+    }
+  }
+  dv.nbuf = 0;
+  for (int s = 0; s < m.num_species; s++) dv.nbuf += is_buf[s];
+  for (int d = 0; d < nd; d++)
+    if (m.domain[d].num_buffers > dv.nbuf) { err = "a domain holds more buffers than there are buffer species"; return CSP_EINVAL; }
+  dv.reaction_flag_mask = 0;  // species.c:1695-1699
+  for (int d = 0; d < nd; d++)
+    for (int bi = 0; bi < dv.nbuf; bi++) dv.reaction_flag_mask |= (1u << bsp0_dom[d][bi]) | (1u << bsp1_dom[d][bi]);
+  dv.stochastic_substep = (int)std::fmax(1., std::floor(o.dt_update_stoch / dv.dt));  // species.c:784
+  dv.reaction_substep = (int)std::fmax(1., std::floor(o.dt_update_react / dv.dt));    // species.c:787
+  long long steps = 0;
+  for (double t = 0.; t < o.tstop; t += dv.dt) steps++;  // calcium_sparks.c:190
+  dv.total_steps = steps;
+  return CSP_OK;
+}
+
+struct PairHost {
+  FluxPair p;
+};
+
+}  // namespace
+
+// Species voxel pairs of one geometry boundary (Species_init_boundary_voxels,
+// species.c:938-1035); coordinates in species voxels, [n][6].
+static void boundary_species_pairs(const csp_boundary& gb, int S, std::vector<unsigned>& out) {
+  const int sub = gb.type == CSP_BOUNDARY_DISCRETE ? 1 : S;
+  out.assign((size_t)gb.num_pairs * sub * sub * 6, 0u);
+  for (int j = 0; j < gb.num_pairs; j++) {
+    const uint16_t* lb = &gb.pairs[6 * j];
+    int dim2 = 0;  // Geometry_get_boundary_dir, geometry.c:1490-1530
+    for (int dim = 0; dim < 3; dim++)
+      if (lb[dim] != lb[dim + 3]) { dim2 = lb[dim] < lb[dim + 3] ? 2 * dim : 2 * dim + 1; break; }
+    const int dim = dim2 / 2, lr = dim2 % 2;
+    const int odim = dim != 0 ? 0 : 1, idim = dim != 2 ? 2 : 1;
+    const unsigned from_ind = lb[dim] * S + (lr == 0 ? S - 1 : 0);
+    const unsigned to_ind = lb[dim + 3] * S + (lr == 0 ? 0 : S - 1);
+    for (int oi = 0; oi < sub; oi++) {
+      unsigned o_ind = S * lb[odim] + oi;
+      if (gb.type == CSP_BOUNDARY_DISCRETE) o_ind += S / 2;
+      for (int ii = 0; ii < sub; ii++) {
+        unsigned i_ind = S * lb[idim] + ii;
+        if (gb.type == CSP_BOUNDARY_DISCRETE) i_ind += S / 2;
+        unsigned* v = &out[((size_t)j * sub * sub + oi * sub + ii) * 6];
+        v[dim] = from_ind; v[odim] = o_ind; v[idim] = i_ind;
+        v[dim + 3] = to_ind; v[odim + 3] = o_ind; v[idim + 3] = i_ind;
+      }
+    }
+  }
+}
+
+static const csp_open_list* open_list(const csp_options& o, const char* name) {
+  for (int i = 0; i < o.num_open_lists; i++)
+    if (strncmp(o.open[i].name, name, CSP_NAME_LEN) == 0) return &o.open[i];
+  return nullptr;
+}
+
+static double t_close_of(const csp_options& o, const char* name) {
+  for (int i = 0; i < o.num_t_close; i++)
+    if (strncmp(o.t_close[i].name, name, CSP_NAME_LEN) == 0) return o.t_close[i].time;
+  return -1;
+}
+
+static void ryr_params(FluxParams& fp, const csp_ryr_params& p, double t_close) {
+  // RyR_model::params layout, boundaryfluxes.c:445-454
+  fp.p[0] = p.Kd_close; fp.p[1] = p.k_max_close; fp.p[2] = p.n_open; fp.p[3] = p.k_max_open;
+  fp.p[4] = p.k_min_open; fp.p[5] = p.n_close; fp.p[6] = p.i_unitary; fp.p[7] = p.k_min_close;
+  fp.p[8] = t_close; fp.p[9] = p.Kd_open;
+  fp.t_close = t_close;
+}
+
+static int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+extern "C" int csp_create(const csp_model* models, const csp_options* options, int32_t n, csp_handle** out) {
+  if (!out) return fail(nullptr, CSP_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!models || !options || n < 1) return fail(nullptr, CSP_EINVAL, "models/options NULL or n < 1");
+  csp_handle* h = new csp_handle();
+  h->n = n;
+  h->real.resize(n);
+  std::vector<Derived> dv(n);
+  size_t field_total = 0, dom_total = 0;
+  for (int r = 0; r < n; r++) {
+    std::string err;
+    int rc = derive(models[r], options[r], dv[r], err);
+    if (rc) { delete h; return fail(nullptr, rc, "realisation %d: %s", r, err.c_str()); }
+    const int plane = dv[r].ny * dv[r].nz;
+    const int P = round_up(plane, PLANE_ALIGN);
+    h->real[r].field_elems = (size_t)dv[r].nx * P;
+    field_total += h->real[r].field_elems * 2 * models[r].num_species;
+    dom_total += h->real[r].field_elems;
+    h->max_plane_vox = std::max(h->max_plane_vox, plane);
+    h->max_vox = std::max(h->max_vox, (long long)dv[r].nx * plane);
+  }
+  // -- device allocation (one arena for all fields) --
+  cudaError_t e;
+  if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreate(&h->ev0)) != cudaSuccess || (e = cudaEventCreate(&h->ev1)) != cudaSuccess) {
+    csp_destroy(h);
+    return fail(nullptr, CSP_ECUDA, "stream/event creation: %s", cudaGetErrorString(e));
+  }
+  if (cudaMalloc(&h->d_fields, field_total * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h->d_dom, dom_total + 256) != cudaSuccess ||
+      cudaMalloc(&h->d_desc, n * sizeof(RealDesc)) != cudaSuccess ||
+      cudaMalloc(&h->d_ctl, n * sizeof(RealCtl)) != cudaSuccess ||
+      cudaMalloc(&h->d_ticket, sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess) {
+    csp_destroy(h);
+    return fail(nullptr, CSP_ENOMEM, "device allocation of %.3f GB failed",
+                (field_total * 4.0 + dom_total) / 1e9);
+  }
+  cudaMemsetAsync(h->d_ticket, 0, sizeof(unsigned), h->stream);
+  cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
+  cudaMemsetAsync(h->d_fields, 0, field_total * sizeof(float), h->stream);
+  cudaMemsetAsync(h->d_dom, 0, dom_total + 256, h->stream);
+
+  std::vector<FluxPair> pairs;
+  std::vector<FluxParams> params;
+  std::vector<unsigned char> states0;
+  std::vector<RealCtl> ctl(n);
+  size_t foff = 0, doff = 0;
+  std::vector<float> hostf;
+  std::vector<unsigned char> hostd;
+  for (int r = 0; r < n; r++) {
+    const csp_model& m = models[r];
+    const csp_options& o = options[r];
+    const Derived& d = dv[r];
+    HostReal& hr = h->real[r];
+    RealDesc& D = hr.desc;
+    memset(&D, 0, sizeof D);
+    const int nd = m.num_domains;
+    hr.nd = nd;
+    D.nx = d.nx; D.ny = d.ny; D.nz = d.nz;
+    D.plane = d.ny * d.nz;
+    D.P = round_up(D.plane, PLANE_ALIGN);
+    D.ns = m.num_species; D.nd = nd; D.ndiff = d.ndiff; D.nbuf = d.nbuf;
+    D.reaction_substep = d.reaction_substep; D.stochastic_substep = d.stochastic_substep;
+    D.dirichlet = o.force_dirichlet ? 1 : 0;
+    for (int k = 0; k < d.ndiff; k++) { D.substeps[k] = d.substeps[k]; D.diff_species[k] = d.diff_species[k]; }
+    D.reaction_flag_mask = d.reaction_flag_mask;
+    D.dt_r = (float)(d.dt * d.reaction_substep);
+    for (int k = 0; k < d.ndiff; k++)
+      for (int a = 0; a < ND; a++)
+        for (int b = 0; b < ND; b++) D.coef[k][a * ND + b] = (float)d.coef[k][a][b];
+    for (int t = 0; t < NB * ND; t++) {
+      D.kon[t] = (float)d.kon[t]; D.koff[t] = (float)d.koff[t]; D.tot[t] = (float)d.tot[t];
+      D.bsp0[t] = d.bsp0[t]; D.bsp1[t] = d.bsp1[t];
+    }
+    // per-species lookup tables of the voxel kernels
+    for (int s = 0; s < NS; s++) D.dsi_of[s] = -1;
+    for (int k = 0; k < d.ndiff; k++) D.dsi_of[d.diff_species[k]] = (signed char)k;
+    D.react_fast = 1;
+    for (int dd = 0; dd < ND; dd++)
+      for (int s = 0; s < NS; s++) D.rtab[dd][s] = -1;
+    for (int dd = 0; dd < nd; dd++)
+      for (int bi = 0; bi < m.domain[dd].num_buffers; bi++) {
+        const int s0 = m.domain[dd].bsp0[bi], s1 = m.domain[dd].bsp1[bi];
+        if (s1 != 0 || s0 == 0 || D.rtab[dd][s0] >= 0) D.react_fast = 0;
+        else D.rtab[dd][s0] = (signed char)bi;
+      }
+    for (int i = 0; i < m.num_fixed_domain_species; i++) {
+      const int dd = m.fixed_domain_species[2 * i], s = m.fixed_domain_species[2 * i + 1];
+      if (dd >= nd || s >= m.num_species) { csp_destroy(h); return fail(nullptr, CSP_EINVAL, "fixed_domain_species out of range"); }
+      D.fixed_mask[dd] |= (unsigned char)(1u << s);
+    }
+    for (int dd = 0; dd < nd; dd++)
+      for (int s = 0; s < m.num_species; s++) D.init[dd][s] = (float)m.domain[dd].init[s];
+    D.total_steps = d.total_steps;
+    D.dt = d.dt; D.h = d.h; D.tabort = o.tabort;
+    D.seed = o.seed;
+    for (int b = 0; b < 2; b++)
+      for (int s = 0; s < m.num_species; s++) {
+        D.u[b][s] = h->d_fields + foff;
+        foff += hr.field_elems;
+      }
+    D.dom = h->d_dom + doff;
+    doff += hr.field_elems;
+    hr.dV = d.h * d.h * d.h;
+    // species voxel domains (species.c:596-605) and the initial state (species.c:887-935)
+    hostd.assign(hr.field_elems, 0);
+    long gcount[ND] = {0};
+    for (int x = 0; x < d.nx; x++)
+      for (int y = 0; y < d.ny; y++)
+        for (int z = 0; z < d.nz; z++) {
+          const unsigned char dd =
+              m.voxels[((size_t)(x / d.S) * m.N[1] + y / d.S) * m.N[2] + z / d.S];
+          if (dd >= nd) { csp_destroy(h); return fail(nullptr, CSP_EINVAL, "voxel domain id %d >= num_domains", dd); }
+          hostd[(size_t)x * D.P + y * d.nz + z] = dd;
+        }
+    for (size_t i = 0; i < (size_t)m.N[0] * m.N[1] * m.N[2]; i++) gcount[m.voxels[i]]++;
+    for (int dd = 0; dd < ND; dd++) hr.volumes[dd] = dd < nd ? gcount[dd] * m.h_geom * m.h_geom * m.h_geom : 0.0;
+    cudaMemcpyAsync((void*)D.dom, hostd.data(), hr.field_elems, cudaMemcpyHostToDevice, h->stream);
+    hostf.assign(hr.field_elems, 0.f);
+    for (int s = 0; s < m.num_species; s++) {
+      for (size_t i = 0; i < hr.field_elems; i++) hostf[i] = (float)m.domain[hostd[i]].init[s];
+      cudaMemcpyAsync(D.u[0][s], hostf.data(), hr.field_elems * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+      cudaStreamSynchronize(h->stream);
+    }
+    // -- boundaries, flux map and channels (boundaryfluxes.c:361-605) --
+    hr.boundary_channel_base.assign(m.num_boundaries, -1);
+    hr.boundary_nch.assign(m.num_boundaries, 0);
+    int bmap[3] = {-1, -1, -1};
+    if (m.use_ryr) bmap[0] = boundary_index(m, m.ryr.boundary);
+    if (m.use_p_ryr) bmap[1] = boundary_index(m, m.p_ryr.boundary);
+    if (m.use_serca) bmap[2] = boundary_index(m, m.serca.boundary);
+    for (int k = 0; k < 3; k++)
+      if ((k == 0 ? m.use_ryr : k == 1 ? m.use_p_ryr : m.use_serca) && bmap[k] < 0) {
+        csp_destroy(h);
+        return fail(nullptr, CSP_EINVAL, "flux boundary \"%s\" not in the geometry",
+                    k == 0 ? m.ryr.boundary : k == 1 ? m.p_ryr.boundary : m.serca.boundary);
+      }
+    std::vector<std::vector<unsigned>> bvox(m.num_boundaries);
+    for (int bi = 0; bi < m.num_boundaries; bi++) {
+      const csp_boundary& gb = m.boundaries[bi];
+      if (gb.num_pairs > 0 && !gb.pairs) { csp_destroy(h); return fail(nullptr, CSP_EINVAL, "boundary %d pairs NULL", bi); }
+      for (int j = 0; j < gb.num_pairs * 6; j++)
+        if (gb.pairs[j] >= m.N[j % 3]) { csp_destroy(h); return fail(nullptr, CSP_EINVAL, "boundary %s voxel out of the geometry", gb.name); }
+      boundary_species_pairs(gb, d.S, bvox[bi]);
+      if (gb.type == CSP_BOUNDARY_DISCRETE) {
+        hr.boundary_channel_base[bi] = (int)states0.size();
+        hr.boundary_nch[bi] = gb.num_pairs;
+        states0.resize(states0.size() + gb.num_pairs, 0);
+        D.has_channels = 1;
+      }
+    }
+    auto lin = [&](const unsigned* c) -> long long { return (long long)c[0] * D.P + (long long)c[1] * d.nz + c[2]; };
+    // flux info per boundary: first of ryr, p_ryr, serca (BoundaryFluxes_get_flux_info)
+    for (int bi = 0; bi < m.num_boundaries; bi++) {
+      int kind = FLUX_NONE;
+      for (int k = 0; k < 3; k++)
+        if (bmap[k] == bi) { kind = k + 1; break; }
+      if (kind == FLUX_NONE) continue;
+      const char* spname = kind == FLUX_RYR ? m.ryr.species : kind == FLUX_P_RYR ? m.p_ryr.species : m.serca.species;
+      const int si = name_index(m.species_names, m.num_species, spname);
+      int dsi = -1;
+      for (int k = 0; k < d.ndiff; k++)
+        if (d.diff_species[k] == si) dsi = k;
+      if (si < 0 || dsi < 0) { csp_destroy(h); return fail(nullptr, CSP_EINVAL, "\"%s\" is not a valid diffusive species name", spname); }
+      FluxParams fp;
+      memset(&fp, 0, sizeof fp);
+      if (kind == FLUX_RYR) ryr_params(fp, m.ryr, t_close_of(o, "ryr"));
+      else if (kind == FLUX_P_RYR) ryr_params(fp, m.p_ryr, t_close_of(o, "p_ryr"));
+      else { fp.p[0] = m.serca.v_cyt_to_A_sr; fp.p[1] = m.serca.density; fp.p[2] = m.serca.scale; fp.t_close = -1; }
+      const int pidx = (int)params.size();
+      params.push_back(fp);
+      const csp_boundary& gb = m.boundaries[bi];
+      const std::vector<unsigned>& bv = bvox[bi];
+      const int np = (int)(bv.size() / 6);
+      const bool inner = gb.num_pairs > 0 && !(gb.pairs[0] == gb.pairs[3] && gb.pairs[1] == gb.pairs[4] && gb.pairs[2] == gb.pairs[5]);
+      for (int i = 0; i < np; i++) {
+        FluxPair p;
+        memset(&p, 0, sizeof p);
+        p.r = r; p.species = si; p.dsi = dsi; p.kind = kind; p.boundary = bi; p.inner = inner ? 1 : 0;
+        p.param = pidx;
+        p.channel = gb.type == CSP_BOUNDARY_DISCRETE ? hr.boundary_channel_base[bi] + i : -1;
+        p.local_channel = i;
+        p.v0 = lin(&bv[6 * i]);
+        p.v1 = lin(&bv[6 * i + 3]);
+        pairs.push_back(p);
+      }
+    }
+    // initial channel states (BoundaryFluxes_init_stochastic_boundaries, boundaryfluxes.c:544-605)
+    int ndiscrete = 0;
+    for (int bi = 0; bi < m.num_boundaries; bi++) ndiscrete += m.boundaries[bi].type == CSP_BOUNDARY_DISCRETE;
+    if (m.use_ryr && ndiscrete > 0) {
+      const int rb = bmap[0];
+      const std::vector<unsigned>& rv = bvox[rb];
+      const int nr = (int)(rv.size() / 6);
+      auto c0_at = [&](const std::vector<unsigned>& bv, int i) -> double {
+        const unsigned* c = &bv[6 * i + 3];
+        const int x = c[0], y = c[1], z = c[2];
+        const unsigned char dd = m.voxels[((size_t)(x / d.S) * m.N[1] + y / d.S) * m.N[2] + z / d.S];
+        return m.domain[dd].init[0];
+      };
+      auto init_boundary = [&](int bi, const csp_ryr_params& rp, const char* bname, bool use_ryr_values) -> int {
+        const int base = hr.boundary_channel_base[bi];
+        if (base < 0) return CSP_OK;
+        const int nchb = hr.boundary_nch[bi];
+        const csp_open_list* ol = open_list(o, bname);
+        if (ol) {
+          for (int i = 0; i < ol->count; i++) {
+            if (ol->indices[i] < 0 || ol->indices[i] >= nchb) return CSP_ERANGE;
+            states0[base + ol->indices[i]] = 1;
+          }
+          return CSP_OK;
+        }
+        FluxParams fp;
+        ryr_params(fp, rp, -1);
+        const double* p = fp.p;
+        for (int i = 0; i < nchb; i++) {
+          // the reference reads the ryr boundary's Ca for the p_ryr draw (boundaryfluxes.c:595-597)
+          const double c0 = use_ryr_values && i < nr ? c0_at(rv, i) : c0_at(bvox[bi], i);
+          const double ko = std::fmax(std::fmin(std::pow(c0 / p[9], p[2]), p[3]), p[4]);
+          const double kc = std::fmax(std::fmin(std::pow(c0 / p[0], p[5]), p[1]), p[7]);
+          const double rv_ = channel_uniform(o.seed, (unsigned)r, (unsigned)i, (unsigned)bi, 0);
+          states0[base + i] = rv_ <= kc / (ko + kc) ? 0 : 1;
+        }
+        return CSP_OK;
+      };
+      if (init_boundary(rb, m.ryr, m.ryr.boundary, false)) { csp_destroy(h); return fail(nullptr, CSP_ERANGE, "-O index out of range for %s", m.ryr.boundary); }
+      if (m.use_p_ryr && bmap[1] >= 0 &&
+          init_boundary(bmap[1], m.p_ryr, m.p_ryr.boundary, true)) {
+        csp_destroy(h);
+        return fail(nullptr, CSP_ERANGE, "-O index out of range for %s", m.p_ryr.boundary);
+      }
+    }
+    // info
+    csp_info& in = hr.info;
+    memset(&in, 0, sizeof in);
+    in.n[0] = d.nx; in.n[1] = d.ny; in.n[2] = d.nz;
+    in.subdivisions = d.S; in.h = d.h; in.dt = d.dt;
+    in.num_species = m.num_species; in.num_diffusive = d.ndiff;
+    for (int k = 0; k < d.ndiff; k++) { in.diffusive_species[k] = d.diff_species[k]; in.substeps[k] = d.substeps[k]; }
+    in.num_buffers = d.nbuf;
+    in.stochastic_substep = d.stochastic_substep;
+    in.reaction_substep = d.reaction_substep;
+    in.total_steps = d.total_steps;
+    for (int bi = 0; bi < m.num_boundaries; bi++) in.num_channels[bi] = hr.boundary_nch[bi];
+    RealCtl& c = ctl[r];
+    memset(&c, 0, sizeof c);
+    c.last_closed = -1.0;
+    c.stopped = d.total_steps <= 0 ? 1 : 0;
+  }
+  h->nch = (int)states0.size();
+  // -- flux rows: group pair sides by (realisation, species, voxel), pair order kept --
+  struct Side { int r, s; long long v; int pair; float sign; int owner; };
+  std::vector<Side> sides;
+  for (int i = 0; i < (int)pairs.size(); i++) {
+    const FluxPair& p = pairs[i];
+    sides.push_back({p.r, p.species, p.v1, i, 1.f, p.channel >= 0 ? 1 : 0});
+    if (p.inner) sides.push_back({p.r, p.species, p.v0, i, -1.f, 0});
+  }
+  std::stable_sort(sides.begin(), sides.end(), [](const Side& a, const Side& b) {
+    if (a.r != b.r) return a.r < b.r;
+    if (a.s != b.s) return a.s < b.s;
+    if (a.v != b.v) return a.v < b.v;
+    return a.pair < b.pair;
+  });
+  std::vector<FluxRow> rows;
+  std::vector<FluxEntry> entries;
+  for (size_t i = 0; i < sides.size();) {
+    size_t j = i;
+    FluxRow row;
+    memset(&row, 0, sizeof row);
+    row.r = sides[i].r; row.species = sides[i].s; row.v = sides[i].v;
+    row.begin = (int)entries.size();
+    while (j < sides.size() && sides[j].r == row.r && sides[j].s == row.species && sides[j].v == row.v) {
+      FluxEntry en;
+      en.pair = sides[j].pair; en.sign = sides[j].sign; en.owner = sides[j].owner; en.pad = 0;
+      entries.push_back(en);
+      j++;
+    }
+    row.end = (int)entries.size();
+    // a voxel reset by the fixed-value rules after the step keeps its reset value
+    const RealDesc& D = h->real[row.r].desc;
+    const int x = (int)(row.v / D.P), p = (int)(row.v - (long long)x * D.P);
+    const int y = p / D.nz, z = p - y * D.nz;
+    const unsigned char dd = models[row.r].voxels[((size_t)(x / dv[row.r].S) * models[row.r].N[1] + y / dv[row.r].S) * models[row.r].N[2] + z / dv[row.r].S];
+    const bool face = x == 0 || x == D.nx - 1 || y == 0 || y == D.ny - 1 || z == 0 || z == D.nz - 1;
+    row.apply = !((D.fixed_mask[dd] >> row.species) & 1u) && !(D.dirichlet && row.species == 0 && face);
+    rows.push_back(row);
+    i = j;
+  }
+  h->nrows = (int)rows.size();
+  auto upload = [&](void** dst, const void* src, size_t bytes) -> bool {
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
+    if (src) cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    return cudaStreamSynchronize(h->stream) == cudaSuccess;
+  };
+  std::vector<unsigned char> st2(2 * (size_t)std::max(h->nch, 1), 0);
+  std::copy(states0.begin(), states0.end(), st2.begin());
+  std::vector<RealDesc> descs(n);
+  for (int r = 0; r < n; r++) descs[r] = h->real[r].desc;
+  bool ok = upload((void**)&h->d_rows, rows.empty() ? nullptr : rows.data(), rows.size() * sizeof(FluxRow)) &&
+            upload((void**)&h->d_entries, entries.empty() ? nullptr : entries.data(), entries.size() * sizeof(FluxEntry)) &&
+            upload((void**)&h->d_pairs, pairs.empty() ? nullptr : pairs.data(), pairs.size() * sizeof(FluxPair)) &&
+            upload((void**)&h->d_params, params.empty() ? nullptr : params.data(), params.size() * sizeof(FluxParams)) &&
+            upload((void**)&h->d_states, st2.data(), st2.size());
+  if (!ok) { csp_destroy(h); return fail(nullptr, CSP_ENOMEM, "device allocation of flux tables failed"); }
+  if ((e = cudaMemcpyAsync(h->d_desc, descs.data(), n * sizeof(RealDesc), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(h->d_ctl, ctl.data(), n * sizeof(RealCtl), cudaMemcpyHostToDevice, h->stream)) != cudaSuccess) {
+    csp_destroy(h);
+    return fail(nullptr, CSP_ECUDA, "descriptor upload: %s", cudaGetErrorString(e));
+  }
+  const int red_blocks = 296;
+  if (cudaMalloc(&h->d_red, red_blocks * 3 * ND * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&h->d_red_out, 3 * ND * sizeof(double)) != cudaSuccess) {
+    csp_destroy(h);
+    return fail(nullptr, CSP_ENOMEM, "device allocation of reduction buffers failed");
+  }
+  h->plan = staged_plan(descs);
+  if (staged_prepare(h->plan) != cudaSuccess) h->kernel = 1;
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) { csp_destroy(h); return fail(nullptr, CSP_ECUDA, "setup: %s", cudaGetErrorString(e)); }
+  *out = h;
+  return CSP_OK;
+}
+
+static cudaError_t launch_step(csp_handle* h) {
+  if (h->kernel == 1) {
+    dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)h->n);
+    k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_err);
+  } else {
+    staged_launch(h->plan, h->d_desc, h->d_ctl, h->d_err, h->stream);
+  }
+  const int blocks = std::max(1, (h->nrows + 255) / 256);
+  k_boundaries<<<blocks, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, h->nrows, h->d_entries, h->d_pairs,
+                                              h->d_params, h->d_states, std::max(h->nch, 1), h->n,
+                                              h->d_ticket);
+  return cudaGetLastError();
+}
+
+static int ensure_graph(csp_handle* h) {
+  if (h->graph && h->graph_kernel == h->kernel) return CSP_OK;
+  if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+  cudaGraph_t g;
+  CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < STEPS_PER_GRAPH; i++) {
+    cudaError_t e = launch_step(h);
+    if (e != cudaSuccess) {
+      cudaStreamEndCapture(h->stream, &g);
+      return fail(h, CSP_ECUDA, "capture: %s", cudaGetErrorString(e));
+    }
+  }
+  CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { h->graph = nullptr; return fail(h, CSP_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+  h->graph_kernel = h->kernel;
+  return CSP_OK;
+}
+
+extern "C" int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags) {
+  if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
+  int rc = ensure_graph(h);
+  if (rc) return rc;
+  CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
+  int64_t left = nsteps;
+  while (left >= STEPS_PER_GRAPH) {
+    CUDA_TRY(h, cudaGraphLaunch(h->graph, h->stream));
+    left -= STEPS_PER_GRAPH;
+  }
+  while (left-- > 0) CUDA_TRY(h, launch_step(h));
+  CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+  int err = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<RealCtl> ctl(h->n);
+  CUDA_TRY(h, cudaMemcpyAsync(ctl.data(), h->d_ctl, h->n * sizeof(RealCtl), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  for (int r = 0; r < h->n; r++) {
+    h->real[r].info.step = ctl[r].step;
+    h->real[r].info.stopped = ctl[r].stopped;
+    if (stop_flags) stop_flags[r] = ctl[r].stopped;
+  }
+  if (err) return fail(h, CSP_EDEVICE, "device error word %d (%s)", err,
+                       (err & ERR_TIMEOUT) ? "bounded wait timed out" : "index out of bounds");
+  return CSP_OK;
+}
+
+static int read_ctl(csp_handle* h, int r, RealCtl& c) {
+  CUDA_TRY(h, cudaMemcpyAsync(&c, h->d_ctl + r, sizeof(RealCtl), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+extern "C" int csp_get_info(const csp_handle* h, int32_t r, csp_info* info) {
+  if (!h || !info) return CSP_EINVAL;
+  if (r < 0 || r >= h->n) return CSP_ERANGE;
+  *info = h->real[r].info;
+  return CSP_OK;
+}
+
+extern "C" int csp_upload_state(csp_handle* h, int32_t r, const double* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  RealCtl c;
+  int rc = read_ctl(h, r, c);
+  if (rc) return rc;
+  const RealDesc& D = h->real[r].desc;
+  const unsigned cur = c.cur_mask[c.step & 1];
+  const size_t nvox = (size_t)D.nx * D.plane;
+  std::vector<float> tmp(nvox);
+  for (int s = 0; s < D.ns; s++) {
+    for (size_t i = 0; i < nvox; i++) tmp[i] = (float)u[(size_t)s * nvox + i];
+    CUDA_TRY(h, cudaMemcpy2DAsync(D.u[(cur >> s) & 1u][s], (size_t)D.P * sizeof(float), tmp.data(),
+                                  (size_t)D.plane * sizeof(float), (size_t)D.plane * sizeof(float), D.nx,
+                                  cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  return CSP_OK;
+}
+
+extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  RealCtl c;
+  int rc = read_ctl(h, r, c);
+  if (rc) return rc;
+  const RealDesc& D = h->real[r].desc;
+  const unsigned cur = c.cur_mask[c.step & 1];
+  const size_t nvox = (size_t)D.nx * D.plane;
+  std::vector<float> tmp(nvox);
+  for (int s = 0; s < D.ns; s++) {
+    CUDA_TRY(h, cudaMemcpy2DAsync(tmp.data(), (size_t)D.plane * sizeof(float), D.u[(cur >> s) & 1u][s],
+                                  (size_t)D.P * sizeof(float), (size_t)D.plane * sizeof(float), D.nx,
+                                  cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (size_t i = 0; i < nvox; i++) u[(size_t)s * nvox + i] = (double)tmp[i];
+  }
+  return CSP_OK;
+}
+
+extern "C" int csp_get_channel_states(const csp_handle* hc, int32_t r, int32_t boundary, int32_t* states) {
+  csp_handle* h = const_cast<csp_handle*>(hc);
+  if (!h || !states) return CSP_EINVAL;
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  const HostReal& hr = h->real[r];
+  if (boundary < 0 || boundary >= (int)hr.boundary_channel_base.size() || hr.boundary_channel_base[boundary] < 0)
+    return fail(h, CSP_ERANGE, "boundary %d is not a discrete boundary", boundary);
+  RealCtl c;
+  int rc = read_ctl(h, r, c);
+  if (rc) return rc;
+  const int nchb = hr.boundary_nch[boundary];
+  std::vector<unsigned char> tmp(nchb);
+  CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->d_states + (c.step & 1) * (size_t)std::max(h->nch, 1) + hr.boundary_channel_base[boundary],
+                              nchb, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int i = 0; i < nchb; i++) states[i] = tmp[i];
+  return CSP_OK;
+}
+
+extern "C" int csp_set_channel_states(csp_handle* h, int32_t r, int32_t boundary, const int32_t* states) {
+  if (!h || !states) return CSP_EINVAL;
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  const HostReal& hr = h->real[r];
+  if (boundary < 0 || boundary >= (int)hr.boundary_channel_base.size() || hr.boundary_channel_base[boundary] < 0)
+    return fail(h, CSP_ERANGE, "boundary %d is not a discrete boundary", boundary);
+  RealCtl c;
+  int rc = read_ctl(h, r, c);
+  if (rc) return rc;
+  const int nchb = hr.boundary_nch[boundary];
+  std::vector<unsigned char> tmp(nchb);
+  for (int i = 0; i < nchb; i++) tmp[i] = (unsigned char)(states[i] ? 1 : 0);
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_states + (c.step & 1) * (size_t)std::max(h->nch, 1) + hr.boundary_channel_base[boundary],
+                              tmp.data(), nchb, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+extern "C" int csp_reduce_outputs(csp_handle* h, int32_t r, double* min_values, double* max_values,
+                                  double* total_values, int32_t* openness) {
+  if (!h) return CSP_EINVAL;
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  const HostReal& hr = h->real[r];
+  const RealDesc& D = hr.desc;
+  const int nblk = 296;
+  double out[3 * ND];
+  for (int s = 0; s < D.ns; s++) {
+    k_reduce_partial<<<nblk, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, r, s, h->d_red);
+    k_reduce_final<<<1, 32, 0, h->stream>>>(h->d_red, nblk, hr.dV, h->d_red_out);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(out, h->d_red_out, sizeof out, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    for (int d = 0; d < hr.nd; d++) {
+      if (min_values) min_values[d * D.ns + s] = out[0 * ND + d];
+      if (max_values) max_values[d * D.ns + s] = out[1 * ND + d];
+      if (total_values) total_values[d * D.ns + s] = out[2 * ND + d];
+    }
+  }
+  if (openness) {
+    int off = 0;
+    for (size_t b = 0; b < hr.boundary_channel_base.size(); b++) {
+      if (hr.boundary_channel_base[b] < 0) continue;
+      int rc = csp_get_channel_states(h, r, (int)b, openness + off);
+      if (rc) return rc;
+      off += hr.boundary_nch[b];
+    }
+  }
+  return CSP_OK;
+}
+
+extern "C" int csp_status(const csp_handle* h, char* msg, size_t n) {
+  const char* m = h ? h->msg.c_str() : g_create_error;
+  if (msg && n) snprintf(msg, n, "%s", m);
+  return CSP_OK;
+}
+
+extern "C" int csp_get_stream(const csp_handle* h, void** stream) {
+  if (!h || !stream) return CSP_EINVAL;
+  *stream = (void*)h->stream;
+  return CSP_OK;
+}
+
+extern "C" int csp_last_advance_ms(const csp_handle* h, float* ms) {
+  if (!h || !ms) return CSP_EINVAL;
+  *ms = h->last_ms;
+  return CSP_OK;
+}
+
+extern "C" int csp_set_kernel(csp_handle* h, int32_t which) {
+  if (!h || which < 0 || which > 1) return CSP_EINVAL;
+  if (which == 0 && !h->plan.ok) return fail(h, CSP_ENOTSUP, "staged kernel unavailable for this batch");
+  h->kernel = which;
+  return CSP_OK;
+}
+
+extern "C" void csp_destroy(csp_handle* h) {
+  if (!h) return;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  staged_release(h->plan);
+  cudaFree(h->d_fields); cudaFree(h->d_dom); cudaFree(h->d_desc); cudaFree(h->d_ctl);
+  cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
+  cudaFree(h->d_states); cudaFree(h->d_ticket); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}

@@ -1,0 +1,228 @@
+/*
+ * csparks.h -- C ABI of the B200 calcium_sparks time step (libcsparks_cuda.so).
+ *
+ * The reference program (ComputationalPhysiology/hpc-ca-phospattern, fvm_mpi/) advances
+ * its reaction-diffusion state through the host-memory FP64 kernels declared in
+ * fvm_mpi/src/kernel.h:2-18 and the step drivers of fvm_mpi/src/species.c.  This
+ * library replaces that step with sm_100a CUDA kernels: the whole domain (or an
+ * ensemble of independent realisations) lives in HBM, and one call advances it by any
+ * number of steps.  The host owns every input array; the library owns device memory.
+ *
+ * Conventions
+ *   - every int-returning call returns 0 (CSP_OK) or a negative CSP_E* code; nothing
+ *     aborts the process.  csp_status() gives a message for the last error.
+ *   - calls on one handle are ordered on one internal CUDA stream; the handle is not
+ *     thread safe.
+ *   - fields are C order [x][y][z] with z fastest, index x*ny*nz + y*nz + z
+ *     (species.c:1513), one array per species, species-major ([species][x][y][z]).
+ *   - units: concentration uM, time ms, length nm, sigma nm^2/ms.
+ */
+#ifndef CSPARKS_H
+#define CSPARKS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CSP_MAX_DOMAINS    5   /* max_num_domains, kernel_generic.cpp:11 */
+#define CSP_MAX_SPECIES    8
+#define CSP_MAX_BUFFERS    8
+#define CSP_MAX_BOUNDARIES 8
+#define CSP_MAX_FIXED      8
+#define CSP_NAME_LEN       20  /* MAX_SPECIES_NAME, types.h:10 */
+
+enum {
+  CSP_OK = 0,
+  CSP_EINVAL = -1,      /* bad argument / inconsistent model */
+  CSP_ENOMEM = -2,      /* device or host allocation failed */
+  CSP_ECUDA = -3,       /* CUDA runtime error */
+  CSP_ERANGE = -4,      /* index out of range (realisation, channel, -O index) */
+  CSP_EDEVICE = -5,     /* device-side error word set (bounds / timeout) */
+  CSP_ENOTSUP = -6      /* a model feature this build does not support */
+};
+
+enum { CSP_BOUNDARY_DENSITY = 0, CSP_BOUNDARY_DISCRETE = 1 };  /* geometry.h:46 */
+
+/* One boundary of the geometry file: /boundaries/<name>, uint16 [n][6] voxel pairs
+ * (x0,y0,z0,x1,y1,z1) in geometry voxels (geometry.c:239-259, 576-620). */
+typedef struct csp_boundary {
+  char name[CSP_NAME_LEN];
+  int32_t type;                 /* CSP_BOUNDARY_DENSITY | CSP_BOUNDARY_DISCRETE */
+  int32_t num_pairs;
+  const uint16_t* pairs;        /* [num_pairs][6] */
+} csp_boundary;
+
+/* Per-domain part of the species file, group /<domain_name> (species.c:171-241). */
+typedef struct csp_domain_species {
+  int32_t num_diffusive;
+  uint8_t diffusive[CSP_MAX_SPECIES];   /* species indices */
+  double sigma[CSP_MAX_SPECIES];        /* sigma[k] belongs to diffusive[k] */
+  double init[CSP_MAX_SPECIES];         /* initial value of every species */
+  int32_t num_buffers;
+  double k_on[CSP_MAX_BUFFERS];
+  double k_off[CSP_MAX_BUFFERS];
+  double tot[CSP_MAX_BUFFERS];
+  uint8_t bsp0[CSP_MAX_BUFFERS];        /* bound buffer species (attr "species"[0]) */
+  uint8_t bsp1[CSP_MAX_BUFFERS];        /* free ligand species (attr "species"[1]) */
+} csp_domain_species;
+
+/* RyR / pRyR group of the species file (boundaryfluxes.c:421-503). */
+typedef struct csp_ryr_params {
+  double Kd_open, k_min_open, k_max_open, n_open;
+  double Kd_close, k_min_close, k_max_close, n_close;
+  double i_unitary;                     /* pA */
+  char boundary[CSP_NAME_LEN];
+  char species[CSP_NAME_LEN];
+} csp_ryr_params;
+
+/* SERCA group of the species file (boundaryfluxes.c:506-527).  The reference reads the
+ * SERCA species name from the /ryr group (boundaryfluxes.c:511); loaders fill
+ * `species` the same way. */
+typedef struct csp_serca_params {
+  double v_cyt_to_A_sr, density, scale;
+  char boundary[CSP_NAME_LEN];
+  char species[CSP_NAME_LEN];
+} csp_serca_params;
+
+/* Everything the geometry file and the species file of one realisation hold. */
+typedef struct csp_model {
+  /* geometry file (geometry.c:96-344) */
+  double h_geom;                        /* root attr "h" */
+  double global_size[3];                /* root attr "global_size" */
+  int32_t N[3];                         /* shape of /domains/voxels */
+  int32_t num_domains;
+  char domain_names[CSP_MAX_DOMAINS][CSP_NAME_LEN];
+  uint8_t domain_indices[CSP_MAX_DOMAINS];
+  const uint8_t* voxels;                /* [N0][N1][N2] domain ids */
+  uint8_t domain_connections[CSP_MAX_DOMAINS * CSP_MAX_DOMAINS];  /* [num][num] */
+  int32_t num_boundaries;
+  csp_boundary boundaries[CSP_MAX_BOUNDARIES];
+  /* species file (species.c:103-258, boundaryfluxes.c:377-527) */
+  int32_t num_species;
+  char species_names[CSP_MAX_SPECIES][CSP_NAME_LEN];
+  csp_domain_species domain[CSP_MAX_DOMAINS];
+  int32_t num_fixed_domain_species;
+  uint8_t fixed_domain_species[2 * CSP_MAX_FIXED];  /* (domain, species) pairs */
+  uint8_t use_ryr, use_p_ryr, use_serca;
+  csp_ryr_params ryr, p_ryr;
+  csp_serca_params serca;
+  double convolution_constants[3];
+} csp_model;
+
+/* One "-O name i j ..." list (options.c:221-311). */
+typedef struct csp_open_list {
+  char name[CSP_NAME_LEN];
+  int32_t count;
+  const int32_t* indices;
+} csp_open_list;
+
+/* One "-C name t" pair (options.c:161-214). */
+typedef struct csp_t_close {
+  char name[CSP_NAME_LEN];
+  double time;
+} csp_t_close;
+
+/* The command-line arguments that reach the time step (options.h:47-137,
+ * defaults options.c:502-542). */
+typedef struct csp_options {
+  double h;                 /* -h requested resolution, nm (default 6) */
+  double dt;                /* -d; <= 0 selects 0.95*h^2/(6*sigma_max) */
+  double tstop;             /* -t, ms (default 10) */
+  double dt_save;           /* -o, ms (default 0.5) */
+  double dt_update_react;   /* -T (default -1) */
+  double dt_update_stoch;   /* -D (default -1) */
+  double tabort;            /* -X value; 0 = inactive */
+  int32_t force_dirichlet;  /* -f */
+  int32_t seed_given;       /* -S given */
+  uint64_t seed;            /* -S; realisation r draws from Philox key (seed, r) */
+  int32_t num_open_lists;
+  csp_open_list open[CSP_MAX_BOUNDARIES];
+  int32_t num_t_close;
+  csp_t_close t_close[CSP_MAX_BOUNDARIES];
+} csp_options;
+
+/* Fills `o` with the reference defaults (options.c:502-542). */
+void csp_options_default(csp_options* o);
+
+/* Derived per-realisation constants (species.c:265-294, 784-787). */
+typedef struct csp_info {
+  int32_t n[3];             /* species voxels per axis */
+  int32_t subdivisions;
+  double h;                 /* species resolution, nm */
+  double dt;                /* ms */
+  int32_t num_species;
+  int32_t num_diffusive;
+  int32_t diffusive_species[CSP_MAX_SPECIES];
+  int32_t substeps[CSP_MAX_SPECIES];
+  int32_t num_buffers;      /* num_all_buffers */
+  int32_t stochastic_substep;
+  int32_t reaction_substep;
+  int64_t total_steps;      /* iterations of `for (t=0; t<tstop; t+=dt)` */
+  int64_t step;             /* steps already taken */
+  int32_t num_channels[CSP_MAX_BOUNDARIES];   /* discrete boundaries, in boundary order */
+  int32_t stopped;          /* 1 once the -X rule or total_steps ended the run */
+} csp_info;
+
+typedef struct csp_handle csp_handle;
+
+/* Build device state for n independent realisations (models[r], options[r]) and set
+ * the initial state exactly as the reference does before its time loop
+ * (calcium_sparks.c:150-178: Species_init_values, channel init, du := u).
+ * Replaces Species_construct + BoundaryFluxes_construct + Species_init_values +
+ * BoundaryFluxes_init_stochastic_boundaries + Species_init_du
+ * (species.c:95, 887, 22; boundaryfluxes.c:361, 544). */
+int csp_create(const csp_model* models, const csp_options* options, int32_t n,
+               csp_handle** out);
+
+/* Derived constants and progress of realisation r. */
+int csp_get_info(const csp_handle* h, int32_t r, csp_info* info);
+
+/* Overwrite / read the fields of realisation r: u[num_species][nx][ny][nz], FP64 on the
+ * host, FP32 on the device.  (The reference keeps these fields in Species_t::u1,
+ * species.h:52.) */
+int csp_upload_state(csp_handle* h, int32_t r, const double* u);
+int csp_download_state(csp_handle* h, int32_t r, double* u);
+
+/* Advance every still-running realisation by up to nsteps steps: diffusion, channel
+ * gating, boundary fluxes, reactions, apply and fixed values, in the order of the
+ * reference loop body calcium_sparks.c:190-228 (Species_step_diffusion species.c:1501,
+ * Species_evaluate_stochastic_events :1910, Species_step_boundary_fluxes :1704,
+ * Species_step_reaction :1653, Species_apply_du :1080, Species_apply_fixed_values
+ * :1066).  A realisation stops at its total_steps.  stop_flags (nullable, n entries)
+ * receives 1 for stopped realisations. */
+int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags);
+
+/* Per (domain, species) min / max / sum(u*dV) in FP64, and the channel openness of
+ * every discrete boundary in boundary order (Species_output_scalar_data,
+ * species.c:2785-2880).  min/max/total: [num_domains][num_species]; openness: all
+ * channels of all discrete boundaries, concatenated. */
+int csp_reduce_outputs(csp_handle* h, int32_t r, double* min_values, double* max_values,
+                       double* total_values, int32_t* openness);
+
+/* Channel states (0 closed / 1 open) of discrete boundary `boundary` (index into
+ * model.boundaries) of realisation r (ModelStates::s0, basefluxinfo.h:9-16). */
+int csp_get_channel_states(const csp_handle* h, int32_t r, int32_t boundary, int32_t* states);
+int csp_set_channel_states(csp_handle* h, int32_t r, int32_t boundary, const int32_t* states);
+
+/* Message of the last error and the device error word (bounds / timeout). */
+int csp_status(const csp_handle* h, char* msg, size_t n);
+
+/* The CUDA stream (cudaStream_t) every call of this handle is ordered on. */
+int csp_get_stream(const csp_handle* h, void** stream);
+
+/* Device time in ms of the last csp_advance call (CUDA events on the handle stream). */
+int csp_last_advance_ms(const csp_handle* h, float* ms);
+
+/* Select the voxel kernel: 0 = staged (TMA bulk copies into shared memory, default),
+ * 1 = direct (one thread per voxel, global loads).  Both give bitwise equal results. */
+int csp_set_kernel(csp_handle* h, int32_t which);
+
+void csp_destroy(csp_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSPARKS_H */

@@ -1,0 +1,235 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
+
+Every case runs the same model and options through libcsparks_cuda.so and through the
+oracle, and compares every species field (per-species relative error <= 1e-4, the FP32
+accuracy bar), the channel states (bit-exact) and the output reductions.
+"""
+import numpy as np
+import pytest
+
+from parity import RTOL, assert_close, species_rel_err
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = [0, 1]   # 0 = TMA-staged, 1 = direct
+
+
+def run_pair(pkg, oracle_mod, spec, opts, nsteps, kernel=1, chunks=1):
+    sim = pkg.Simulation(spec, opts)
+    sim.set_kernel(kernel)
+    orc = oracle_mod.Oracle(spec, opts)
+    per = nsteps // chunks
+    for _ in range(chunks):
+        sim.advance(per)
+        orc.step(per)
+    return sim, orc
+
+
+def discrete_boundaries(spec):
+    return [i for i, b in enumerate(spec["boundaries"]) if b["type"] == "discrete"]
+
+
+def check_channels(sim, orc, spec, r=0):
+    for b in discrete_boundaries(spec):
+        np.testing.assert_array_equal(sim.channels(b, r), orc.channels(b))
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_forced_channels_parity(pkg, oracle_mod, synth, kernel):
+    spec = synth.tiny((12, 12, 16))
+    opts = dict(h=6.0, tstop=5.0, seed=1, open_states={"ryr": [0, 3], "p_ryr": [1]},
+                t_close={"ryr": 0.004, "p_ryr": 0.006})
+    sim, orc = run_pair(pkg, oracle_mod, spec, opts, 400, kernel, chunks=4)
+    assert sim.info().step == orc.info().step == 400
+    assert_close(sim.state(), orc.state(), what="forced")
+    check_channels(sim, orc, spec)
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_stochastic_parity(pkg, oracle_mod, synth, kernel):
+    """Same Philox draws on both sides: identical channel trajectories."""
+    spec = synth.tiny((12, 12, 16))
+    opts = dict(h=6.0, tstop=5.0, seed=7, open_states={"ryr": [0]})
+    sim = pkg.Simulation(spec, opts)
+    sim.set_kernel(kernel)
+    orc = oracle_mod.Oracle(spec, opts)
+    for _ in range(10):
+        sim.advance(50)
+        orc.step(50)
+        check_channels(sim, orc, spec)
+    assert_close(sim.state(), orc.state(), what="stochastic")
+
+
+def test_kernels_bitwise_equal(pkg, synth):
+    spec = synth.tiny((20, 18, 24))
+    opts = dict(h=6.0, tstop=5.0, seed=3, open_states={"ryr": [0, 1, 2]})
+    a = pkg.Simulation(spec, opts)
+    b = pkg.Simulation(spec, opts)
+    a.set_kernel(0)
+    b.set_kernel(1)
+    a.advance(137)
+    b.advance(137)
+    np.testing.assert_array_equal(a.state(), b.state())
+
+
+def test_batched_equals_single(pkg, oracle_mod, synth):
+    rng = np.random.default_rng(5)
+    specs = []
+    for k, shape in enumerate([(12, 12, 16), (16, 10, 12), (10, 14, 20)]):
+        specs.append(synth.tiny(shape, pryr=(k != 1)))
+    opts = [dict(h=6.0, tstop=5.0, seed=11, open_states={"ryr": [k]}) for k in range(3)]
+    batch = pkg.Simulation(specs, opts)
+    batch.advance(120)
+    for r in range(3):
+        single = pkg.Simulation(specs[r], opts[r])
+        single.advance(120)
+        orc = oracle_mod.Oracle(specs[r], opts[r], realisation=r)
+        orc.step(120)
+        # realisation r of the batch draws the Philox stream of index r
+        np.testing.assert_array_equal(batch.channels(0, r), orc.channels(0))
+        assert_close(batch.state(r), orc.state(), what=f"batch r={r}")
+        if r == 0:
+            np.testing.assert_array_equal(batch.state(0), single.state(0))
+    _ = rng
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_subdivisions(pkg, oracle_mod, synth, kernel):
+    """Geometry at 12 nm simulated at 6 nm: every geometry voxel becomes 2^3 voxels;
+    density pairs expand to 4 pairs, discrete ones sit at the sub-voxel centre."""
+    spec = synth.tiny((8, 8, 10))
+    spec["h"] = 12.0
+    opts = dict(h=6.0, tstop=5.0, seed=2, open_states={"ryr": [0, 2], "p_ryr": [0]})
+    sim, orc = run_pair(pkg, oracle_mod, spec, opts, 200, kernel)
+    assert sim.info().subdivisions == 2
+    assert_close(sim.state(), orc.state(), what="subdivisions")
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_dirichlet_fixed_and_substeps(pkg, oracle_mod, synth, kernel):
+    spec = synth.tiny((12, 12, 16))
+    spec["fixed_domain_species"] = [(3, 0)]          # nsr Ca fixed
+    dt = 0.95 * 36 / (6 * 220000.0)
+    opts = dict(h=6.0, tstop=5.0, seed=4, force_dirichlet=True, dt_update_react=3.5 * dt,
+                dt_update_stoch=2 * dt, open_states={"ryr": [1, 4]}, t_close={"ryr": 0.003})
+    sim, orc = run_pair(pkg, oracle_mod, spec, opts, 300, kernel, chunks=3)
+    inf = sim.info()
+    assert inf.reaction_substep == 3 and inf.stochastic_substep == 2
+    assert_close(sim.state(), orc.state(), what="dirichlet/fixed/substeps")
+    check_channels(sim, orc, spec)
+
+
+def test_forced_dt_and_odd_sizes(pkg, oracle_mod, synth):
+    """-d forcing the time step, a grid with planes that are not multiples of 4 and a
+    z extent of 9 (below the reference's vector width + 1)."""
+    spec = synth.tiny((9, 11, 9), serca=False)
+    opts = dict(h=6.0, dt=2e-5, tstop=1.0, seed=9, open_states={"ryr": [4]})
+    sim, orc = run_pair(pkg, oracle_mod, spec, opts, 250, 1)
+    assert abs(sim.info().dt - 2e-5) < 1e-20
+    assert_close(sim.state(), orc.state(), what="odd sizes")
+    sim0, _ = run_pair(pkg, oracle_mod, spec, opts, 250, 0)
+    np.testing.assert_array_equal(sim0.state(), sim.state())
+
+
+def test_outputs_match_oracle(pkg, oracle_mod, synth):
+    spec = synth.tiny((12, 12, 16))
+    opts = dict(h=6.0, tstop=5.0, seed=1, open_states={"ryr": [0]})
+    sim, orc = run_pair(pkg, oracle_mod, spec, opts, 100)
+    mn, mx, tot, op = sim.outputs()
+    omn, omx, otot = orc.outputs()
+    present = [d for d in range(len(spec["domains"])) if np.any(spec["voxels"] == d)]
+    for d in present:
+        np.testing.assert_allclose(mn[d], omn[d], rtol=RTOL, atol=1e-9)
+        np.testing.assert_allclose(mx[d], omx[d], rtol=RTOL, atol=1e-9)
+        np.testing.assert_allclose(tot[d], otot[d], rtol=RTOL, atol=1e-6)
+    # an empty domain keeps the reference's FLT_MAX / FLT_MIN initial values
+    tt = spec["domains"].index("tt")
+    assert mn[tt, 0] == np.float32(3.4028235e38) and mx[tt, 0] == np.float32(1.1754944e-38)
+    assert list(op) == list(np.concatenate([orc.channels(b) for b in discrete_boundaries(spec)]))
+
+
+def test_abort_rule(pkg, oracle_mod, synth):
+    """All channels forced closed at t_close; the run stops tabort ms later."""
+    spec = synth.tiny((12, 12, 16))
+    dt = 0.95 * 36 / (6 * 220000.0)
+    opts = dict(h=6.0, tstop=5.0, seed=1, open_states={"ryr": [0], "p_ryr": []},
+                t_close={"ryr": 50 * dt, "p_ryr": 50 * dt}, tabort=30 * dt)
+    sim = pkg.Simulation(spec, opts)
+    orc = oracle_mod.Oracle(spec, opts)
+    flags = sim.advance(200)
+    orc.step(200)
+    assert flags[0] == 1
+    assert sim.info().step == orc.info().step
+    assert 70 < sim.info().step < 90
+    assert_close(sim.state(), orc.state(), what="abort")
+
+
+def test_state_roundtrip_and_channels(pkg, synth):
+    spec = synth.tiny((12, 12, 16))
+    sim = pkg.Simulation(spec, dict(h=6.0, tstop=1.0, seed=1))
+    u = sim.state()
+    rng = np.random.default_rng(0)
+    v = u * (1 + 0.01 * rng.standard_normal(u.shape))
+    sim.set_state(v)
+    np.testing.assert_array_equal(sim.state(), v.astype(np.float32).astype(np.float64))
+    st = np.array([1, 0, 1, 1, 0, 0, 1], dtype=np.int32)
+    sim.set_channels(0, st)
+    np.testing.assert_array_equal(sim.channels(0), st)
+
+
+def test_errors_are_codes_not_aborts(pkg, synth):
+    spec = synth.tiny((12, 12, 16))
+    with pytest.raises(pkg.CspError) as e:
+        pkg.Simulation(spec, dict(h=6.0, open_states={"ryr": [99]}))
+    assert e.value.code == -4
+    import copy
+    bad = copy.deepcopy(spec)
+    bad["domain_species"]["cyt"]["buffers"][0]["species"] = [7, 0]   # no species 7
+    with pytest.raises(pkg.CspError) as e:
+        pkg.Simulation(bad, dict(h=6.0))
+    assert e.value.code == -1
+    bad = copy.deepcopy(spec)
+    bad["voxels"] = bad["voxels"].copy()
+    bad["voxels"][0, 0, 0] = 6                                        # domain id >= num_domains
+    with pytest.raises(pkg.CspError) as e:
+        pkg.Simulation(bad, dict(h=6.0))
+    assert e.value.code == -1
+    sim = pkg.Simulation(spec, dict(h=6.0, tstop=1.0))
+    with pytest.raises(pkg.CspError):
+        sim.state(3)
+    with pytest.raises(pkg.CspError):
+        sim.channels(2)   # serca is a density boundary
+
+
+def test_equilibrium_is_steady_full_size(pkg, synth):
+    """Config-3-sized realisation with every channel closed and no SERCA: the initial
+    state is the buffer equilibrium, so it must stay (up to FP32 rounding)."""
+    spec = synth.spark_model((100, 100, 50), serca=False)
+    sim = pkg.Simulation(spec, dict(h=6.0, tstop=10.0, seed=1, open_states={"ryr": []},
+                                    t_close={"ryr": 1e-9}))
+    u0 = sim.state()
+    sim.advance(64)
+    u1 = sim.state()
+    err = species_rel_err(u1, u0)
+    assert np.all(err < 1e-5), err
+
+
+def test_mass_conservation_full_size(pkg, synth):
+    """Closed system (no SERCA, channels open only between jSR and cleft): total calcium,
+    free plus bound, is conserved; the FP64 sums must agree to FP32 precision."""
+    spec = synth.spark_model((100, 100, 50), serca=False)
+    sim = pkg.Simulation(spec, dict(h=6.0, tstop=10.0, seed=1, open_states={"ryr": list(range(25))}))
+
+    def total_ca():
+        _, _, tot, _ = sim.outputs()
+        return tot.sum()  # Ca + every bound form: each buffer binds one Ca
+
+    t0 = total_ca()
+    sim.advance(200)
+    t1 = total_ca()
+    assert abs(t1 - t0) / t0 < 2e-5, (t0, t1)
+    u = sim.state()
+    assert np.all(np.isfinite(u))
+    # the cleft under open channels is far above rest
+    lay = spec["layout"]
+    assert u[0, 50, 50, lay["cleft_z"][1] - 1] > 10.0
