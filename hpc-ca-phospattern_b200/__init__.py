@@ -102,6 +102,12 @@ class Simulation:
         self._check(self.lib.csp_advance(self.h, int(nsteps), flags.ctypes.data_as(C.POINTER(C.c_int32))))
         return flags
 
+    def profile(self, nsteps):
+        """Advance nsteps with per-kernel CUDA events: (voxel_ms, boundary_ms) summed."""
+        a, b = C.c_float(), C.c_float()
+        self._check(self.lib.csp_profile_advance(self.h, int(nsteps), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def last_ms(self):
         ms = C.c_float()
         self._check(self.lib.csp_last_advance_ms(self.h, C.byref(ms)))

@@ -232,6 +232,7 @@ def declare(lib):
         "csp_get_stream": (C.c_int, [h, P(C.c_void_p)]),
         "csp_last_advance_ms": (C.c_int, [h, P(C.c_float)]),
         "csp_set_kernel": (C.c_int, [h, C.c_int32]),
+        "csp_profile_advance": (C.c_int, [h, C.c_int64, P(C.c_float), P(C.c_float)]),
         "csp_destroy": (None, [h]),
     }
     for name, (res, args) in sig.items():

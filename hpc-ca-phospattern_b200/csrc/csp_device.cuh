@@ -134,41 +134,6 @@ __device__ __forceinline__ void addto(float (&a)[N], int i, float v) {
     if (i == s) a[s] += v;
 }
 
-// Masked 7-point update of one species at one voxel (species.c:1572-1611 and the
-// face terms of species.c:1282-1498): out = u + sum_n c[d][d_n]*(u_n - u), with the
-// neighbours outside the box dropped (no flux).  Neighbour order: z-, z+, y-, y+, x-, x+.
-// valid bit k = neighbour k inside the box.
-__device__ __forceinline__ float stencil7(const float* __restrict__ c, float u, const float (&un)[6],
-                                          const unsigned char (&dn)[6], unsigned valid) {
-  float acc = 0.f;
-#pragma unroll
-  for (int k = 0; k < 6; k++) {
-    float ck = (valid >> k & 1u) ? c[dn[k]] : 0.f;
-    float dk = (valid >> k & 1u) ? (un[k] - u) : 0.f;
-    acc = fmaf(ck, dk, acc);
-  }
-  return u + acc;
-}
-
-// Buffer reactions of one voxel (reaction_SIMD, kernel_generic.cpp:397-509): for each
-// buffer bi of the voxel's domain, J = k_on*(tot-b0)*b1 - k_off*b0 with the values at
-// step start; a species already updated this step accumulates, otherwise it is assigned
-// from its step-start value.
-template <int N>
-__device__ __forceinline__ void react(const RealDesc& D, int d, const float (&val)[N], float (&out)[N],
-                                      unsigned pre) {
-  for (int bi = 0; bi < NB; bi++) {
-    if (bi >= D.nbuf) break;
-    const int t = bi * D.nd + d;
-    const int s0 = D.bsp0[t], s1 = D.bsp1[t];
-    const float b0 = sel(val, s0), b1 = sel(val, s1);
-    const float J = D.kon[t] * (D.tot[t] - b0) * b1 - D.koff[t] * b0;
-    const float dJ = D.dt_r * J;
-    if (pre >> s0 & 1u) addto(out, s0, dJ); else put(out, s0, b0 + dJ);
-    if (pre >> s1 & 1u) addto(out, s1, -dJ); else put(out, s1, b1 - dJ);
-  }
-}
-
 // ---------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) for the channel draws.
 __host__ __device__ inline void philox4x32(const unsigned (&ctr)[4], unsigned k0, unsigned k1, unsigned (&out)[4]) {

@@ -17,12 +17,55 @@ namespace csp {
 // Device error word bits.
 enum : int { ERR_BOUNDS = 1, ERR_TIMEOUT = 2 };
 
+// ---- per-voxel arithmetic, with explicit rounding (no contraction differences between
+// the code paths that share it) ----
+
+// Uniform neighbourhood (all six neighbours in the voxel's domain): the reference's fast
+// path c*(sum_n u_n - 6u) + u (kernel_generic.cpp:529-533) in the form u + c*sum_n(u_n - u);
+// out-of-box neighbours carry u_n = u and add nothing.
+__device__ __forceinline__ float diffuse_uniform(float c, float u, const float (&un)[6]) {
+  float a = __fsub_rn(un[0], u);
+#pragma unroll
+  for (int k = 1; k < 6; k++) a = __fadd_rn(a, __fsub_rn(un[k], u));
+  return __fmaf_rn(c, a, u);
+}
+
+// General neighbourhood: u + sum_n c[d][d_n]*(u_n - u) (species.c:1572-1611, 1282-1498).
+__device__ __forceinline__ float diffuse_general(const float* c, const int (&dn)[6], float u, const float (&un)[6]) {
+  float a = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; k++) a = __fmaf_rn(c[dn[k]], __fsub_rn(un[k], u), a);
+  return __fadd_rn(u, a);
+}
+
+// dt_r * J for one buffer, J = k_on*(tot-b)*ca - k_off*b (kernel_generic.cpp:495-507).
+__device__ __forceinline__ float buffer_dj(float kon, float koff, float tot, float dt_r, float b, float ca) {
+  const float J = __fsub_rn(__fmul_rn(__fmul_rn(kon, __fsub_rn(tot, b)), ca), __fmul_rn(koff, b));
+  return __fmul_rn(dt_r, J);
+}
+
+// General buffer reactions: the reference's assign-or-accumulate rule, per buffer in
+// buffer order (species.c:1653-1702, kernel_generic.cpp:397-509).
+template <int N>
+__device__ __forceinline__ void react_general(const RealDesc& D, int d, const float (&val)[N], float (&out)[N],
+                                              unsigned pre) {
+  for (int bi = 0; bi < NB; bi++) {
+    if (bi >= D.nbuf) break;
+    const int t = bi * D.nd + d;
+    const int s0 = D.bsp0[t], s1 = D.bsp1[t];
+    const float b0 = sel(val, s0), b1 = sel(val, s1);
+    const float dJ = buffer_dj(D.kon[t], D.koff[t], D.tot[t], D.dt_r, b0, b1);
+    if (pre >> s0 & 1u) put(out, s0, __fadd_rn(sel(out, s0), dJ)); else put(out, s0, __fadd_rn(b0, dJ));
+    if (pre >> s1 & 1u) put(out, s1, __fsub_rn(sel(out, s1), dJ)); else put(out, s1, __fsub_rn(b1, dJ));
+  }
+}
+
 // What a step does for one realisation (computed once per CTA / unit).
 struct StepInfo {
   unsigned pre;        // species flagged before the reaction (diffusing ones, species.c:1542, 1746)
   unsigned updated;    // species written this step (apply_du copies these, species.c:1080-1121)
   int react;           // reaction step (species.c:1657)
-  int react_fast;      // the reaction can use the per-species table (see voxel_update)
+  int react_fast;      // the reaction can walk the per-species table rtab (see voxel_update)
 };
 
 __host__ __device__ inline StepInfo step_info(const RealDesc& D, long long time_ind) {
@@ -34,21 +77,16 @@ __host__ __device__ inline StepInfo step_info(const RealDesc& D, long long time_
   return si;
 }
 
-// Arithmetic of one voxel given its 7-point neighbourhood.  Loads go through the caller:
-// ld(s, k) = species s at neighbour k (0..5 = z-, z+, y-, y+, x-, x+; 6 = the voxel),
-// ldd(k) = the domain id there.  The direct and the staged kernel share this function,
-// so both give bitwise equal fields.  N = species slots the caller carries (>= D.ns);
-// every species index below is a compile-time constant, so nothing leaves registers.
+// One voxel given its 7-point neighbourhood.  Loads go through the caller: ld(s, k) =
+// species s at neighbour k (0..5 = z-, z+, y-, y+, x-, x+; 6 = the voxel; out-of-box
+// neighbours may return anything: they are replaced by the voxel's own value), ldd(k) =
+// the domain id there.  N = species slots the caller carries (>= D.ns).
 //
-//  diffusion (species.c:1501-1650 with the faces of :1282-1498 and kernel_generic.cpp:
-//  512-600): out = u + sum_n c[d][d_n]*(u_n - u) over the in-box neighbours; when all six
-//  neighbours share the voxel's domain this is u + c[d][d]*sum_n (u_n - u), the
-//  reference's uniform-neighbourhood fast path (kernel_generic.cpp:529-533).
-//  reactions (species.c:1653-1702, kernel_generic.cpp:397-509): J = k_on*(tot-b)*Ca -
-//  k_off*b per buffer, with the step-start values.  When every buffer binds species 0,
-//  the bound species are distinct per domain and species 0 is already updated this step,
-//  the reference's assign-or-accumulate rule reduces to accumulation and the buffers are
-//  walked per bound species (table rtab); otherwise the general rule runs (react).
+//  diffusion (species.c:1501-1650): diffuse_uniform / diffuse_general above.
+//  reactions (species.c:1653-1702): when every buffer binds species 0, the bound species
+//  are distinct per domain and species 0 is already updated this step (react_fast), the
+//  reference's assign-or-accumulate rule reduces to accumulation and the buffers are
+//  walked per bound species (table rtab); otherwise react_general.
 //  fixed values (species.c:1037-1077): fixed (domain, species) pairs and, with -f, the
 //  outer faces of species 0 are reset to their initial values.
 template <int N, class LoadU, class LoadD>
@@ -66,7 +104,8 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
     bool uniform = true;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-      dn[k] = (valid >> k & 1u) ? ldd(k) : d;
+      const int dk = ldd(k);
+      dn[k] = (valid >> k & 1u) ? dk : d;
       uniform = uniform && dn[k] == d;
     }
 #pragma unroll
@@ -75,19 +114,12 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
       const float u = val[s];
       float un[6];
 #pragma unroll
-      for (int k = 0; k < 6; k++) un[k] = (valid >> k & 1u) ? ld(s, k) : u;
-      const float* c = &D.coef[D.dsi_of[s]][d * ND];
-      if (uniform) {
-        float a = un[0] - u;
-#pragma unroll
-        for (int k = 1; k < 6; k++) a += un[k] - u;
-        out[s] = fmaf(c[d], a, u);
-      } else {
-        float a = 0.f;
-#pragma unroll
-        for (int k = 0; k < 6; k++) a = fmaf(c[dn[k]], un[k] - u, a);
-        out[s] = u + a;
+      for (int k = 0; k < 6; k++) {
+        const float v = ld(s, k);
+        un[k] = (valid >> k & 1u) ? v : u;
       }
+      const float* c = &D.coef[D.dsi_of[s]][d * ND];
+      out[s] = uniform ? diffuse_uniform(c[d], u, un) : diffuse_general(c, dn, u, un);
     }
   }
   if (si.react) {
@@ -98,14 +130,12 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
         const int bi = D.rtab[d][s];
         if (bi < 0) continue;
         const int t = bi * D.nd + d;
-        const float b = val[s];
-        const float J = D.kon[t] * (D.tot[t] - b) * ca - D.koff[t] * b;
-        const float dJ = D.dt_r * J;
-        out[s] += dJ;
-        out[0] -= dJ;
+        const float dJ = buffer_dj(D.kon[t], D.koff[t], D.tot[t], D.dt_r, val[s], ca);
+        out[s] = __fadd_rn(out[s], dJ);
+        out[0] = __fsub_rn(out[0], dJ);
       }
     } else {
-      react<N>(D, d, val, out, si.pre);
+      react_general<N>(D, d, val, out, si.pre);
     }
   }
   const unsigned fm = D.fixed_mask[d];

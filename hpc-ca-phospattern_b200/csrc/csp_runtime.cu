@@ -35,8 +35,46 @@ struct HostReal {
   double volumes[ND];
   std::vector<int> boundary_channel_base;   // per boundary: first global channel, or -1
   std::vector<int> boundary_nch;
-  size_t field_elems;             // nx*P
+  size_t field_elems;             // n0*P
+  int perm[3];                    // device axis i holds physical axis perm[i]
+  int nphys[3];                   // species voxels per physical axis
+  // padded linear device index of physical species voxel (x, y, z)
+  long long dev_index(int x, int y, int z) const {
+    const int c[3] = {x, y, z};
+    return (long long)c[perm[0]] * desc.P + (long long)c[perm[1]] * desc.nz + c[perm[2]];
+  }
 };
+
+// Device axis order of one realisation.  The stencil is isotropic and every face has the
+// same no-flux rule, so the kernels may hold the field in any axis order.  The marching
+// axis (device axis 0) is the physical axis crossed by the most domain changes, so that
+// domain-boundary sheets (cleft, jSR, network SR at fixed z in a dyad) become whole
+// planes and the voxels sharing a warp share a neighbourhood type; the contiguous axis
+// (device axis 2) is the one with the fewest changes.
+static void choose_axes(const csp_model& m, int perm[3]) {
+  long long ch[3] = {0, 0, 0};
+  const int N0 = m.N[0], N1 = m.N[1], N2 = m.N[2];
+  for (int x = 0; x < N0; x++)
+    for (int y = 0; y < N1; y++)
+      for (int z = 0; z < N2; z++) {
+        const size_t v = ((size_t)x * N1 + y) * N2 + z;
+        if (x + 1 < N0 && m.voxels[v] != m.voxels[v + (size_t)N1 * N2]) ch[0]++;
+        if (y + 1 < N1 && m.voxels[v] != m.voxels[v + N2]) ch[1]++;
+        if (z + 1 < N2 && m.voxels[v] != m.voxels[v + 1]) ch[2]++;
+      }
+  int a0 = 0;
+  for (int a = 1; a < 3; a++)
+    if (ch[a] > ch[a0]) a0 = a;
+  if (ch[a0] == 0) { perm[0] = 0; perm[1] = 1; perm[2] = 2; return; }
+  int rest[2], k = 0;
+  for (int a = 0; a < 3; a++)
+    if (a != a0) rest[k++] = a;
+  // fewest changes last; on a tie keep the physical order
+  const bool swap = ch[rest[0]] < ch[rest[1]];
+  perm[0] = a0;
+  perm[1] = swap ? rest[1] : rest[0];
+  perm[2] = swap ? rest[0] : rest[1];
+}
 
 }  // namespace
 
@@ -284,13 +322,18 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     std::string err;
     int rc = derive(models[r], options[r], dv[r], err);
     if (rc) { delete h; return fail(nullptr, rc, "realisation %d: %s", r, err.c_str()); }
-    const int plane = dv[r].ny * dv[r].nz;
+    HostReal& hr0 = h->real[r];
+    choose_axes(models[r], hr0.perm);
+    hr0.nphys[0] = dv[r].nx; hr0.nphys[1] = dv[r].ny; hr0.nphys[2] = dv[r].nz;
+    const int n0 = hr0.nphys[hr0.perm[0]], n1 = hr0.nphys[hr0.perm[1]], n2 = hr0.nphys[hr0.perm[2]];
+    const int plane = n1 * n2;
     const int P = round_up(plane, PLANE_ALIGN);
-    h->real[r].field_elems = (size_t)dv[r].nx * P;
-    field_total += h->real[r].field_elems * 2 * models[r].num_species;
-    dom_total += h->real[r].field_elems;
+    if ((long long)n0 * P >= (1ll << 31)) { delete h; return fail(nullptr, CSP_EINVAL, "realisation %d: grid too large (2^31 voxels per field)", r); }
+    hr0.field_elems = (size_t)n0 * P;
+    field_total += hr0.field_elems * 2 * models[r].num_species;
+    dom_total += hr0.field_elems;
     h->max_plane_vox = std::max(h->max_plane_vox, plane);
-    h->max_vox = std::max(h->max_vox, (long long)dv[r].nx * plane);
+    h->max_vox = std::max(h->max_vox, (long long)n0 * plane);
   }
   // -- device allocation (one arena for all fields) --
   cudaError_t e;
@@ -330,8 +373,9 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     memset(&D, 0, sizeof D);
     const int nd = m.num_domains;
     hr.nd = nd;
-    D.nx = d.nx; D.ny = d.ny; D.nz = d.nz;
-    D.plane = d.ny * d.nz;
+    // device axes (choose_axes): nx / ny / nz below are device axes 0 / 1 / 2
+    D.nx = hr.nphys[hr.perm[0]]; D.ny = hr.nphys[hr.perm[1]]; D.nz = hr.nphys[hr.perm[2]];
+    D.plane = D.ny * D.nz;
     D.P = round_up(D.plane, PLANE_ALIGN);
     D.ns = m.num_species; D.nd = nd; D.ndiff = d.ndiff; D.nbuf = d.nbuf;
     D.reaction_substep = d.reaction_substep; D.stochastic_substep = d.stochastic_substep;
@@ -385,7 +429,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
           const unsigned char dd =
               m.voxels[((size_t)(x / d.S) * m.N[1] + y / d.S) * m.N[2] + z / d.S];
           if (dd >= nd) { csp_destroy(h); return fail(nullptr, CSP_EINVAL, "voxel domain id %d >= num_domains", dd); }
-          hostd[(size_t)x * D.P + y * d.nz + z] = dd;
+          hostd[hr.dev_index(x, y, z)] = dd;
         }
     for (size_t i = 0; i < (size_t)m.N[0] * m.N[1] * m.N[2]; i++) gcount[m.voxels[i]]++;
     for (int dd = 0; dd < ND; dd++) hr.volumes[dd] = dd < nd ? gcount[dd] * m.h_geom * m.h_geom * m.h_geom : 0.0;
@@ -423,7 +467,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         D.has_channels = 1;
       }
     }
-    auto lin = [&](const unsigned* c) -> long long { return (long long)c[0] * D.P + (long long)c[1] * d.nz + c[2]; };
+    auto lin = [&](const unsigned* c) -> long long { return hr.dev_index((int)c[0], (int)c[1], (int)c[2]); };
     // flux info per boundary: first of ryr, p_ryr, serca (BoundaryFluxes_get_flux_info)
     for (int bi = 0; bi < m.num_boundaries; bi++) {
       int kind = FLUX_NONE;
@@ -552,11 +596,15 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     }
     row.end = (int)entries.size();
     // a voxel reset by the fixed-value rules after the step keeps its reset value
-    const RealDesc& D = h->real[row.r].desc;
-    const int x = (int)(row.v / D.P), p = (int)(row.v - (long long)x * D.P);
-    const int y = p / D.nz, z = p - y * D.nz;
-    const unsigned char dd = models[row.r].voxels[((size_t)(x / dv[row.r].S) * models[row.r].N[1] + y / dv[row.r].S) * models[row.r].N[2] + z / dv[row.r].S];
-    const bool face = x == 0 || x == D.nx - 1 || y == 0 || y == D.ny - 1 || z == 0 || z == D.nz - 1;
+    const HostReal& rr = h->real[row.r];
+    const RealDesc& D = rr.desc;
+    const int c0 = (int)(row.v / D.P), p = (int)(row.v - (long long)c0 * D.P);
+    const int c1 = p / D.nz, c2 = p - c1 * D.nz;
+    int ph[3];
+    ph[rr.perm[0]] = c0; ph[rr.perm[1]] = c1; ph[rr.perm[2]] = c2;
+    const int S = dv[row.r].S;
+    const unsigned char dd = models[row.r].voxels[((size_t)(ph[0] / S) * models[row.r].N[1] + ph[1] / S) * models[row.r].N[2] + ph[2] / S];
+    const bool face = c0 == 0 || c0 == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
     row.apply = !((D.fixed_mask[dd] >> row.species) & 1u) && !(D.dirichlet && row.species == 0 && face);
     rows.push_back(row);
     i = j;
@@ -597,17 +645,25 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
   return CSP_OK;
 }
 
-static cudaError_t launch_step(csp_handle* h) {
+static void launch_voxels(csp_handle* h) {
   if (h->kernel == 1) {
     dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)h->n);
     k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_err);
   } else {
     staged_launch(h->plan, h->d_desc, h->d_ctl, h->d_err, h->stream);
   }
+}
+
+static void launch_boundaries(csp_handle* h) {
   const int blocks = std::max(1, (h->nrows + 255) / 256);
   k_boundaries<<<blocks, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, h->nrows, h->d_entries, h->d_pairs,
                                               h->d_params, h->d_states, std::max(h->nch, 1), h->n,
                                               h->d_ticket);
+}
+
+static cudaError_t launch_step(csp_handle* h) {
+  launch_voxels(h);
+  launch_boundaries(h);
   return cudaGetLastError();
 }
 
@@ -631,6 +687,50 @@ static int ensure_graph(csp_handle* h) {
   return CSP_OK;
 }
 
+static int finish_advance(csp_handle* h, int32_t* stop_flags) {
+  int err = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  std::vector<RealCtl> ctl(h->n);
+  CUDA_TRY(h, cudaMemcpyAsync(ctl.data(), h->d_ctl, h->n * sizeof(RealCtl), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int r = 0; r < h->n; r++) {
+    h->real[r].info.step = ctl[r].step;
+    h->real[r].info.stopped = ctl[r].stopped;
+    if (stop_flags) stop_flags[r] = ctl[r].stopped;
+  }
+  if (err) return fail(h, CSP_EDEVICE, "device error word %d (%s)", err,
+                       (err & ERR_TIMEOUT) ? "bounded wait timed out" : "index out of bounds");
+  return CSP_OK;
+}
+
+extern "C" int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_ms, float* boundary_ms) {
+  if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
+  std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
+  for (auto& e : ev) CUDA_TRY(h, cudaEventCreate(&e));
+  for (int64_t i = 0; i < nsteps; i++) {
+    cudaEventRecord(ev[3 * i], h->stream);
+    launch_voxels(h);
+    cudaEventRecord(ev[3 * i + 1], h->stream);
+    launch_boundaries(h);
+    cudaEventRecord(ev[3 * i + 2], h->stream);
+  }
+  cudaError_t le = cudaGetLastError();
+  int rc = finish_advance(h, nullptr);
+  float tv = 0.f, tb = 0.f;
+  for (int64_t i = 0; i < nsteps; i++) {
+    float a = 0.f, b = 0.f;
+    cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]);
+    cudaEventElapsedTime(&b, ev[3 * i + 1], ev[3 * i + 2]);
+    tv += a;
+    tb += b;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (le != cudaSuccess) return fail(h, CSP_ECUDA, "launch: %s", cudaGetErrorString(le));
+  if (voxel_ms) *voxel_ms = tv;
+  if (boundary_ms) *boundary_ms = tb;
+  return rc;
+}
+
 extern "C" int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags) {
   if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
   int rc = ensure_graph(h);
@@ -643,20 +743,9 @@ extern "C" int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags) {
   }
   while (left-- > 0) CUDA_TRY(h, launch_step(h));
   CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
-  int err = 0;
-  CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-  std::vector<RealCtl> ctl(h->n);
-  CUDA_TRY(h, cudaMemcpyAsync(ctl.data(), h->d_ctl, h->n * sizeof(RealCtl), cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  int rc2 = finish_advance(h, stop_flags);
   cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
-  for (int r = 0; r < h->n; r++) {
-    h->real[r].info.step = ctl[r].step;
-    h->real[r].info.stopped = ctl[r].stopped;
-    if (stop_flags) stop_flags[r] = ctl[r].stopped;
-  }
-  if (err) return fail(h, CSP_EDEVICE, "device error word %d (%s)", err,
-                       (err & ERR_TIMEOUT) ? "bounded wait timed out" : "index out of bounds");
-  return CSP_OK;
+  return rc2;
 }
 
 static int read_ctl(csp_handle* h, int r, RealCtl& c) {
@@ -678,15 +767,19 @@ extern "C" int csp_upload_state(csp_handle* h, int32_t r, const double* u) {
   RealCtl c;
   int rc = read_ctl(h, r, c);
   if (rc) return rc;
-  const RealDesc& D = h->real[r].desc;
+  const HostReal& hr = h->real[r];
+  const RealDesc& D = hr.desc;
   const unsigned cur = c.cur_mask[c.step & 1];
-  const size_t nvox = (size_t)D.nx * D.plane;
-  std::vector<float> tmp(nvox);
+  const int nx = hr.nphys[0], ny = hr.nphys[1], nz = hr.nphys[2];
+  const size_t nvox = (size_t)nx * ny * nz;
+  std::vector<float> tmp(hr.field_elems, 0.f);
   for (int s = 0; s < D.ns; s++) {
-    for (size_t i = 0; i < nvox; i++) tmp[i] = (float)u[(size_t)s * nvox + i];
-    CUDA_TRY(h, cudaMemcpy2DAsync(D.u[(cur >> s) & 1u][s], (size_t)D.P * sizeof(float), tmp.data(),
-                                  (size_t)D.plane * sizeof(float), (size_t)D.plane * sizeof(float), D.nx,
-                                  cudaMemcpyHostToDevice, h->stream));
+    const double* us = u + (size_t)s * nvox;
+    for (int x = 0; x < nx; x++)
+      for (int y = 0; y < ny; y++)
+        for (int z = 0; z < nz; z++) tmp[hr.dev_index(x, y, z)] = (float)us[((size_t)x * ny + y) * nz + z];
+    CUDA_TRY(h, cudaMemcpyAsync(D.u[(cur >> s) & 1u][s], tmp.data(), hr.field_elems * sizeof(float),
+                                cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   }
   return CSP_OK;
@@ -698,16 +791,20 @@ extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
   RealCtl c;
   int rc = read_ctl(h, r, c);
   if (rc) return rc;
-  const RealDesc& D = h->real[r].desc;
+  const HostReal& hr = h->real[r];
+  const RealDesc& D = hr.desc;
   const unsigned cur = c.cur_mask[c.step & 1];
-  const size_t nvox = (size_t)D.nx * D.plane;
-  std::vector<float> tmp(nvox);
+  const int nx = hr.nphys[0], ny = hr.nphys[1], nz = hr.nphys[2];
+  const size_t nvox = (size_t)nx * ny * nz;
+  std::vector<float> tmp(hr.field_elems);
   for (int s = 0; s < D.ns; s++) {
-    CUDA_TRY(h, cudaMemcpy2DAsync(tmp.data(), (size_t)D.plane * sizeof(float), D.u[(cur >> s) & 1u][s],
-                                  (size_t)D.P * sizeof(float), (size_t)D.plane * sizeof(float), D.nx,
-                                  cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), D.u[(cur >> s) & 1u][s], hr.field_elems * sizeof(float),
+                                cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    for (size_t i = 0; i < nvox; i++) u[(size_t)s * nvox + i] = (double)tmp[i];
+    double* us = u + (size_t)s * nvox;
+    for (int x = 0; x < nx; x++)
+      for (int y = 0; y < ny; y++)
+        for (int z = 0; z < nz; z++) us[((size_t)x * ny + y) * nz + z] = (double)tmp[hr.dev_index(x, y, z)];
   }
   return CSP_OK;
 }

@@ -24,7 +24,7 @@
 
 namespace csp {
 
-constexpr int NST = 5;                    // ring stages: planes x-1, x, x+1 resident, 2 in flight
+constexpr int NST = 4;                    // ring stages: planes x-1, x, x+1 resident, 1 in flight
 constexpr long long WAIT_LIMIT = 1ll << 26;
 
 struct StagedGeom {
@@ -111,8 +111,15 @@ __device__ __forceinline__ void issue_plane(const RealDesc& D, unsigned cur, uns
   bulk_g2s(smem_u32(stage + (size_t)g.ms * g.slot * 4), D.dom + (long long)q * D.P + lob, dbytes, bar);
 }
 
+// 4 bytes starting at any byte address (two aligned 32-bit shared loads + funnel shift).
+__device__ __forceinline__ unsigned ld_u32_any(const unsigned char* p) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const unsigned* w = reinterpret_cast<const unsigned*>(a & ~(uintptr_t)3);
+  return __funnelshift_r(w[0], w[1], 8u * (unsigned)(a & 3));
+}
+
 template <int MS, int T>
-__global__ void __launch_bounds__(T, 1) k_voxels_staged(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                         const int4* __restrict__ units, StagedGeom g,
                                                         int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -157,18 +164,19 @@ __global__ void __launch_bounds__(T, 1) k_voxels_staged(const RealDesc* __restri
     const int ql = max(0, x0 - 1), qh = min(nx - 1, x1);
     const int p0 = cL + 4 * tid;
     unsigned vzy[4];
-    bool inb[4];
+    bool all_in = true;
+    unsigned ymask_m = 0, ymask_p = 0;     // bytes of the y-/y+ words that are in-box neighbours
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int p = p0 + j;
-      inb[j] = p < plane;
+      all_in = all_in && p < plane;
       const int y = p / nz, z = p - y * nz;
       vzy[j] = (z > 0 ? 1u : 0u) | (z < nz - 1 ? 2u : 0u) | (y > 0 ? 4u : 0u) | (y < D.ny - 1 ? 8u : 0u);
+      if (vzy[j] & 4u) ymask_m |= 0xffu << (8 * j);
+      if (vzy[j] & 8u) ymask_p |= 0xffu << (8 * j);
     }
-    // smem slot of every loaded species (popcount rank in lmask)
-    int slot_of[MS];
-#pragma unroll
-    for (int s = 0; s < MS; s++) slot_of[s] = __popc(lmask & ((1u << s) - 1u));
+    // the y- word would start before the staged range only in the first chunk's first row
+    const bool group_ok = all_in && (ymask_m == 0 || p0 - nz >= lob);
 
     if (tid == 0) {
       fence_proxy_async();
@@ -188,6 +196,8 @@ __global__ void __launch_bounds__(T, 1) k_voxels_staged(const RealDesc* __restri
       phase ^= 1u << st;
     };
     auto stage_of = [&](int q) -> const unsigned char* { return ring + (size_t)((q - ql) % NST) * g.stage_bytes; };
+    const int so = g.slot;
+    const size_t dom_off = (size_t)g.ms * g.slot * 4;
 
     if (x0 > 0) wait_plane(x0 - 1);
     wait_plane(x0);
@@ -201,84 +211,146 @@ __global__ void __launch_bounds__(T, 1) k_voxels_staged(const RealDesc* __restri
       const float* fc = reinterpret_cast<const float*>(sc) - lo;
       const float* fp = reinterpret_cast<const float*>(sp) - lo;
       const float* fn = reinterpret_cast<const float*>(sn) - lo;
-      const unsigned char* dc = sc + (size_t)g.ms * g.slot * 4 - lob;
-      const unsigned char* dp = sp + (size_t)g.ms * g.slot * 4 - lob;
-      const unsigned char* dnp = sn + (size_t)g.ms * g.slot * 4 - lob;
-      const int so = g.slot;
-      // own positions of planes x-1, x, x+1: 128-bit shared loads
-      float vc[MS][4], vp[MS][4], vn[MS][4];
+      const unsigned char* dc = sc + dom_off - lob;
+      const unsigned char* dp = sp + dom_off - lob;
+      const unsigned char* dnx = sn + dom_off - lob;
+      const unsigned xval = (has_prev ? 16u : 0u) | (has_next ? 32u : 0u);
+      float out[MS][4];
+
+      // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
+      const unsigned wc = *reinterpret_cast<const unsigned*>(dc + p0);
+      const int d0 = wc & 0xff;
+      const unsigned dw = (unsigned)d0 * 0x01010101u;
+      bool uni = group_ok && wc == dw;
+      if (uni && has_prev) uni = *reinterpret_cast<const unsigned*>(dp + p0) == dw;
+      if (uni && has_next) uni = *reinterpret_cast<const unsigned*>(dnx + p0) == dw;
+      if (uni && (vzy[0] & 1u)) uni = dc[p0 - 1] == d0;
+      if (uni && (vzy[3] & 2u)) uni = dc[p0 + 4] == d0;
+      if (uni && ymask_m) uni = ((ld_u32_any(dc + p0 - nz) ^ dw) & ymask_m) == 0u;
+      if (uni && ymask_p) uni = ((ld_u32_any(dc + p0 + nz) ^ dw) & ymask_p) == 0u;
+
+      if (__builtin_expect(uni, 1)) {
+        // ---- uniform group: constants once per group, one species at a time ----
+        float val[MS][4];
+        int slot = 0;
 #pragma unroll
-      for (int s = 0; s < MS; s++) {
-        if (lmask >> s & 1u) {
-          const int o = slot_of[s] * so + p0;
-          const float4 a = *reinterpret_cast<const float4*>(fc + o);
-          vc[s][0] = a.x; vc[s][1] = a.y; vc[s][2] = a.z; vc[s][3] = a.w;
-          if (si.pre >> s & 1u) {
-            const float4 b = *reinterpret_cast<const float4*>(fp + o);
-            const float4 e = *reinterpret_cast<const float4*>(fn + o);
-            vp[s][0] = b.x; vp[s][1] = b.y; vp[s][2] = b.z; vp[s][3] = b.w;
-            vn[s][0] = e.x; vn[s][1] = e.y; vn[s][2] = e.z; vn[s][3] = e.w;
+        for (int s = 0; s < MS; s++) {
+          if (lmask >> s & 1u) {
+            const float4 a = *reinterpret_cast<const float4*>(fc + slot * so + p0);
+            val[s][0] = a.x; val[s][1] = a.y; val[s][2] = a.z; val[s][3] = a.w;
+            slot++;
+          } else {
+            val[s][0] = val[s][1] = val[s][2] = val[s][3] = 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; j++) out[s][j] = val[s][j];
+        }
+        slot = 0;
+#pragma unroll
+        for (int s = 0; s < MS; s++) {
+          if (!(lmask >> s & 1u)) continue;
+          const int so_s = slot * so;
+          slot++;
+          if (!(si.pre >> s & 1u)) continue;
+          const float cdd = D.coef[D.dsi_of[s]][d0 * ND + d0];
+          float4 vp = make_float4(0.f, 0.f, 0.f, 0.f), vn = vp;
+          if (has_prev) vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
+          if (has_next) vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
+          const float pv[4] = {vp.x, vp.y, vp.z, vp.w};
+          const float nv[4] = {vn.x, vn.y, vn.z, vn.w};
+          const float zm = fc[so_s + ((vzy[0] & 1u) ? p0 - 1 : p0)];
+          const float zp = fc[so_s + ((vzy[3] & 2u) ? p0 + 4 : p0 + 3)];
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const unsigned valid = vzy[j] | xval;
+            const float u = val[s][j];
+            const float ym = fc[so_s + ((valid & 4u) ? p0 + j - nz : p0 + j)];
+            const float yp = fc[so_s + ((valid & 8u) ? p0 + j + nz : p0 + j)];
+            float unb[6];
+            unb[0] = j > 0 ? val[s][j > 0 ? j - 1 : 0] : zm;
+            unb[1] = j < 3 ? val[s][j < 3 ? j + 1 : 3] : zp;
+            unb[2] = ym; unb[3] = yp; unb[4] = pv[j]; unb[5] = nv[j];
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) unb[kk] = (valid >> kk & 1u) ? unb[kk] : u;
+            out[s][j] = diffuse_uniform(cdd, u, unb);
+          }
+        }
+        if (si.react) {
+          if (si.react_fast) {
+#pragma unroll
+            for (int s = 1; s < MS; s++) {
+              const int bi = D.rtab[d0][s];
+              if (bi < 0) continue;
+              const int t = bi * D.nd + d0;
+              const float kon = D.kon[t], koff = D.koff[t], tot = D.tot[t], dtr = D.dt_r;
+#pragma unroll
+              for (int j = 0; j < 4; j++) {
+                const float dJ = buffer_dj(kon, koff, tot, dtr, val[s][j], val[0][j]);
+                out[s][j] = __fadd_rn(out[s][j], dJ);
+                out[0][j] = __fsub_rn(out[0][j], dJ);
+              }
+            }
           } else {
 #pragma unroll
-            for (int j = 0; j < 4; j++) vp[s][j] = vn[s][j] = 0.f;
-          }
-        } else {
+            for (int j = 0; j < 4; j++) {
+              float vj[MS], oj[MS];
 #pragma unroll
-          for (int j = 0; j < 4; j++) vc[s][j] = vp[s][j] = vn[s][j] = 0.f;
+              for (int s = 0; s < MS; s++) { vj[s] = val[s][j]; oj[s] = out[s][j]; }
+              react_general<MS>(D, d0, vj, oj, si.pre);
+#pragma unroll
+              for (int s = 0; s < MS; s++) out[s][j] = oj[s];
+            }
+          }
         }
-      }
-      const unsigned wc = *reinterpret_cast<const unsigned*>(dc + p0);
-      const unsigned wp = *reinterpret_cast<const unsigned*>(dp + p0);
-      const unsigned wn = *reinterpret_cast<const unsigned*>(dnp + p0);
-      const unsigned xval = (has_prev ? 16u : 0u) | (has_next ? 32u : 0u);
-      float outv[4][MS];
+        const unsigned fm = D.fixed_mask[d0];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const unsigned valid = vzy[j] | xval;
-        const bool on_face = valid != 63u;
-        const int pj = p0 + j;
-        auto ld = [&](int s, int kk) -> float {
-          switch (kk) {
-            case 6: return vc[s][j];
-            case 4: return vp[s][j];
-            case 5: return vn[s][j];
-            // out-of-box neighbours read the voxel itself (addresses stay inside the stage)
-            case 0: return j > 0 ? vc[s][j > 0 ? j - 1 : 0] : fc[slot_of[s] * so + ((valid & 1u) ? pj - 1 : pj)];
-            case 1: return j < 3 ? vc[s][j < 3 ? j + 1 : 3] : fc[slot_of[s] * so + ((valid & 2u) ? pj + 1 : pj)];
-            case 2: return fc[slot_of[s] * so + ((valid & 4u) ? pj - nz : pj)];
-            default: return fc[slot_of[s] * so + ((valid & 8u) ? pj + nz : pj)];
+        for (int s = 0; s < MS; s++)
+          if (fm >> s & 1u) {
+            const float iv = D.init[d0][s];
+#pragma unroll
+            for (int j = 0; j < 4; j++) out[s][j] = iv;
           }
-        };
-        auto ldd = [&](int kk) -> int {
-          switch (kk) {
-            case 6: return (wc >> (8 * j)) & 0xff;
-            case 4: return (wp >> (8 * j)) & 0xff;
-            case 5: return (wn >> (8 * j)) & 0xff;
-            case 0: return j > 0 ? (wc >> (8 * (j > 0 ? j - 1 : 0))) & 0xff : dc[(valid & 1u) ? pj - 1 : pj];
-            case 1: return j < 3 ? (wc >> (8 * (j < 3 ? j + 1 : 3))) & 0xff : dc[(valid & 2u) ? pj + 1 : pj];
-            case 2: return dc[(valid & 4u) ? pj - nz : pj];
-            default: return dc[(valid & 8u) ? pj + nz : pj];
-          }
-        };
-        if (inb[j]) {
-          voxel_update<MS>(D, si, valid, on_face, ld, ldd, outv[j]);
-        } else {
-#pragma unroll
-          for (int s = 0; s < MS; s++) outv[j][s] = 0.f;
-        }
-      }
-      const long long base = (long long)x * D.P + p0;
-      const bool full = p0 + 3 < plane;
-#pragma unroll
-      for (int s = 0; s < MS; s++) {
-        if (!(lmask >> s & 1u)) continue;
-        float* dst = D.u[((cur >> s) & 1u) ^ 1u][s] + base;
-        if (full) {
-          *reinterpret_cast<float4*>(dst) = make_float4(outv[0][s], outv[1][s], outv[2][s], outv[3][s]);
-        } else {
+        if (D.dirichlet) {
 #pragma unroll
           for (int j = 0; j < 4; j++)
-            if (inb[j]) dst[j] = outv[j][s];
+            if ((vzy[j] | xval) != 63u) out[0][j] = D.init[d0][0];
+        }
+        // ---- stores (128-bit) ----
+#pragma unroll
+        for (int s = 0; s < MS; s++) {
+          if (!(lmask >> s & 1u)) continue;
+          float4* dst = reinterpret_cast<float4*>(D.u[((cur >> s) & 1u) ^ 1u][s] + (long long)x * D.P + p0);
+          *dst = make_float4(out[s][0], out[s][1], out[s][2], out[s][3]);
+        }
+      } else {
+        // ---- general path: per voxel, straight from the staged planes (kept small:
+        // the 4 positions are not unrolled) ----
+#pragma unroll 1
+        for (int j = 0; j < 4; j++) {
+          const int pj = p0 + j;
+          if (pj >= plane) break;
+          const unsigned valid = vzy[j] | xval;
+          // out-of-box neighbours read the voxel itself (addresses stay inside the stage)
+          const int ia[4] = {(valid & 1u) ? pj - 1 : pj, (valid & 2u) ? pj + 1 : pj,
+                             (valid & 4u) ? pj - nz : pj, (valid & 8u) ? pj + nz : pj};
+          auto ld = [&](int s, int kk) -> float {
+            const int so_s = __popc(lmask & ((1u << s) - 1u)) * so;
+            if (kk == 6) return fc[so_s + pj];
+            if (kk == 4) return fp[so_s + pj];
+            if (kk == 5) return fn[so_s + pj];
+            return fc[so_s + ia[kk]];
+          };
+          auto ldd = [&](int kk) -> int {
+            if (kk == 6) return dc[pj];
+            if (kk == 4) return dp[pj];
+            if (kk == 5) return dnx[pj];
+            return dc[ia[kk]];
+          };
+          float oj[MS];
+          voxel_update<MS>(D, si, valid, valid != 63u, ld, ldd, oj);
+#pragma unroll
+          for (int s = 0; s < MS; s++)
+            if (lmask >> s & 1u) D.u[((cur >> s) & 1u) ^ 1u][s][(long long)x * D.P + pj] = oj[s];
         }
       }
       // plane x-1 is no longer needed: refill its stage with plane x-1+NST
@@ -287,8 +359,8 @@ __global__ void __launch_bounds__(T, 1) k_voxels_staged(const RealDesc* __restri
         const int qn = x - 1 + NST;
         if (qn <= qh) {
           fence_proxy_async();
-          issue_plane(D, cur, lmask, qn, (x - 1 - ql) % NST, ring, g, smem_u32(&bars[(x - 1 - ql) % NST]), lo, hi,
-                      lob, hib);
+          const int st = (x - 1 - ql) % NST;
+          issue_plane(D, cur, lmask, qn, st, ring, g, smem_u32(&bars[st]), lo, hi, lob, hib);
         }
       }
     }

@@ -216,6 +216,11 @@ int csp_get_stream(const csp_handle* h, void** stream);
 /* Device time in ms of the last csp_advance call (CUDA events on the handle stream). */
 int csp_last_advance_ms(const csp_handle* h, float* ms);
 
+/* Advance like csp_advance, but launch the two kernels of every step one by one with CUDA
+ * events around each launch (no graph); voxel_ms / boundary_ms receive the summed device
+ * times of the voxel kernel and of the boundary / gating kernel. */
+int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_ms, float* boundary_ms);
+
 /* Select the voxel kernel: 0 = staged (TMA bulk copies into shared memory, default),
  * 1 = direct (one thread per voxel, global loads).  Both give bitwise equal results. */
 int csp_set_kernel(csp_handle* h, int32_t which);
