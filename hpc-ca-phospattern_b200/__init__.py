@@ -41,6 +41,14 @@ def _status(lib, h):
     return buf.value.decode(errors="replace")
 
 
+def set_device(device):
+    """Select the CUDA device for the handles created next by this thread."""
+    lib = load()
+    rc = lib.csp_set_device(int(device))
+    if rc != 0:
+        raise CspError(rc, _status(lib, None))
+
+
 class Simulation:
     """One handle of libcsparks_cuda.so over n realisations.
 

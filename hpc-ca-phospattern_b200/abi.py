@@ -98,7 +98,8 @@ class csp_info(C.Structure):
                 ("substeps", C.c_int32 * MAX_SPECIES), ("num_buffers", C.c_int32),
                 ("stochastic_substep", C.c_int32), ("reaction_substep", C.c_int32),
                 ("total_steps", C.c_int64), ("step", C.c_int64),
-                ("num_channels", C.c_int32 * MAX_BOUNDARIES), ("stopped", C.c_int32)]
+                ("num_channels", C.c_int32 * MAX_BOUNDARIES), ("stopped", C.c_int32),
+                ("fused_pairs", C.c_int64), ("flux_rows", C.c_int64)]
 
 
 def _name(s):
@@ -220,6 +221,7 @@ def declare(lib):
     h = C.c_void_p
     sig = {
         "csp_options_default": (None, [P(csp_options)]),
+        "csp_set_device": (C.c_int, [C.c_int32]),
         "csp_create": (C.c_int, [P(csp_model), P(csp_options), C.c_int32, P(C.c_void_p)]),
         "csp_get_info": (C.c_int, [h, C.c_int32, P(csp_info)]),
         "csp_upload_state": (C.c_int, [h, C.c_int32, P(C.c_double)]),

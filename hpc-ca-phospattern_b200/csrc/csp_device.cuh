@@ -19,6 +19,7 @@ constexpr int ND = CSP_MAX_DOMAINS;
 constexpr int NS = CSP_MAX_SPECIES;
 constexpr int NB = CSP_MAX_BUFFERS;
 constexpr int PLANE_ALIGN = 128;
+constexpr int DOMAIN_BITS = 7;      // domain id = domain byte & DOMAIN_BITS
 
 enum FluxKind : int { FLUX_NONE = 0, FLUX_RYR = 1, FLUX_P_RYR = 2, FLUX_SERCA = 3 };
 
@@ -39,6 +40,14 @@ struct RealDesc {
   signed char dsi_of[NS];            // diffusive index of species s, or -1
   signed char rtab[ND][NS];          // fast reaction table: buffer index bi with bsp0 = s in domain d, or -1
   int react_fast;                    // every buffer binds species 0 and bound species are distinct per domain
+  // Density-boundary fluxes evaluated inside the voxel kernels.  A voxel's domain byte
+  // holds the domain id in bits 0-2 and a flux pattern index in bits 3-7 (0 = none).
+  // fpat[pattern][k] for neighbour direction k: 0 = no flux, else (slot + 1), with bit 7
+  // set when this voxel is the receiving ("to") side of the pair.
+  unsigned char fpat[32][6];
+  int fslot_species[4];
+  int fslot_kind[4];
+  double fslot_p[4][10];
   float init[ND][NS];
   float* u[2][NS];                   // the two buffers of every species
   const unsigned char* dom;          // [nx][P]
@@ -183,6 +192,30 @@ __host__ __device__ inline double serca_flux(double dt, double h, double u0, dou
   const double J = h * h * (params[1] * (v_cycle * Q));
   const double V = 1e-24 * h * h * h;
   return dt * (J / V);
+}
+
+// The same SERCA law with its two common denominators cleared, so one division remains
+// (den_i = T_Cai^2(1+T_Hi) + T_Hi(1+T_H1), den_sr = T_H(T_Casr^2+1) + T_Hsr(1+T_H)):
+//   v = (a_p1 P2 P3 - M1 M2 a_m3) /
+//       (P2 P3 + M1 P3 + M1 M2 + den_i (a_p1 P3 + a_p1 M2 + M2 a_m3) + den_sr (a_p1 P2 + a_m3 M1 + a_m3 P2))
+// with P2 = k_p2 T_Cai^2, M1 = k_m1 T_Hi, P3 = k_p3 T_Hsr, M2 = k_m2 ADP T_Casr^2 T_H, the
+// numerators of a_p2, a_m1, a_p3, a_m2 in serca_flux.  Equal to serca_flux up to FP64
+// rounding; `scale` = dt*density*Q/(1e-24 h) folds the unit conversion of the flux.
+__host__ __device__ inline double serca_flux_fast(double u0, double u1, double scale) {
+  const double k_p1 = 25900, k_p2 = 2540, k_p3 = 20.5, k_m1 = 16, k_m2 = 67200, k_m3 = 149;
+  const double inv_kdcai = 1.0 / 0.9, inv_kdcasr = 1.0 / 2.24;
+  const double H_i = 1e-4, ATP = 5, ADP = 36.3e-3, P_i = 1;
+  const double T_H1 = H_i / 1.09e-5, T_Hi = (H_i * H_i) / 3.54e-3, T_Hsr = (H_i * H_i) / 1.05e-8, T_H = H_i / 7.24e-5;
+  const double T_Cai = u0 * 1e-3 * inv_kdcai, T_Casr = u1 * 1e-3 * inv_kdcasr;
+  const double T_Cai2 = T_Cai * T_Cai, T_Casr2 = T_Casr * T_Casr;
+  const double a_p1 = k_p1 * ATP, a_m3 = k_m3 * P_i;
+  const double den_i = T_Cai2 * (1 + T_Hi) + T_Hi * (1 + T_H1);
+  const double den_sr = T_H * (T_Casr2 + 1) + T_Hsr * (1 + T_H);
+  const double P2 = k_p2 * T_Cai2, M1 = k_m1 * T_Hi, P3 = k_p3 * T_Hsr, M2 = k_m2 * ADP * T_Casr2 * T_H;
+  const double num = a_p1 * P2 * P3 - M1 * M2 * a_m3;
+  const double den = P2 * P3 + M1 * P3 + M1 * M2 + den_i * (a_p1 * P3 + a_p1 * M2 + M2 * a_m3) +
+                     den_sr * (a_p1 * P2 + a_m3 * M1 + a_m3 * P2);
+  return scale * (num / den);
 }
 
 __host__ __device__ inline double ryr_flux(double dt, double h, double u0, double u1, const double* params) {

@@ -89,10 +89,19 @@ __host__ __device__ inline StepInfo step_info(const RealDesc& D, long long time_
 //  walked per bound species (table rtab); otherwise react_general.
 //  fixed values (species.c:1037-1077): fixed (domain, species) pairs and, with -f, the
 //  outer faces of species 0 are reset to their initial values.
+// Boundary flux of one pair, FP64 (boundaryfluxes.c:12-141), u0 on the "from" side.
+// fslot_p[slot][9] holds the SERCA scale dt*density*Q/(1e-24 h) (serca_flux_fast).
+__device__ __forceinline__ double pair_flux(const RealDesc& D, int slot, double u0, double u1) {
+  return D.fslot_kind[slot] == FLUX_SERCA ? serca_flux_fast(u0, u1, D.fslot_p[slot][9])
+                                          : ryr_flux(D.dt, D.h, u0, u1, D.fslot_p[slot]);
+}
+
 template <int N, class LoadU, class LoadD>
 __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& si, unsigned valid, bool on_face,
                                              LoadU ld, LoadD ldd, float (&out)[N]) {
-  const int d = ldd(6);
+  const int braw = ldd(6);
+  const int d = braw & DOMAIN_BITS;
+  const int pat = braw >> 3;
   float val[N];
 #pragma unroll
   for (int s = 0; s < N; s++) {
@@ -104,7 +113,7 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
     bool uniform = true;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-      const int dk = ldd(k);
+      const int dk = ldd(k) & DOMAIN_BITS;
       dn[k] = (valid >> k & 1u) ? dk : d;
       uniform = uniform && dn[k] == d;
     }
@@ -120,6 +129,24 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
       }
       const float* c = &D.coef[D.dsi_of[s]][d * ND];
       out[s] = uniform ? diffuse_uniform(c[d], u, un) : diffuse_general(c, dn, u, un);
+      if (pat) {
+        // density-boundary fluxes across this voxel's faces (Species_step_boundary_fluxes,
+        // species.c:1751-1807: du[to] += J, du[from] -= J), after diffusion, before reactions
+        double acc = 0.0;
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          const int code = D.fpat[pat][k];
+          if (!code) continue;
+          const int slot = (code & 0x7f) - 1;
+          if (D.fslot_species[slot] != s) continue;
+          const double self = (double)u, other = (double)un[k];
+          if (code & 0x80) acc += pair_flux(D, slot, other, self);
+          else acc -= pair_flux(D, slot, self, other);
+          any = true;
+        }
+        if (any) out[s] = (float)((double)out[s] + acc);
+      }
     }
   }
   if (si.react) {
@@ -258,7 +285,7 @@ __global__ void __launch_bounds__(256) k_boundaries(const RealDesc* __restrict__
         }
         if (ti % D.substeps[pr.dsi] != 0) continue;
         const double u0 = (double)__ldg(uold + pr.v0), u1 = (double)__ldg(uold + pr.v1);
-        const double J = pr.kind == FLUX_SERCA ? serca_flux(D.dt, D.h, u0, u1, fp.p) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
+        const double J = pr.kind == FLUX_SERCA ? serca_flux_fast(u0, u1, fp.p[9]) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
         acc += (double)en.sign * J;
         any = true;
       }
@@ -315,7 +342,7 @@ __global__ void __launch_bounds__(256) k_reduce_partial(const RealDesc* __restri
   for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox; v += (long long)gridDim.x * blockDim.x) {
     const int x = (int)(v / D.plane);
     const long long idx = (long long)x * D.P + (v - (long long)x * D.plane);
-    const int d = D.dom[idx];
+    const int d = D.dom[idx] & DOMAIN_BITS;
     const double val = (double)u[idx];
 #pragma unroll
     for (int dd = 0; dd < ND; dd++) {

@@ -9,9 +9,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
+#include <unordered_map>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <ctime>
 #include <string>
@@ -358,6 +362,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
   cudaMemsetAsync(h->d_dom, 0, dom_total + 256, h->stream);
 
   std::vector<FluxPair> pairs;
+  std::vector<char> fused;           // pair evaluated inside the voxel kernels
   std::vector<FluxParams> params;
   std::vector<unsigned char> states0;
   std::vector<RealCtl> ctl(n);
@@ -433,7 +438,6 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         }
     for (size_t i = 0; i < (size_t)m.N[0] * m.N[1] * m.N[2]; i++) gcount[m.voxels[i]]++;
     for (int dd = 0; dd < ND; dd++) hr.volumes[dd] = dd < nd ? gcount[dd] * m.h_geom * m.h_geom * m.h_geom : 0.0;
-    cudaMemcpyAsync((void*)D.dom, hostd.data(), hr.field_elems, cudaMemcpyHostToDevice, h->stream);
     hostf.assign(hr.field_elems, 0.f);
     for (int s = 0; s < m.num_species; s++) {
       for (size_t i = 0; i < hr.field_elems; i++) hostf[i] = (float)m.domain[hostd[i]].init[s];
@@ -484,7 +488,11 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
       memset(&fp, 0, sizeof fp);
       if (kind == FLUX_RYR) ryr_params(fp, m.ryr, t_close_of(o, "ryr"));
       else if (kind == FLUX_P_RYR) ryr_params(fp, m.p_ryr, t_close_of(o, "p_ryr"));
-      else { fp.p[0] = m.serca.v_cyt_to_A_sr; fp.p[1] = m.serca.density; fp.p[2] = m.serca.scale; fp.t_close = -1; }
+      else {
+        fp.p[0] = m.serca.v_cyt_to_A_sr; fp.p[1] = m.serca.density; fp.p[2] = m.serca.scale; fp.t_close = -1;
+        // serca_flux (boundaryfluxes.c:73-84): dt * density*v*Q * h^2 / (1e-24 h^3)
+        fp.p[9] = d.dt * (m.serca.density * (1e-3 / 6e17)) / (1e-24 * d.h);
+      }
       const int pidx = (int)params.size();
       params.push_back(fp);
       const csp_boundary& gb = m.boundaries[bi];
@@ -501,8 +509,109 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         p.v0 = lin(&bv[6 * i]);
         p.v1 = lin(&bv[6 * i + 3]);
         pairs.push_back(p);
+        fused.push_back(0);
       }
     }
+    int64_t nfused = 0;
+    // -- density-boundary pairs joining two face-adjacent voxels are evaluated inside the
+    // voxel kernels: per voxel a 6-direction code vector, deduplicated into <= 31 patterns
+    // stored in the domain byte (bits 3-7).  Anything that does not fit stays a flux row.
+    {
+      std::vector<size_t> cand;
+      for (size_t i = 0; i < pairs.size(); i++) {
+        const FluxPair& p = pairs[i];
+#ifdef CSP_FUSE_DENSITY
+        if (p.r == r && p.kind == FLUX_SERCA && p.inner && p.channel < 0) cand.push_back(i);
+#endif
+      }
+      int nslot = 0;
+      int slot_boundary[4] = {-1, -1, -1, -1};
+      auto dev_coords = [&](long long v, int c[3]) {
+        c[0] = (int)(v / D.P);
+        const int rem = (int)(v - (long long)c[0] * D.P);
+        c[1] = rem / D.nz;
+        c[2] = rem - c[1] * D.nz;
+      };
+      bool ok = true;
+      // candidate pairs that can be fused: (pair, slot, k_from, k_to)
+      struct Cand { size_t i; int slot, kf, kt; };
+      std::vector<Cand> cands;
+      for (size_t i : cand) {
+        const FluxPair& p = pairs[i];
+        int a[3], b[3];
+        dev_coords(p.v0, a);
+        dev_coords(p.v1, b);
+        int axis = -1, nd_ = 0;
+        for (int q = 0; q < 3; q++)
+          if (a[q] != b[q]) { nd_++; axis = q; }
+        if (nd_ != 1 || std::abs(a[axis] - b[axis]) != 1) continue;   // not face-adjacent
+        int slot = -1;
+        for (int q = 0; q < nslot; q++)
+          if (slot_boundary[q] == p.boundary) slot = q;
+        if (slot < 0) {
+          if (nslot == 4) continue;
+          slot = nslot++;
+          slot_boundary[slot] = p.boundary;
+          D.fslot_species[slot] = p.species;
+          D.fslot_kind[slot] = p.kind;
+          for (int q = 0; q < 10; q++) D.fslot_p[slot][q] = params[p.param].p[q];
+        }
+        // direction k: device axis 2 -> 0/1, axis 1 -> 2/3, axis 0 -> 4/5 (minus / plus)
+        const int kbase = 2 * (2 - axis);
+        cands.push_back({i, slot, kbase + (b[axis] > a[axis] ? 1 : 0), kbase + (b[axis] > a[axis] ? 0 : 1)});
+      }
+      // per-voxel code vectors; pairs touching voxels whose pattern is not among the 31
+      // most frequent ones go back to the boundary kernel, until the patterns fit
+      std::vector<char> keep(cands.size(), 1);
+      std::unordered_map<long long, std::array<unsigned char, 6>> vc;
+      std::map<std::array<unsigned char, 6>, int> patterns;
+      for (int iter = 0; iter < 64; iter++) {
+        vc.clear();
+        for (size_t q = 0; q < cands.size(); q++) {
+          if (!keep[q]) continue;
+          const FluxPair& p = pairs[cands[q].i];
+          auto& c0 = vc[p.v0];
+          auto& c1 = vc[p.v1];
+          if (c0[cands[q].kf] || c1[cands[q].kt]) { keep[q] = 0; continue; }   // face already used
+          c0[cands[q].kf] = (unsigned char)(cands[q].slot + 1);
+          c1[cands[q].kt] = (unsigned char)((cands[q].slot + 1) | 0x80);
+        }
+        std::map<std::array<unsigned char, 6>, long long> freq;
+        for (auto& kv : vc) freq[kv.second]++;
+        patterns.clear();
+        if ((int)freq.size() <= 31) {
+          for (auto& kv : freq) patterns.emplace(kv.first, (int)patterns.size() + 1);
+          break;
+        }
+        std::vector<std::pair<long long, std::array<unsigned char, 6>>> byf;
+        for (auto& kv : freq) byf.push_back({kv.second, kv.first});
+        std::stable_sort(byf.begin(), byf.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        std::map<std::array<unsigned char, 6>, int> top;
+        for (int q = 0; q < 31; q++) top.emplace(byf[q].second, 1);
+        for (size_t q = 0; q < cands.size(); q++) {
+          if (!keep[q]) continue;
+          const FluxPair& p = pairs[cands[q].i];
+          if (!top.count(vc[p.v0]) || !top.count(vc[p.v1])) keep[q] = 0;
+        }
+      }
+      std::vector<size_t> taken;
+      for (size_t q = 0; q < cands.size(); q++)
+        if (keep[q]) taken.push_back(cands[q].i);
+      if (patterns.empty() && !vc.empty()) ok = false;
+      if (getenv("CSP_DEBUG"))
+        fprintf(stderr, "csp: realisation %d: %zu density pairs, %zu fused, %zu flux patterns\n", r, cand.size(),
+                ok ? taken.size() : (size_t)0, patterns.size());
+      if (ok && !taken.empty()) {
+        memset(D.fpat, 0, sizeof D.fpat);
+        for (auto& kv : patterns)
+          for (int k = 0; k < 6; k++) D.fpat[kv.second][k] = kv.first[k];
+        for (auto& kv : vc) hostd[kv.first] = (unsigned char)(hostd[kv.first] | (patterns[kv.second] << 3));
+        for (size_t i : taken) fused[i] = 1;
+        nfused = (int64_t)taken.size();
+      }
+    }
+    cudaMemcpyAsync((void*)D.dom, hostd.data(), hr.field_elems, cudaMemcpyHostToDevice, h->stream);
+    cudaStreamSynchronize(h->stream);
     // initial channel states (BoundaryFluxes_init_stochastic_boundaries, boundaryfluxes.c:544-605)
     int ndiscrete = 0;
     for (int bi = 0; bi < m.num_boundaries; bi++) ndiscrete += m.boundaries[bi].type == CSP_BOUNDARY_DISCRETE;
@@ -551,6 +660,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     // info
     csp_info& in = hr.info;
     memset(&in, 0, sizeof in);
+    in.fused_pairs = nfused;
     in.n[0] = d.nx; in.n[1] = d.ny; in.n[2] = d.nz;
     in.subdivisions = d.S; in.h = d.h; in.dt = d.dt;
     in.num_species = m.num_species; in.num_diffusive = d.ndiff;
@@ -571,6 +681,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
   std::vector<Side> sides;
   for (int i = 0; i < (int)pairs.size(); i++) {
     const FluxPair& p = pairs[i];
+    if (fused[i]) continue;
     sides.push_back({p.r, p.species, p.v1, i, 1.f, p.channel >= 0 ? 1 : 0});
     if (p.inner) sides.push_back({p.r, p.species, p.v0, i, -1.f, 0});
   }
@@ -607,6 +718,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     const bool face = c0 == 0 || c0 == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
     row.apply = !((D.fixed_mask[dd] >> row.species) & 1u) && !(D.dirichlet && row.species == 0 && face);
     rows.push_back(row);
+    h->real[row.r].info.flux_rows++;
     i = j;
   }
   h->nrows = (int)rows.size();
@@ -893,6 +1005,12 @@ extern "C" int csp_get_stream(const csp_handle* h, void** stream) {
 extern "C" int csp_last_advance_ms(const csp_handle* h, float* ms) {
   if (!h || !ms) return CSP_EINVAL;
   *ms = h->last_ms;
+  return CSP_OK;
+}
+
+extern "C" int csp_set_device(int32_t device) {
+  const cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(nullptr, CSP_ECUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
   return CSP_OK;
 }
 

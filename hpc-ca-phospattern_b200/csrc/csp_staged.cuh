@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
       const unsigned wc = *reinterpret_cast<const unsigned*>(dc + p0);
       const int d0 = wc & 0xff;
       const unsigned dw = (unsigned)d0 * 0x01010101u;
-      bool uni = group_ok && wc == dw;
+      bool uni = group_ok && wc == dw && d0 <= DOMAIN_BITS;   // no flux pattern in the group
       if (uni && has_prev) uni = *reinterpret_cast<const unsigned*>(dp + p0) == dw;
       if (uni && has_next) uni = *reinterpret_cast<const unsigned*>(dnx + p0) == dw;
       if (uni && (vzy[0] & 1u)) uni = dc[p0 - 1] == d0;

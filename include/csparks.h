@@ -164,9 +164,15 @@ typedef struct csp_info {
   int64_t step;             /* steps already taken */
   int32_t num_channels[CSP_MAX_BOUNDARIES];   /* discrete boundaries, in boundary order */
   int32_t stopped;          /* 1 once the -X rule or total_steps ended the run */
+  int64_t fused_pairs;      /* boundary pairs evaluated inside the voxel kernels */
+  int64_t flux_rows;        /* voxels updated by the boundary / channel kernel */
 } csp_info;
 
 typedef struct csp_handle csp_handle;
+
+/* Select the CUDA device of the calling thread for the handles it creates next (one
+ * process per GPU: rank i calls csp_set_device(i) before csp_create). */
+int csp_set_device(int32_t device);
 
 /* Build device state for n independent realisations (models[r], options[r]) and set
  * the initial state exactly as the reference does before its time loop
