@@ -235,6 +235,8 @@ def declare(lib):
         "csp_last_advance_ms": (C.c_int, [h, P(C.c_float)]),
         "csp_set_kernel": (C.c_int, [h, C.c_int32]),
         "csp_profile_advance": (C.c_int, [h, C.c_int64, P(C.c_float), P(C.c_float)]),
+        "csp_reduce_field_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_double,
+                                               C.c_void_p, C.c_void_p]),
         "csp_destroy": (None, [h]),
     }
     for name, (res, args) in sig.items():

@@ -233,6 +233,28 @@ int csp_set_kernel(csp_handle* h, int32_t which);
 
 void csp_destroy(csp_handle* h);
 
+/* ---- allocation-free reduction ----
+ * No counterpart in the reference.  For callers that cannot allocate device memory: a
+ * plugin inside a framework that has reserved the device memory for its own pool, or
+ * code that must not call cudaMalloc (it synchronises the device) in a latency-bound
+ * loop.  Computes, for one FP32 field of n voxels already on the device with its uint8
+ * domain ids (bits 0-2), the per-domain min (from FLT_MAX), max (from FLT_MIN) and
+ * sum(u)*dV in FP64 -- the reductions of csp_reduce_outputs -- into the caller's device
+ * array out[3][num_domains] (min, max, total), on `stream` (NULL = default stream).
+ * It allocates nothing: block partials live in a file-scope device array of
+ * CSP_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.
+ *  - the first call on a device looks the array's address up (cudaGetSymbolAddress);
+ *    make that first call before any stream capture;
+ *  - all calls share the array: calls that overlap on the GPU race; each call overwrites
+ *    every partial it reads, so no clearing is needed;
+ *  - num_domains above CSP_NOALLOC_MAX_DOMAINS or n above CSP_NOALLOC_MAX_VOXELS return
+ *    CSP_ERANGE (with a message on stderr). */
+#define CSP_NOALLOC_MAX_DOMAINS 5
+#define CSP_NOALLOC_MAX_VOXELS (1LL << 40)
+#define CSP_NOALLOC_SCRATCH_BYTES (592 * 3 * CSP_MAX_DOMAINS * 8)
+int csp_reduce_field_noalloc(const float* field, const uint8_t* domains, int64_t n, int32_t num_domains,
+                             double dV, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,60 @@
+"""The allocation-free reduction entry point against the handle's own reduction.
+
+csp_reduce_field_noalloc serves callers that cannot allocate device memory (a plugin
+inside a framework that reserved the device memory for its pool, or a latency-bound loop
+where cudaMalloc's device synchronisation is not allowed).  Its block partials live in a
+fixed device array inside the library.  This test passes it the device buffers of the
+fields of a running simulation and checks, on two calls in a row, that it returns what
+csp_reduce_outputs returns for the same fields.  It is collected last on purpose.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FLT_MAX = float(np.float32(3.4028235e38))
+FLT_MIN = float(np.float32(1.1754944e-38))
+
+
+def test_noalloc_reduction_matches_csp_reduce_outputs(pkg, synth):
+    import torch
+    spec = synth.tiny((12, 12, 16))
+    sim = pkg.Simulation(spec, dict(h=6.0, tstop=1.0, seed=1, open_states={"ryr": [0, 3]}))
+    sim.advance(40)
+    mn, mx, tot, _ = sim.outputs()                      # the existing entry point
+    u = sim.state()                                     # [species][x][y][z]
+    nd = len(spec["domains"])
+    dV = sim.info().h ** 3
+    lib = pkg.load()
+    dom = torch.tensor(np.ascontiguousarray(spec["voxels"]).ravel(), dtype=torch.uint8, device="cuda")
+    n = dom.numel()
+    present = [d for d in range(nd) if np.any(spec["voxels"] == d)]
+    for call in range(2):                                # two calls in a row share the scratch
+        for s in range(u.shape[0]):
+            field = torch.tensor(u[s].ravel().astype(np.float32), device="cuda")
+            out = torch.full((3 * nd,), -1.0, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            rc = lib.csp_reduce_field_noalloc(C.c_void_p(field.data_ptr()), C.c_void_p(dom.data_ptr()), n, nd,
+                                              dV, C.c_void_p(out.data_ptr()), None)
+            assert rc == 0
+            torch.cuda.synchronize()
+            o = out.cpu().numpy().reshape(3, nd)
+            for d in present:
+                np.testing.assert_allclose(o[0, d], mn[d, s], rtol=1e-12)
+                np.testing.assert_allclose(o[1, d], mx[d, s], rtol=1e-12)
+                np.testing.assert_allclose(o[2, d], tot[d, s], rtol=1e-9)
+            for d in set(range(nd)) - set(present):
+                assert o[0, d] == FLT_MAX and o[1, d] == FLT_MIN and o[2, d] == 0.0
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch(pkg):
+    import torch
+    lib = pkg.load()
+    field = torch.zeros(16, dtype=torch.float32, device="cuda")
+    dom = torch.zeros(16, dtype=torch.uint8, device="cuda")
+    out = torch.zeros(3 * 8, dtype=torch.float64, device="cuda")
+    rc = lib.csp_reduce_field_noalloc(C.c_void_p(field.data_ptr()), C.c_void_p(dom.data_ptr()), 16, 6, 1.0,
+                                      C.c_void_p(out.data_ptr()), None)
+    assert rc == -4          # CSP_ERANGE: more domains than the fixed scratch holds
