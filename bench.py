@@ -127,6 +127,13 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def shard_workload(rank, world, nreal):
+    """The realisations of one rank: its own seed range (weak scaling, nothing shared)."""
+    synth = importlib.import_module("hpc-ca-phospattern_b200.synth")
+    specs, opts = synth.config3(n=nreal, seed=3 + 1000 * rank)
+    return specs, opts
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -199,7 +206,7 @@ def main():
     D = Dist(world, local)
     pkg.set_device(local)
     nreal = args.realisations
-    specs, opts = synth.config3(n=nreal, seed=3 + 1000 * rank)
+    specs, opts = shard_workload(rank, world, nreal)
     sim = pkg.Simulation(specs, opts)
     nvox = sum(int(np.prod(s["voxels"].shape)) for s in specs)
     W, K = max(3, args.warmup), args.steps
