@@ -264,7 +264,7 @@ def main():
                "sample": f"{args.cpu_steps} steps of one 100x100x50 realisation of the workload "
                          f"({dt:.1f} s), FP64 port of the reference"}
 
-    kernels = 2 * K   # voxel kernel + boundary/gating kernel per step
+    kernels = 3 * K   # voxel kernel + boundary/gating kernel + step epilogue per step
     if rank == 0:
         line = {
             "metric": "ensemble voxel-steps/s", "value": value, "unit": "voxel-steps/s",

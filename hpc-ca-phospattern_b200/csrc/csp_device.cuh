@@ -81,14 +81,20 @@ struct FluxPair {
   int pad;
 };
 
-// One voxel receiving flux: entries [begin, end) of the entry list, in pair order.
+// One voxel receiving flux.  Its first pair is stored inline (most voxels touch one
+// pair); further pairs are entries [more_begin, more_end) of the entry list, in pair order.
 struct FluxRow {
-  int r, species;
-  long long v;
-  int begin, end;
-  int apply;              // 0 if the voxel is reset by the fixed-value rules after the step
-  int pad;
+  long long v;            // receiving voxel
+  long long v0, v1;       // first pair: from / to voxel
+  int r;                  // realisation
+  int param;              // first pair: parameter block
+  int channel;            // first pair: global channel index, -1 for density boundaries
+  int local_channel;      // first pair: channel index within its boundary (RNG counter)
+  float sign;             // first pair: +1 receiving side, -1 giving side
+  int more_begin, more_end;
+  unsigned char species, dsi, kind, owner, boundary, apply, pad0, pad1;
 };
+static_assert(sizeof(FluxRow) == 64, "a flux row is one 64-byte line");
 
 struct FluxEntry {
   int pair;

@@ -238,93 +238,104 @@ __device__ __forceinline__ int gate(const FluxParams& fp, int state, double c0, 
   return state;
 }
 
-// One thread per flux row (a voxel receiving boundary flux).  Each row sums, in pair
-// order, the flux of every pair that touches it, with the channel states after this
-// step's gating; the owner entry of a channel stores its new state.  The last block
-// to finish runs the step epilogue for every realisation.
+// Flux of one pair at this step, with the channel gated first (a discrete pair flows
+// only when its channel is open after this step's gating).  The owner side of a channel
+// stores its new state.  Returns false when the pair carries no flux this step.
+__device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int r, int kind, int dsi,
+                                          int channel, int local_channel, int boundary, int owner, long long v0,
+                                          long long v1, const FluxParams& fp, const float* __restrict__ uold,
+                                          const float* __restrict__ ca, unsigned char* __restrict__ states, int nch,
+                                          long long k, bool stoch, double& J) {
+  const long long ti = k + 1;
+  if (channel >= 0) {
+    const int s_old = states[(k & 1) * (long long)nch + channel];
+    int s_new = s_old;
+    if (stoch && kind != FLUX_SERCA)
+      s_new = gate(fp, s_old, (double)__ldg(ca + v1), (double)ti * D.dt, D.dt * D.stochastic_substep, D.seed,
+                   (unsigned)r, (unsigned)local_channel, (unsigned)boundary, ti);
+    if (owner) {
+      states[((k + 1) & 1) * (long long)nch + channel] = (unsigned char)s_new;
+      if (s_new == 1) atomicAdd(&ctl_r->open_count[(k + 1) & 1], 1);
+    }
+    if (s_new != 1) return false;
+  }
+  if (ti % D.substeps[dsi] != 0) return false;
+  const double u0 = (double)__ldg(uold + v0), u1 = (double)__ldg(uold + v1);
+  J = kind == FLUX_SERCA ? serca_flux_fast(u0, u1, fp.p[9]) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
+  return true;
+}
+
+// One thread per flux row (a voxel receiving boundary flux): channel gating
+// (evaluate_RyR_stochastically, boundaryfluxes.c:295-359) and the flux of every pair that
+// touches the voxel, summed in pair order (Species_step_boundary_fluxes,
+// species.c:1704-1907), added to the voxel's new value.
 __global__ void __launch_bounds__(256) k_boundaries(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                      const FluxRow* __restrict__ rows, int nrows,
                                                      const FluxEntry* __restrict__ entries,
                                                      const FluxPair* __restrict__ pairs,
                                                      const FluxParams* __restrict__ params,
                                                      unsigned char* __restrict__ states,  // [2][nch]
-                                                     int nch, int nreal,
-                                                     unsigned* __restrict__ ticket) {
+                                                     int nch) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nrows) {
-    const FluxRow row = rows[i];
-    const RealDesc& D = descs[row.r];
-    const RealCtl& C = ctl[row.r];
-    if (!C.stopped) {
-      const long long k = C.step;
-      const long long ti = k + 1;
-      unsigned pre, updated, diffusing;
-      step_masks(D, ti, pre, updated, diffusing);
-      const unsigned cur = C.cur_mask[k & 1];
-      const bool stoch = (ti % D.stochastic_substep) == 0;
-      const double t = (double)ti * D.dt, dts = D.dt * D.stochastic_substep;
-      const float* __restrict__ uold = D.u[(cur >> row.species) & 1u][row.species];
-      const float* __restrict__ ca = D.u[cur & 1u][0];
-      double acc = 0.0;
-      bool any = false;
-      for (int e = row.begin; e < row.end; e++) {
-        const FluxEntry en = entries[e];
-        const FluxPair pr = pairs[en.pair];
-        const FluxParams& fp = params[pr.param];
-        if (pr.channel >= 0) {
-          int s_old = states[(k & 1) * (long long)nch + pr.channel];
-          int s_new = s_old;
-          if (stoch && pr.kind != FLUX_SERCA)
-            s_new = gate(fp, s_old, (double)__ldg(ca + pr.v1), t, dts, D.seed, (unsigned)row.r,
-                         (unsigned)pr.local_channel, (unsigned)pr.boundary, ti);
-          if (en.owner) {
-            states[((k + 1) & 1) * (long long)nch + pr.channel] = (unsigned char)s_new;
-            if (s_new == 1) atomicAdd(&ctl[row.r].open_count[(k + 1) & 1], 1);
-          }
-          if (s_new != 1) continue;
-        }
-        if (ti % D.substeps[pr.dsi] != 0) continue;
-        const double u0 = (double)__ldg(uold + pr.v0), u1 = (double)__ldg(uold + pr.v1);
-        const double J = pr.kind == FLUX_SERCA ? serca_flux_fast(u0, u1, fp.p[9]) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
-        acc += (double)en.sign * J;
-        any = true;
-      }
-      if (any && row.apply && (updated >> row.species & 1u)) {
-        float* unew = D.u[((cur >> row.species) & 1u) ^ 1u][row.species];
-        unew[row.v] = (float)((double)unew[row.v] + acc);
-      }
+  if (i >= nrows) return;
+  const FluxRow row = rows[i];
+  const RealDesc& D = descs[row.r];
+  const RealCtl& C = ctl[row.r];
+  if (C.stopped) return;
+  const long long k = C.step;
+  const long long ti = k + 1;
+  unsigned pre, updated, diffusing;
+  step_masks(D, ti, pre, updated, diffusing);
+  const unsigned cur = C.cur_mask[k & 1];
+  const bool stoch = (ti % D.stochastic_substep) == 0;
+  const float* __restrict__ uold = D.u[(cur >> row.species) & 1u][row.species];
+  const float* __restrict__ ca = D.u[cur & 1u][0];
+  double acc = 0.0, J;
+  bool any = false;
+  if (pair_step(D, &ctl[row.r], row.r, row.kind, row.dsi, row.channel, row.local_channel, row.boundary,
+                row.owner, row.v0, row.v1, params[row.param], uold, ca, states, nch, k, stoch, J)) {
+    acc += (double)row.sign * J;
+    any = true;
+  }
+  for (int e = row.more_begin; e < row.more_end; e++) {
+    const FluxEntry en = entries[e];
+    const FluxPair pr = pairs[en.pair];
+    if (pair_step(D, &ctl[row.r], row.r, pr.kind, pr.dsi, pr.channel, pr.local_channel, pr.boundary, en.owner,
+                  pr.v0, pr.v1, params[pr.param], uold, ca, states, nch, k, stoch, J)) {
+      acc += (double)en.sign * J;
+      any = true;
     }
   }
-  // step epilogue, by the last block to finish
-  __shared__ bool last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int r = threadIdx.x; r < nreal; r += blockDim.x) {
-    RealCtl& C = ctl[r];
-    if (C.stopped) continue;
-    const RealDesc& D = descs[r];
-    const long long k = C.step;
-    const long long ti = k + 1;
-    const int open = C.open_count[(k + 1) & 1];
-    C.open_count[k & 1] = 0;
-    C.step = ti;
-    if (D.has_channels && D.tabort != 0) {
-      // abort rule (species.c:3476-3486) on the current openness
-      const double tt = (double)ti * D.dt;
-      if (open) {
-        C.last_closed = -1.0;
-      } else if (D.tabort >= 0) {
-        if (C.last_closed < 0) C.last_closed = tt;
-        if (tt - C.last_closed >= D.tabort) C.stopped = 1;
-      }
-    }
-    if (C.step >= D.total_steps) C.stopped = 1;
+  if (any && row.apply && (updated >> row.species & 1u)) {
+    float* unew = D.u[((cur >> row.species) & 1u) ^ 1u][row.species];
+    unew[row.v] = (float)((double)unew[row.v] + acc);
   }
-  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Step epilogue, one thread per realisation, after the boundary kernel: advance the
+// step counter, apply the abort rule (species.c:3476-3486) on the openness counted by
+// the boundary kernel, stop at the last step.
+__global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl, int nreal) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nreal) return;
+  RealCtl& C = ctl[r];
+  if (C.stopped) return;
+  const RealDesc& D = descs[r];
+  const long long k = C.step;
+  const long long ti = k + 1;
+  const int open = C.open_count[(k + 1) & 1];
+  C.open_count[k & 1] = 0;
+  C.step = ti;
+  if (D.has_channels && D.tabort != 0) {
+    const double tt = (double)ti * D.dt;
+    if (open) {
+      C.last_closed = -1.0;
+    } else if (D.tabort >= 0) {
+      if (C.last_closed < 0) C.last_closed = tt;
+      if (tt - C.last_closed >= D.tabort) C.stopped = 1;
+    }
+  }
+  if (C.step >= D.total_steps) C.stopped = 1;
 }
 
 // Output reductions: partial min / max / sum over a block for one species of one

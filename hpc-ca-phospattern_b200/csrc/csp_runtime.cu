@@ -98,7 +98,6 @@ struct csp_handle {
   FluxPair* d_pairs = nullptr;
   FluxParams* d_params = nullptr;
   unsigned char* d_states = nullptr;
-  unsigned* d_ticket = nullptr;
   int* d_err = nullptr;
   double* d_red = nullptr;
   double* d_red_out = nullptr;
@@ -350,13 +349,11 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
       cudaMalloc(&h->d_dom, dom_total + 256) != cudaSuccess ||
       cudaMalloc(&h->d_desc, n * sizeof(RealDesc)) != cudaSuccess ||
       cudaMalloc(&h->d_ctl, n * sizeof(RealCtl)) != cudaSuccess ||
-      cudaMalloc(&h->d_ticket, sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc(&h->d_err, sizeof(int)) != cudaSuccess) {
     csp_destroy(h);
     return fail(nullptr, CSP_ENOMEM, "device allocation of %.3f GB failed",
                 (field_total * 4.0 + dom_total) / 1e9);
   }
-  cudaMemsetAsync(h->d_ticket, 0, sizeof(unsigned), h->stream);
   cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream);
   cudaMemsetAsync(h->d_fields, 0, field_total * sizeof(float), h->stream);
   cudaMemsetAsync(h->d_dom, 0, dom_total + 256, h->stream);
@@ -697,15 +694,24 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     size_t j = i;
     FluxRow row;
     memset(&row, 0, sizeof row);
-    row.r = sides[i].r; row.species = sides[i].s; row.v = sides[i].v;
-    row.begin = (int)entries.size();
+    row.r = sides[i].r; row.v = sides[i].v;
+    row.species = (unsigned char)sides[i].s;
+    {
+      const FluxPair& p0 = pairs[sides[i].pair];
+      row.v0 = p0.v0; row.v1 = p0.v1; row.param = p0.param; row.channel = p0.channel;
+      row.local_channel = p0.local_channel; row.sign = sides[i].sign;
+      row.dsi = (unsigned char)p0.dsi; row.kind = (unsigned char)p0.kind; row.owner = (unsigned char)sides[i].owner;
+      row.boundary = (unsigned char)p0.boundary;
+    }
+    j = i + 1;
+    row.more_begin = (int)entries.size();
     while (j < sides.size() && sides[j].r == row.r && sides[j].s == row.species && sides[j].v == row.v) {
       FluxEntry en;
       en.pair = sides[j].pair; en.sign = sides[j].sign; en.owner = sides[j].owner; en.pad = 0;
       entries.push_back(en);
       j++;
     }
-    row.end = (int)entries.size();
+    row.more_end = (int)entries.size();
     // a voxel reset by the fixed-value rules after the step keeps its reset value
     const HostReal& rr = h->real[row.r];
     const RealDesc& D = rr.desc;
@@ -767,10 +773,11 @@ static void launch_voxels(csp_handle* h) {
 }
 
 static void launch_boundaries(csp_handle* h) {
-  const int blocks = std::max(1, (h->nrows + 255) / 256);
-  k_boundaries<<<blocks, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, h->nrows, h->d_entries, h->d_pairs,
-                                              h->d_params, h->d_states, std::max(h->nch, 1), h->n,
-                                              h->d_ticket);
+  if (h->nrows > 0)
+    k_boundaries<<<(h->nrows + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, h->nrows,
+                                                                h->d_entries, h->d_pairs, h->d_params, h->d_states,
+                                                                std::max(h->nch, 1));
+  k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->n);
 }
 
 static cudaError_t launch_step(csp_handle* h) {
@@ -1028,7 +1035,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   staged_release(h->plan);
   cudaFree(h->d_fields); cudaFree(h->d_dom); cudaFree(h->d_desc); cudaFree(h->d_ctl);
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
-  cudaFree(h->d_states); cudaFree(h->d_ticket); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
+  cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -217,17 +217,22 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
       const unsigned xval = (has_prev ? 16u : 0u) | (has_next ? 32u : 0u);
       float out[MS][4];
 
-      // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
+      // ---- domain bytes of the group and of its neighbourhood (4 per word) ----
       const unsigned wc = *reinterpret_cast<const unsigned*>(dc + p0);
+      unsigned wp = wc, wn = wc, wym = wc, wyp = wc, ezm = wc & 0xffu, ezp = wc >> 24;
+      if (group_ok) {
+        if (has_prev) wp = *reinterpret_cast<const unsigned*>(dp + p0);
+        if (has_next) wn = *reinterpret_cast<const unsigned*>(dnx + p0);
+        if (vzy[0] & 1u) ezm = dc[p0 - 1];
+        if (vzy[3] & 2u) ezp = dc[p0 + 4];
+        if (ymask_m) wym = ld_u32_any(dc + p0 - nz);
+        if (ymask_p) wyp = ld_u32_any(dc + p0 + nz);
+      }
+      // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
       const int d0 = wc & 0xff;
       const unsigned dw = (unsigned)d0 * 0x01010101u;
-      bool uni = group_ok && wc == dw && d0 <= DOMAIN_BITS;   // no flux pattern in the group
-      if (uni && has_prev) uni = *reinterpret_cast<const unsigned*>(dp + p0) == dw;
-      if (uni && has_next) uni = *reinterpret_cast<const unsigned*>(dnx + p0) == dw;
-      if (uni && (vzy[0] & 1u)) uni = dc[p0 - 1] == d0;
-      if (uni && (vzy[3] & 2u)) uni = dc[p0 + 4] == d0;
-      if (uni && ymask_m) uni = ((ld_u32_any(dc + p0 - nz) ^ dw) & ymask_m) == 0u;
-      if (uni && ymask_p) uni = ((ld_u32_any(dc + p0 + nz) ^ dw) & ymask_p) == 0u;
+      const bool uni = group_ok && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw && ezm == (unsigned)d0 &&
+                       ezp == (unsigned)d0 && ((wym ^ dw) & ymask_m) == 0u && ((wyp ^ dw) & ymask_p) == 0u;
 
       if (__builtin_expect(uni, 1)) {
         // ---- uniform group: constants once per group, one species at a time ----
@@ -316,6 +321,129 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             if ((vzy[j] | xval) != 63u) out[0][j] = D.init[d0][0];
         }
         // ---- stores (128-bit) ----
+#pragma unroll
+        for (int s = 0; s < MS; s++) {
+          if (!(lmask >> s & 1u)) continue;
+          float4* dst = reinterpret_cast<float4*>(D.u[((cur >> s) & 1u) ^ 1u][s] + (long long)x * D.P + p0);
+          *dst = make_float4(out[s][0], out[s][1], out[s][2], out[s][3]);
+        }
+#ifdef CSP_FUSE_DENSITY
+      } else if (group_ok) {
+#else
+      } else if (group_ok && (wc & 0xf8f8f8f8u) == 0u) {
+#endif
+        // ---- mixed-domain group: the same loads as above, domains and constants per voxel ----
+        float val[MS][4];
+        int dj[4], dnb[4][6];
+        bool unij[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const unsigned valid = vzy[j] | xval;
+          dj[j] = (wc >> (8 * j)) & DOMAIN_BITS;
+          const int zmb = j > 0 ? (int)(wc >> (8 * (j > 0 ? j - 1 : 0))) : (int)ezm;
+          const int zpb = j < 3 ? (int)(wc >> (8 * (j < 3 ? j + 1 : 3))) : (int)ezp;
+          const int raw[6] = {zmb, zpb, (int)(wym >> (8 * j)), (int)(wyp >> (8 * j)), (int)(wp >> (8 * j)),
+                              (int)(wn >> (8 * j))};
+          bool u = true;
+#pragma unroll
+          for (int k = 0; k < 6; k++) {
+            dnb[j][k] = (valid >> k & 1u) ? (raw[k] & DOMAIN_BITS) : dj[j];
+            u = u && dnb[j][k] == dj[j];
+          }
+          unij[j] = u;
+        }
+        int slot = 0;
+#pragma unroll
+        for (int s = 0; s < MS; s++) {
+          if (lmask >> s & 1u) {
+            const float4 a = *reinterpret_cast<const float4*>(fc + slot * so + p0);
+            val[s][0] = a.x; val[s][1] = a.y; val[s][2] = a.z; val[s][3] = a.w;
+            slot++;
+          } else {
+            val[s][0] = val[s][1] = val[s][2] = val[s][3] = 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; j++) out[s][j] = val[s][j];
+        }
+        slot = 0;
+#pragma unroll
+        for (int s = 0; s < MS; s++) {
+          if (!(lmask >> s & 1u)) continue;
+          const int so_s = slot * so;
+          slot++;
+          if (!(si.pre >> s & 1u)) continue;
+          const float* cs = D.coef[D.dsi_of[s]];
+          float4 vp = make_float4(0.f, 0.f, 0.f, 0.f), vn = vp;
+          if (has_prev) vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
+          if (has_next) vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
+          const float pv[4] = {vp.x, vp.y, vp.z, vp.w};
+          const float nv[4] = {vn.x, vn.y, vn.z, vn.w};
+          const float zm = fc[so_s + ((vzy[0] & 1u) ? p0 - 1 : p0)];
+          const float zp = fc[so_s + ((vzy[3] & 2u) ? p0 + 4 : p0 + 3)];
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const unsigned valid = vzy[j] | xval;
+            const float u = val[s][j];
+            const float ym = fc[so_s + ((valid & 4u) ? p0 + j - nz : p0 + j)];
+            const float yp = fc[so_s + ((valid & 8u) ? p0 + j + nz : p0 + j)];
+            float unb[6];
+            unb[0] = j > 0 ? val[s][j > 0 ? j - 1 : 0] : zm;
+            unb[1] = j < 3 ? val[s][j < 3 ? j + 1 : 3] : zp;
+            unb[2] = ym; unb[3] = yp; unb[4] = pv[j]; unb[5] = nv[j];
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++) unb[kk] = (valid >> kk & 1u) ? unb[kk] : u;
+            const float* c = cs + dj[j] * ND;
+            out[s][j] = unij[j] ? diffuse_uniform(c[dj[j]], u, unb) : diffuse_general(c, dnb[j], u, unb);
+#ifdef CSP_FUSE_DENSITY
+            const int pat = (int)((wc >> (8 * j + 3)) & 0x1fu);
+            if (pat) {   // density-boundary fluxes, as in voxel_update
+              double acc = 0.0;
+              bool any = false;
+#pragma unroll
+              for (int k = 0; k < 6; k++) {
+                const int code = D.fpat[pat][k];
+                if (!code) continue;
+                const int fs = (code & 0x7f) - 1;
+                if (D.fslot_species[fs] != s) continue;
+                const double self = (double)u, other = (double)unb[k];
+                if (code & 0x80) acc += pair_flux(D, fs, other, self);
+                else acc -= pair_flux(D, fs, self, other);
+                any = true;
+              }
+              if (any) out[s][j] = (float)((double)out[s][j] + acc);
+            }
+#endif
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int d = dj[j];
+          if (si.react) {
+            if (si.react_fast) {
+#pragma unroll
+              for (int s = 1; s < MS; s++) {
+                const int bi = D.rtab[d][s];
+                if (bi < 0) continue;
+                const int t = bi * D.nd + d;
+                const float dJ = buffer_dj(D.kon[t], D.koff[t], D.tot[t], D.dt_r, val[s][j], val[0][j]);
+                out[s][j] = __fadd_rn(out[s][j], dJ);
+                out[0][j] = __fsub_rn(out[0][j], dJ);
+              }
+            } else {
+              float vj[MS], oj[MS];
+#pragma unroll
+              for (int s = 0; s < MS; s++) { vj[s] = val[s][j]; oj[s] = out[s][j]; }
+              react_general<MS>(D, d, vj, oj, si.pre);
+#pragma unroll
+              for (int s = 0; s < MS; s++) out[s][j] = oj[s];
+            }
+          }
+          const unsigned fm = D.fixed_mask[d];
+#pragma unroll
+          for (int s = 0; s < MS; s++)
+            if (fm >> s & 1u) out[s][j] = D.init[d][s];
+          if (D.dirichlet && (vzy[j] | xval) != 63u) out[0][j] = D.init[d][0];
+        }
 #pragma unroll
         for (int s = 0; s < MS; s++) {
           if (!(lmask >> s & 1u)) continue;
