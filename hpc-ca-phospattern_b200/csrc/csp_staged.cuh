@@ -177,6 +177,9 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
     }
     // the y- word would start before the staged range only in the first chunk's first row
     const bool group_ok = all_in && (ymask_m == 0 || p0 - nz >= lob);
+    // the 4 positions lie in one row (same y, z-neighbours inside the group exist)
+    const bool one_row = (vzy[1] & vzy[2] & vzy[3] & 1u) != 0u;
+    const bool yvec = (nz & 3) == 0;      // y-neighbour rows are 16-byte aligned in the stage
 
     if (tid == 0) {
       fence_proxy_async();
@@ -231,8 +234,9 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
       // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
       const int d0 = wc & 0xff;
       const unsigned dw = (unsigned)d0 * 0x01010101u;
-      const bool uni = group_ok && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw && ezm == (unsigned)d0 &&
-                       ezp == (unsigned)d0 && ((wym ^ dw) & ymask_m) == 0u && ((wyp ^ dw) & ymask_p) == 0u;
+      const bool uni = group_ok && one_row && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw &&
+                       ezm == (unsigned)d0 && ezp == (unsigned)d0 && ((wym ^ dw) & ymask_m) == 0u &&
+                       ((wyp ^ dw) & ymask_p) == 0u;
 
       if (__builtin_expect(uni, 1)) {
         // ---- uniform group: constants once per group, one species at a time ----
@@ -258,25 +262,33 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           slot++;
           if (!(si.pre >> s & 1u)) continue;
           const float cdd = D.coef[D.dsi_of[s]][d0 * ND + d0];
-          float4 vp = make_float4(0.f, 0.f, 0.f, 0.f), vn = vp;
-          if (has_prev) vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
-          if (has_next) vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
+          // an out-of-box neighbour is read at the voxel itself (fp / fn point at the
+          // centre plane on the first / last plane; y and z addresses are clamped), so
+          // the values need no selection afterwards
+          const float4 vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
+          const float4 vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
           const float pv[4] = {vp.x, vp.y, vp.z, vp.w};
           const float nv[4] = {vn.x, vn.y, vn.z, vn.w};
           const float zm = fc[so_s + ((vzy[0] & 1u) ? p0 - 1 : p0)];
           const float zp = fc[so_s + ((vzy[3] & 2u) ? p0 + 4 : p0 + 3)];
+          const int pym = (vzy[0] & 4u) ? p0 - nz : p0, pyp = (vzy[0] & 8u) ? p0 + nz : p0;
+          float ym[4], yp[4];
+          if (yvec) {
+            const float4 a = *reinterpret_cast<const float4*>(fc + so_s + pym);
+            const float4 b = *reinterpret_cast<const float4*>(fc + so_s + pyp);
+            ym[0] = a.x; ym[1] = a.y; ym[2] = a.z; ym[3] = a.w;
+            yp[0] = b.x; yp[1] = b.y; yp[2] = b.z; yp[3] = b.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) { ym[j] = fc[so_s + pym + j]; yp[j] = fc[so_s + pyp + j]; }
+          }
 #pragma unroll
           for (int j = 0; j < 4; j++) {
-            const unsigned valid = vzy[j] | xval;
             const float u = val[s][j];
-            const float ym = fc[so_s + ((valid & 4u) ? p0 + j - nz : p0 + j)];
-            const float yp = fc[so_s + ((valid & 8u) ? p0 + j + nz : p0 + j)];
             float unb[6];
             unb[0] = j > 0 ? val[s][j > 0 ? j - 1 : 0] : zm;
             unb[1] = j < 3 ? val[s][j < 3 ? j + 1 : 3] : zp;
-            unb[2] = ym; unb[3] = yp; unb[4] = pv[j]; unb[5] = nv[j];
-#pragma unroll
-            for (int kk = 0; kk < 6; kk++) unb[kk] = (valid >> kk & 1u) ? unb[kk] : u;
+            unb[2] = ym[j]; unb[3] = yp[j]; unb[4] = pv[j]; unb[5] = nv[j];
             out[s][j] = diffuse_uniform(cdd, u, unb);
           }
         }
