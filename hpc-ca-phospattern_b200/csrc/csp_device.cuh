@@ -34,7 +34,11 @@ struct RealDesc {
   unsigned reaction_flag_mask;       // species flagged after a reaction step (species.c:1695-1699)
   float dt_r;                        // dt * reaction_substep (species.c:1666)
   float coef[NS][ND * ND];           // dt*substeps*sigma/h^2 tables (species.c:1545-1560)
-  float kon[NB * ND], koff[NB * ND], tot[NB * ND];   // [bi*nd + di] (species.c:249-253)
+  // buffer constants [bi*nd + di] (species.c:249-253); the rates are stored multiplied by
+  // the reaction time step dt_r
+  float kon_dt[NB * ND], koff_dt[NB * ND], tot[NB * ND];
+  float cdiag[ND][NS];               // coef of species s between two voxels of domain d (0: not diffusive)
+  float4 rk[ND][NS];                 // fast reactions: {kon_dt, koff_dt, tot, 1} of the buffer bound to s in d, or 0
   unsigned char bsp0[NB * ND], bsp1[NB * ND];
   unsigned char fixed_mask[ND];      // bit s: species s is fixed in domain d
   signed char dsi_of[NS];            // diffusive index of species s, or -1

@@ -24,10 +24,11 @@ enum : int { ERR_BOUNDS = 1, ERR_TIMEOUT = 2 };
 // path c*(sum_n u_n - 6u) + u (kernel_generic.cpp:529-533) in the form u + c*sum_n(u_n - u);
 // out-of-box neighbours carry u_n = u and add nothing.
 __device__ __forceinline__ float diffuse_uniform(float c, float u, const float (&un)[6]) {
-  float a = __fsub_rn(un[0], u);
-#pragma unroll
-  for (int k = 1; k < 6; k++) a = __fadd_rn(a, __fsub_rn(un[k], u));
-  return __fmaf_rn(c, a, u);
+  // per axis (u_- + u_+) - 2u: exact zero in a uniform field, one rounding per axis
+  const float az = __fmaf_rn(-2.f, u, __fadd_rn(un[0], un[1]));
+  const float ay = __fmaf_rn(-2.f, u, __fadd_rn(un[2], un[3]));
+  const float ax = __fmaf_rn(-2.f, u, __fadd_rn(un[4], un[5]));
+  return __fmaf_rn(c, __fadd_rn(__fadd_rn(az, ay), ax), u);
 }
 
 // General neighbourhood: u + sum_n c[d][d_n]*(u_n - u) (species.c:1572-1611, 1282-1498).
@@ -38,10 +39,10 @@ __device__ __forceinline__ float diffuse_general(const float* c, const int (&dn)
   return __fadd_rn(u, a);
 }
 
-// dt_r * J for one buffer, J = k_on*(tot-b)*ca - k_off*b (kernel_generic.cpp:495-507).
-__device__ __forceinline__ float buffer_dj(float kon, float koff, float tot, float dt_r, float b, float ca) {
-  const float J = __fsub_rn(__fmul_rn(__fmul_rn(kon, __fsub_rn(tot, b)), ca), __fmul_rn(koff, b));
-  return __fmul_rn(dt_r, J);
+// dt_r * J for one buffer, J = k_on*(tot-b)*ca - k_off*b (kernel_generic.cpp:495-507), with
+// the rates given premultiplied by dt_r.
+__device__ __forceinline__ float buffer_dj(float kon_dt, float koff_dt, float tot, float b, float ca) {
+  return __fmaf_rn(__fmul_rn(kon_dt, __fsub_rn(tot, b)), ca, -__fmul_rn(koff_dt, b));
 }
 
 // General buffer reactions: the reference's assign-or-accumulate rule, per buffer in
@@ -54,7 +55,7 @@ __device__ __forceinline__ void react_general(const RealDesc& D, int d, const fl
     const int t = bi * D.nd + d;
     const int s0 = D.bsp0[t], s1 = D.bsp1[t];
     const float b0 = sel(val, s0), b1 = sel(val, s1);
-    const float dJ = buffer_dj(D.kon[t], D.koff[t], D.tot[t], D.dt_r, b0, b1);
+    const float dJ = buffer_dj(D.kon_dt[t], D.koff_dt[t], D.tot[t], b0, b1);
     if (pre >> s0 & 1u) put(out, s0, __fadd_rn(sel(out, s0), dJ)); else put(out, s0, __fadd_rn(b0, dJ));
     if (pre >> s1 & 1u) put(out, s1, __fsub_rn(sel(out, s1), dJ)); else put(out, s1, __fsub_rn(b1, dJ));
   }
@@ -154,10 +155,9 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
       const float ca = val[0];
 #pragma unroll
       for (int s = 1; s < N; s++) {
-        const int bi = D.rtab[d][s];
-        if (bi < 0) continue;
-        const int t = bi * D.nd + d;
-        const float dJ = buffer_dj(D.kon[t], D.koff[t], D.tot[t], D.dt_r, val[s], ca);
+        const float4 k = D.rk[d][s];
+        if (k.w == 0.f) continue;
+        const float dJ = buffer_dj(k.x, k.y, k.z, val[s], ca);
         out[s] = __fadd_rn(out[s], dJ);
         out[0] = __fsub_rn(out[0], dJ);
       }

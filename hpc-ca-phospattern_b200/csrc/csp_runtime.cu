@@ -389,7 +389,9 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
       for (int a = 0; a < ND; a++)
         for (int b = 0; b < ND; b++) D.coef[k][a * ND + b] = (float)d.coef[k][a][b];
     for (int t = 0; t < NB * ND; t++) {
-      D.kon[t] = (float)d.kon[t]; D.koff[t] = (float)d.koff[t]; D.tot[t] = (float)d.tot[t];
+      D.kon_dt[t] = (float)(d.kon[t] * (d.dt * d.reaction_substep));
+      D.koff_dt[t] = (float)(d.koff[t] * (d.dt * d.reaction_substep));
+      D.tot[t] = (float)d.tot[t];
       D.bsp0[t] = d.bsp0[t]; D.bsp1[t] = d.bsp1[t];
     }
     // per-species lookup tables of the voxel kernels
@@ -403,6 +405,17 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         const int s0 = m.domain[dd].bsp0[bi], s1 = m.domain[dd].bsp1[bi];
         if (s1 != 0 || s0 == 0 || D.rtab[dd][s0] >= 0) D.react_fast = 0;
         else D.rtab[dd][s0] = (signed char)bi;
+      }
+    for (int dd = 0; dd < ND; dd++)
+      for (int s = 0; s < NS; s++) {
+        D.cdiag[dd][s] = (dd < nd && D.dsi_of[s] >= 0) ? D.coef[D.dsi_of[s]][dd * ND + dd] : 0.f;
+        const int bi = D.rtab[dd][s];
+        if (bi >= 0) {
+          const int t = bi * nd + dd;
+          D.rk[dd][s] = make_float4(D.kon_dt[t], D.koff_dt[t], D.tot[t], 1.f);
+        } else {
+          D.rk[dd][s] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
       }
     for (int i = 0; i < m.num_fixed_domain_species; i++) {
       const int dd = m.fixed_domain_species[2 * i], s = m.fixed_domain_species[2 * i + 1];

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           const int so_s = slot * so;
           slot++;
           if (!(si.pre >> s & 1u)) continue;
-          const float cdd = D.coef[D.dsi_of[s]][d0 * ND + d0];
+          const float cdd = D.cdiag[d0][s];
           // an out-of-box neighbour is read at the voxel itself (fp / fn point at the
           // centre plane on the first / last plane; y and z addresses are clamped), so
           // the values need no selection afterwards
@@ -296,13 +296,11 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           if (si.react_fast) {
 #pragma unroll
             for (int s = 1; s < MS; s++) {
-              const int bi = D.rtab[d0][s];
-              if (bi < 0) continue;
-              const int t = bi * D.nd + d0;
-              const float kon = D.kon[t], koff = D.koff[t], tot = D.tot[t], dtr = D.dt_r;
+              const float4 kk = D.rk[d0][s];
+              if (kk.w == 0.f) continue;
 #pragma unroll
               for (int j = 0; j < 4; j++) {
-                const float dJ = buffer_dj(kon, koff, tot, dtr, val[s][j], val[0][j]);
+                const float dJ = buffer_dj(kk.x, kk.y, kk.z, val[s][j], val[0][j]);
                 out[s][j] = __fadd_rn(out[s][j], dJ);
                 out[0][j] = __fsub_rn(out[0][j], dJ);
               }
@@ -434,10 +432,9 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             if (si.react_fast) {
 #pragma unroll
               for (int s = 1; s < MS; s++) {
-                const int bi = D.rtab[d][s];
-                if (bi < 0) continue;
-                const int t = bi * D.nd + d;
-                const float dJ = buffer_dj(D.kon[t], D.koff[t], D.tot[t], D.dt_r, val[s][j], val[0][j]);
+                const float4 kk = D.rk[d][s];
+                if (kk.w == 0.f) continue;
+                const float dJ = buffer_dj(kk.x, kk.y, kk.z, val[s][j], val[0][j]);
                 out[s][j] = __fadd_rn(out[s][j], dJ);
                 out[0][j] = __fsub_rn(out[0][j], dJ);
               }
