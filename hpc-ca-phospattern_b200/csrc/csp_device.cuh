@@ -20,6 +20,8 @@ constexpr int NS = CSP_MAX_SPECIES;
 constexpr int NB = CSP_MAX_BUFFERS;
 constexpr int PLANE_ALIGN = 128;
 constexpr int DOMAIN_BITS = 7;      // domain id = domain byte & DOMAIN_BITS
+constexpr int CLASS_L = 1024;       // plane positions per chunk of the chunk class table
+constexpr unsigned char CLASS_MIXED = 0xff;
 
 enum FluxKind : int { FLUX_NONE = 0, FLUX_RYR = 1, FLUX_P_RYR = 2, FLUX_SERCA = 3 };
 
@@ -55,6 +57,12 @@ struct RealDesc {
   float init[ND][NS];
   float* u[2][NS];                   // the two buffers of every species
   const unsigned char* dom;          // [nx][P]
+  // Chunk class table [nx][ncls]: for plane x and chunk c (positions c*CLASS_L ...
+  // c*CLASS_L + CLASS_L - 1), the domain id when every voxel of planes x-1..x+1 within
+  // nz positions of the chunk lies in that domain with no flux pattern and nz % 4 == 0,
+  // else CLASS_MIXED.
+  const unsigned char* cls;
+  int ncls;
   long long total_steps;
   double dt, h, tabort;
   unsigned long long seed;           // Philox key of the realisation's channel draws

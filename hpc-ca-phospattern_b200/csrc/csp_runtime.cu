@@ -42,6 +42,7 @@ struct HostReal {
   size_t field_elems;             // n0*P
   int perm[3];                    // device axis i holds physical axis perm[i]
   int nphys[3];                   // species voxels per physical axis
+  std::vector<unsigned char> cls; // chunk class table (RealDesc::cls)
   // padded linear device index of physical species voxel (x, y, z)
   long long dev_index(int x, int y, int z) const {
     const int c[3] = {x, y, z};
@@ -80,6 +81,32 @@ static void choose_axes(const csp_model& m, int perm[3]) {
   perm[2] = swap ? rest[0] : rest[1];
 }
 
+// Chunk class table of one realisation from its device-layout domain bytes (see
+// RealDesc::cls).
+static void chunk_classes(const RealDesc& D, const std::vector<unsigned char>& dom, std::vector<unsigned char>& cls) {
+  const int nch = (D.plane + CLASS_L - 1) / CLASS_L;
+  cls.assign((size_t)D.nx * nch, CLASS_MIXED);
+  if (D.nz % 4 != 0) return;
+  std::vector<unsigned char> pu((size_t)D.nx * nch, CLASS_MIXED);
+  for (int q = 0; q < D.nx; q++)
+    for (int c = 0; c < nch; c++) {
+      const int lo = std::max(0, c * CLASS_L - D.nz), hi = std::min(D.plane, c * CLASS_L + CLASS_L + D.nz);
+      const unsigned char* row = dom.data() + (size_t)q * D.P;
+      const unsigned char d = row[lo];
+      bool same = d <= DOMAIN_BITS;
+      for (int p = lo + 1; same && p < hi; p++) same = row[p] == d;
+      if (same) pu[(size_t)q * nch + c] = d;
+    }
+  for (int x = 0; x < D.nx; x++)
+    for (int c = 0; c < nch; c++) {
+      const unsigned char d = pu[(size_t)x * nch + c];
+      if (d == CLASS_MIXED) continue;
+      if (x > 0 && pu[(size_t)(x - 1) * nch + c] != d) continue;
+      if (x + 1 < D.nx && pu[(size_t)(x + 1) * nch + c] != d) continue;
+      cls[(size_t)x * nch + c] = d;
+    }
+}
+
 }  // namespace
 
 struct csp_handle {
@@ -91,6 +118,7 @@ struct csp_handle {
   // device memory
   float* d_fields = nullptr;
   unsigned char* d_dom = nullptr;
+  unsigned char* d_cls = nullptr;
   RealDesc* d_desc = nullptr;
   RealCtl* d_ctl = nullptr;
   FluxRow* d_rows = nullptr;
@@ -621,6 +649,8 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
       }
     }
     cudaMemcpyAsync((void*)D.dom, hostd.data(), hr.field_elems, cudaMemcpyHostToDevice, h->stream);
+    chunk_classes(D, hostd, hr.cls);
+    D.ncls = (D.plane + CLASS_L - 1) / CLASS_L;
     cudaStreamSynchronize(h->stream);
     // initial channel states (BoundaryFluxes_init_stochastic_boundaries, boundaryfluxes.c:544-605)
     int ndiscrete = 0;
@@ -749,8 +779,21 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
   };
   std::vector<unsigned char> st2(2 * (size_t)std::max(h->nch, 1), 0);
   std::copy(states0.begin(), states0.end(), st2.begin());
+  size_t cls_total = 0;
+  for (int r = 0; r < n; r++) cls_total += h->real[r].cls.size();
+  std::vector<unsigned char> cls_all;
+  cls_all.reserve(cls_total);
+  for (int r = 0; r < n; r++) cls_all.insert(cls_all.end(), h->real[r].cls.begin(), h->real[r].cls.end());
+  if (!upload((void**)&h->d_cls, cls_all.empty() ? nullptr : cls_all.data(), cls_all.size())) {
+    csp_destroy(h);
+    return fail(nullptr, CSP_ENOMEM, "device allocation of the chunk class table failed");
+  }
   std::vector<RealDesc> descs(n);
-  for (int r = 0; r < n; r++) descs[r] = h->real[r].desc;
+  for (int r = 0, off = 0; r < n; r++) {
+    h->real[r].desc.cls = h->d_cls + off;
+    off += (int)h->real[r].cls.size();
+    descs[r] = h->real[r].desc;
+  }
   bool ok = upload((void**)&h->d_rows, rows.empty() ? nullptr : rows.data(), rows.size() * sizeof(FluxRow)) &&
             upload((void**)&h->d_entries, entries.empty() ? nullptr : entries.data(), entries.size() * sizeof(FluxEntry)) &&
             upload((void**)&h->d_pairs, pairs.empty() ? nullptr : pairs.data(), pairs.size() * sizeof(FluxPair)) &&
@@ -1046,7 +1089,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   staged_release(h->plan);
-  cudaFree(h->d_fields); cudaFree(h->d_dom); cudaFree(h->d_desc); cudaFree(h->d_ctl);
+  cudaFree(h->d_fields); cudaFree(h->d_dom); cudaFree(h->d_cls); cudaFree(h->d_desc); cudaFree(h->d_ctl);
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
   cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
   if (h->ev0) cudaEventDestroy(h->ev0);

@@ -180,6 +180,8 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
     // the 4 positions lie in one row (same y, z-neighbours inside the group exist)
     const bool one_row = (vzy[1] & vzy[2] & vzy[3] & 1u) != 0u;
     const bool yvec = (nz & 3) == 0;      // y-neighbour rows are 16-byte aligned in the stage
+    // class bytes of this chunk (one per plane), when the chunk matches the class table's
+    const unsigned char* cls_row = (g.L == CLASS_L && D.cls) ? D.cls + c : nullptr;
 
     if (tid == 0) {
       fence_proxy_async();
@@ -220,23 +222,34 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
       const unsigned xval = (has_prev ? 16u : 0u) | (has_next ? 32u : 0u);
       float out[MS][4];
 
-      // ---- domain bytes of the group and of its neighbourhood (4 per word) ----
-      const unsigned wc = *reinterpret_cast<const unsigned*>(dc + p0);
-      unsigned wp = wc, wn = wc, wym = wc, wyp = wc, ezm = wc & 0xffu, ezp = wc >> 24;
-      if (group_ok) {
-        if (has_prev) wp = *reinterpret_cast<const unsigned*>(dp + p0);
-        if (has_next) wn = *reinterpret_cast<const unsigned*>(dnx + p0);
-        if (vzy[0] & 1u) ezm = dc[p0 - 1];
-        if (vzy[3] & 2u) ezp = dc[p0 + 4];
-        if (ymask_m) wym = ld_u32_any(dc + p0 - nz);
-        if (ymask_p) wyp = ld_u32_any(dc + p0 + nz);
+      // ---- chunk class: the whole chunk neighbourhood in one domain (CTA-uniform) ----
+      const int pc = cls_row ? __ldg(cls_row + (size_t)x * D.ncls) : CLASS_MIXED;
+      unsigned wc, wp, wn, wym, wyp, ezm, ezp;
+      int d0;
+      bool uni;
+      if (pc != CLASS_MIXED) {
+        d0 = pc;
+        uni = all_in;
+        wc = wp = wn = wym = wyp = ezm = ezp = 0u;
+      } else {
+        // ---- domain bytes of the group and of its neighbourhood (4 per word) ----
+        wc = *reinterpret_cast<const unsigned*>(dc + p0);
+        wp = wc; wn = wc; wym = wc; wyp = wc; ezm = wc & 0xffu; ezp = wc >> 24;
+        if (group_ok) {
+          if (has_prev) wp = *reinterpret_cast<const unsigned*>(dp + p0);
+          if (has_next) wn = *reinterpret_cast<const unsigned*>(dnx + p0);
+          if (vzy[0] & 1u) ezm = dc[p0 - 1];
+          if (vzy[3] & 2u) ezp = dc[p0 + 4];
+          if (ymask_m) wym = ld_u32_any(dc + p0 - nz);
+          if (ymask_p) wyp = ld_u32_any(dc + p0 + nz);
+        }
+        // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
+        d0 = wc & 0xff;
+        const unsigned dw = (unsigned)d0 * 0x01010101u;
+        uni = group_ok && one_row && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw &&
+              ezm == (unsigned)d0 && ezp == (unsigned)d0 && ((wym ^ dw) & ymask_m) == 0u &&
+              ((wyp ^ dw) & ymask_p) == 0u;
       }
-      // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
-      const int d0 = wc & 0xff;
-      const unsigned dw = (unsigned)d0 * 0x01010101u;
-      const bool uni = group_ok && one_row && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw &&
-                       ezm == (unsigned)d0 && ezp == (unsigned)d0 && ((wym ^ dw) & ymask_m) == 0u &&
-                       ((wyp ^ dw) & ymask_p) == 0u;
 
       if (__builtin_expect(uni, 1)) {
         // ---- uniform group: constants once per group, one species at a time ----
