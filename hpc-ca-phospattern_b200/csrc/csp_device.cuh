@@ -59,8 +59,7 @@ struct RealDesc {
   const unsigned char* dom;          // [nx][P]
   // Chunk class table [nx][ncls]: for plane x and chunk c (positions c*CLASS_L ...
   // c*CLASS_L + CLASS_L - 1), the domain id when every voxel of planes x-1..x+1 within
-  // nz positions of the chunk lies in that domain with no flux pattern and nz % 4 == 0,
-  // else CLASS_MIXED.
+  // nz positions of the chunk lies in that domain with no flux pattern, else CLASS_MIXED.
   const unsigned char* cls;
   int ncls;
   long long total_steps;

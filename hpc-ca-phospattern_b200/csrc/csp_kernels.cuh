@@ -21,8 +21,8 @@ enum : int { ERR_BOUNDS = 1, ERR_TIMEOUT = 2 };
 // the code paths that share it) ----
 
 // Uniform neighbourhood (all six neighbours in the voxel's domain): the reference's fast
-// path c*(sum_n u_n - 6u) + u (kernel_generic.cpp:529-533) in the form u + c*sum_n(u_n - u);
-// out-of-box neighbours carry u_n = u and add nothing.
+// path c*(sum_n u_n - 6u) + u (kernel_generic.cpp:529-533) in the form
+// u + c*sum_axes((u_- + u_+) - 2u); out-of-box neighbours carry u_n = u and add nothing.
 __device__ __forceinline__ float diffuse_uniform(float c, float u, const float (&un)[6]) {
   // per axis (u_- + u_+) - 2u: exact zero in a uniform field, one rounding per axis
   const float az = __fmaf_rn(-2.f, u, __fadd_rn(un[0], un[1]));
@@ -31,12 +31,62 @@ __device__ __forceinline__ float diffuse_uniform(float c, float u, const float (
   return __fmaf_rn(c, __fadd_rn(__fadd_rn(az, ay), ax), u);
 }
 
-// General neighbourhood: u + sum_n c[d][d_n]*(u_n - u) (species.c:1572-1611, 1282-1498).
-__device__ __forceinline__ float diffuse_general(const float* c, const int (&dn)[6], float u, const float (&un)[6]) {
+// General neighbourhood: u + sum_n c_n*(u_n - u) with c_n = c[d][d_n] (species.c:1572-1611,
+// 1282-1498).
+__device__ __forceinline__ float diffuse_coef6(const float (&c6)[6], float u, const float (&un)[6]) {
   float a = 0.f;
 #pragma unroll
-  for (int k = 0; k < 6; k++) a = __fmaf_rn(c[dn[k]], __fsub_rn(un[k], u), a);
+  for (int k = 0; k < 6; k++) a = __fmaf_rn(c6[k], __fsub_rn(un[k], u), a);
   return __fadd_rn(u, a);
+}
+__device__ __forceinline__ float diffuse_general(const float* c, const int (&dn)[6], float u, const float (&un)[6]) {
+  const float c6[6] = {c[dn[0]], c[dn[1]], c[dn[2]], c[dn[3]], c[dn[4]], c[dn[5]]};
+  return diffuse_coef6(c6, u, un);
+}
+
+// ---- two FP32 lanes per instruction (sm_100 add/sub/mul/fma .rn.f32x2): every lane is
+// rounded exactly as the scalar __fadd_rn / __fsub_rn / __fmul_rn / __fmaf_rn ----
+struct F2 {
+  unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float lo, float hi) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_split(F2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ F2 f2_add(F2 a, F2 b) {
+  F2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_sub(F2 a, F2 b) {
+  F2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_mul(F2 a, F2 b) {
+  F2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ F2 f2_fma(F2 a, F2 b, F2 c) {
+  F2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+// diffuse_uniform on two voxels: zs = z- + z+, ys, xs the other axis sums.
+__device__ __forceinline__ F2 diffuse_uniform2(F2 c, F2 m2, F2 u, F2 zs, F2 ys, F2 xs) {
+  const F2 az = f2_fma(m2, u, zs), ay = f2_fma(m2, u, ys), ax = f2_fma(m2, u, xs);
+  return f2_fma(c, f2_add(f2_add(az, ay), ax), u);
+}
+
+// buffer_dj on two voxels, nkoff_dt = -koff_dt.
+__device__ __forceinline__ F2 buffer_dj2(F2 kon_dt, F2 nkoff_dt, F2 tot, F2 b, F2 ca) {
+  return f2_fma(f2_mul(kon_dt, f2_sub(tot, b)), ca, f2_mul(nkoff_dt, b));
 }
 
 // dt_r * J for one buffer, J = k_on*(tot-b)*ca - k_off*b (kernel_generic.cpp:495-507), with

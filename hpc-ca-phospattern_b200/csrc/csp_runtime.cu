@@ -54,8 +54,7 @@ struct HostReal {
 // same no-flux rule, so the kernels may hold the field in any axis order.  The marching
 // axis (device axis 0) is the physical axis crossed by the most domain changes, so that
 // domain-boundary sheets (cleft, jSR, network SR at fixed z in a dyad) become whole
-// planes and the voxels sharing a warp share a neighbourhood type; the contiguous axis
-// (device axis 2) is the one with the fewest changes.
+// planes and the voxels sharing a warp share a neighbourhood type.
 static void choose_axes(const csp_model& m, int perm[3]) {
   long long ch[3] = {0, 0, 0};
   const int N0 = m.N[0], N1 = m.N[1], N2 = m.N[2];
@@ -70,12 +69,14 @@ static void choose_axes(const csp_model& m, int perm[3]) {
   int a0 = 0;
   for (int a = 1; a < 3; a++)
     if (ch[a] > ch[a0]) a0 = a;
-  if (ch[a0] == 0) { perm[0] = 0; perm[1] = 1; perm[2] = 2; return; }
   int rest[2], k = 0;
   for (int a = 0; a < 3; a++)
     if (a != a0) rest[k++] = a;
-  // fewest changes last; on a tie keep the physical order
-  const bool swap = ch[rest[0]] < ch[rest[1]];
+  // contiguous last: a length that is a multiple of 4 (4-voxel groups then never straddle
+  // a row), then the fewest changes; on a tie keep the physical order
+  const int n[3] = {N0, N1, N2};
+  const bool a4 = n[rest[0]] % 4 == 0, b4 = n[rest[1]] % 4 == 0;
+  const bool swap = a4 != b4 ? a4 : ch[rest[0]] < ch[rest[1]];
   perm[0] = a0;
   perm[1] = swap ? rest[1] : rest[0];
   perm[2] = swap ? rest[0] : rest[1];
@@ -86,7 +87,6 @@ static void choose_axes(const csp_model& m, int perm[3]) {
 static void chunk_classes(const RealDesc& D, const std::vector<unsigned char>& dom, std::vector<unsigned char>& cls) {
   const int nch = (D.plane + CLASS_L - 1) / CLASS_L;
   cls.assign((size_t)D.nx * nch, CLASS_MIXED);
-  if (D.nz % 4 != 0) return;
   std::vector<unsigned char> pu((size_t)D.nx * nch, CLASS_MIXED);
   for (int q = 0; q < D.nx; q++)
     for (int c = 0; c < nch; c++) {

@@ -177,9 +177,9 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
     }
     // the y- word would start before the staged range only in the first chunk's first row
     const bool group_ok = all_in && (ymask_m == 0 || p0 - nz >= lob);
-    // the 4 positions lie in one row (same y, z-neighbours inside the group exist)
-    const bool one_row = (vzy[1] & vzy[2] & vzy[3] & 1u) != 0u;
-    const bool yvec = (nz & 3) == 0;      // y-neighbour rows are 16-byte aligned in the stage
+    // rows of a multiple of 4 voxels: every group lies in one row and its y-neighbour
+    // rows are 16-byte aligned in the stage
+    const bool yvec = (nz & 3) == 0;
     // class bytes of this chunk (one per plane), when the chunk matches the class table's
     const unsigned char* cls_row = (g.L == CLASS_L && D.cls) ? D.cls + c : nullptr;
 
@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
 
     if (x0 > 0) wait_plane(x0 - 1);
     wait_plane(x0);
+    int pc_next = cls_row ? __ldg(cls_row + (size_t)x0 * D.ncls) : CLASS_MIXED;
     for (int x = x0; x < x1; x++) {
       const bool has_prev = x > 0, has_next = x + 1 < nx;
       if (has_next) wait_plane(x + 1);
@@ -222,8 +223,10 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
       const unsigned xval = (has_prev ? 16u : 0u) | (has_next ? 32u : 0u);
       float out[MS][4];
 
-      // ---- chunk class: the whole chunk neighbourhood in one domain (CTA-uniform) ----
-      const int pc = cls_row ? __ldg(cls_row + (size_t)x * D.ncls) : CLASS_MIXED;
+      // ---- chunk class: the whole chunk neighbourhood in one domain (CTA-uniform);
+      // the next plane's byte is fetched one plane ahead ----
+      const int pc = pc_next;
+      if (cls_row && x + 1 < x1) pc_next = __ldg(cls_row + (size_t)(x + 1) * D.ncls);
       unsigned wc, wp, wn, wym, wyp, ezm, ezp;
       int d0;
       bool uni;
@@ -246,14 +249,16 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
         // ---- is the whole 4-voxel group and its neighbourhood in one domain? ----
         d0 = wc & 0xff;
         const unsigned dw = (unsigned)d0 * 0x01010101u;
-        uni = group_ok && one_row && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw &&
+        uni = group_ok && wc == dw && d0 <= DOMAIN_BITS && wp == dw && wn == dw &&
               ezm == (unsigned)d0 && ezp == (unsigned)d0 && ((wym ^ dw) & ymask_m) == 0u &&
               ((wyp ^ dw) & ymask_p) == 0u;
       }
 
       if (__builtin_expect(uni, 1)) {
-        // ---- uniform group: constants once per group, one species at a time ----
+        // ---- uniform group: constants once per group, one species at a time, voxel
+        // pairs (0,1) and (2,3) in two-lane FP32 ----
         float val[MS][4];
+        F2 o2[MS][2];
         int slot = 0;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -264,9 +269,10 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           } else {
             val[s][0] = val[s][1] = val[s][2] = val[s][3] = 0.f;
           }
-#pragma unroll
-          for (int j = 0; j < 4; j++) out[s][j] = val[s][j];
+          o2[s][0] = f2(val[s][0], val[s][1]);
+          o2[s][1] = f2(val[s][2], val[s][3]);
         }
+        const F2 m2 = f2(-2.f, -2.f);
         slot = 0;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -280,45 +286,61 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           // the values need no selection afterwards
           const float4 vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
           const float4 vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
-          const float pv[4] = {vp.x, vp.y, vp.z, vp.w};
-          const float nv[4] = {vn.x, vn.y, vn.z, vn.w};
           const float zm = fc[so_s + ((vzy[0] & 1u) ? p0 - 1 : p0)];
           const float zp = fc[so_s + ((vzy[3] & 2u) ? p0 + 4 : p0 + 3)];
-          const int pym = (vzy[0] & 4u) ? p0 - nz : p0, pyp = (vzy[0] & 8u) ? p0 + nz : p0;
-          float ym[4], yp[4];
+          const float* v = val[s];
+          float4 ym, yp;
+          F2 zs0, zs1;
           if (yvec) {
-            const float4 a = *reinterpret_cast<const float4*>(fc + so_s + pym);
-            const float4 b = *reinterpret_cast<const float4*>(fc + so_s + pyp);
-            ym[0] = a.x; ym[1] = a.y; ym[2] = a.z; ym[3] = a.w;
-            yp[0] = b.x; yp[1] = b.y; yp[2] = b.z; yp[3] = b.w;
+            // rows of a multiple of 4 voxels: the group lies in one row
+            const int pym = (vzy[0] & 4u) ? p0 - nz : p0, pyp = (vzy[0] & 8u) ? p0 + nz : p0;
+            ym = *reinterpret_cast<const float4*>(fc + so_s + pym);
+            yp = *reinterpret_cast<const float4*>(fc + so_s + pyp);
+            zs0 = f2(__fadd_rn(zm, v[1]), __fadd_rn(v[0], v[2]));
+            zs1 = f2(__fadd_rn(v[1], v[3]), __fadd_rn(v[2], zp));
           } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++) { ym[j] = fc[so_s + pym + j]; yp[j] = fc[so_s + pyp + j]; }
+            // the group may straddle a row end: y and z neighbours per voxel
+            const float* r = fc + so_s + p0;
+            ym = make_float4(r[(vzy[0] & 4u) ? -nz : 0], r[(vzy[1] & 4u) ? 1 - nz : 1], r[(vzy[2] & 4u) ? 2 - nz : 2],
+                             r[(vzy[3] & 4u) ? 3 - nz : 3]);
+            yp = make_float4(r[(vzy[0] & 8u) ? nz : 0], r[(vzy[1] & 8u) ? 1 + nz : 1], r[(vzy[2] & 8u) ? 2 + nz : 2],
+                             r[(vzy[3] & 8u) ? 3 + nz : 3]);
+            const float zm1 = (vzy[1] & 1u) ? v[0] : v[1], zm2 = (vzy[2] & 1u) ? v[1] : v[2];
+            const float zm3 = (vzy[3] & 1u) ? v[2] : v[3];
+            const float zp0 = (vzy[0] & 2u) ? v[1] : v[0], zp1 = (vzy[1] & 2u) ? v[2] : v[1];
+            const float zp2 = (vzy[2] & 2u) ? v[3] : v[2];
+            zs0 = f2(__fadd_rn(zm, zp0), __fadd_rn(zm1, zp1));
+            zs1 = f2(__fadd_rn(zm2, zp2), __fadd_rn(zm3, zp));
           }
+          const F2 c2 = f2(cdd, cdd);
+          const F2 ys0 = f2_add(f2(ym.x, ym.y), f2(yp.x, yp.y)), ys1 = f2_add(f2(ym.z, ym.w), f2(yp.z, yp.w));
+          const F2 xs0 = f2_add(f2(vp.x, vp.y), f2(vn.x, vn.y)), xs1 = f2_add(f2(vp.z, vp.w), f2(vn.z, vn.w));
+          o2[s][0] = diffuse_uniform2(c2, m2, f2(v[0], v[1]), zs0, ys0, xs0);
+          o2[s][1] = diffuse_uniform2(c2, m2, f2(v[2], v[3]), zs1, ys1, xs1);
+        }
+        float out[MS][4];
+        if (si.react && si.react_fast) {
+          const F2 ca0 = f2(val[0][0], val[0][1]), ca1 = f2(val[0][2], val[0][3]);
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const float u = val[s][j];
-            float unb[6];
-            unb[0] = j > 0 ? val[s][j > 0 ? j - 1 : 0] : zm;
-            unb[1] = j < 3 ? val[s][j < 3 ? j + 1 : 3] : zp;
-            unb[2] = ym[j]; unb[3] = yp[j]; unb[4] = pv[j]; unb[5] = nv[j];
-            out[s][j] = diffuse_uniform(cdd, u, unb);
+          for (int s = 1; s < MS; s++) {
+            const float4 kk = D.rk[d0][s];
+            if (kk.w == 0.f) continue;
+            const F2 kon = f2(kk.x, kk.x), nkoff = f2(-kk.y, -kk.y), tot = f2(kk.z, kk.z);
+            const F2 dj0 = buffer_dj2(kon, nkoff, tot, f2(val[s][0], val[s][1]), ca0);
+            const F2 dj1 = buffer_dj2(kon, nkoff, tot, f2(val[s][2], val[s][3]), ca1);
+            o2[s][0] = f2_add(o2[s][0], dj0);
+            o2[s][1] = f2_add(o2[s][1], dj1);
+            o2[0][0] = f2_sub(o2[0][0], dj0);
+            o2[0][1] = f2_sub(o2[0][1], dj1);
           }
         }
-        if (si.react) {
-          if (si.react_fast) {
 #pragma unroll
-            for (int s = 1; s < MS; s++) {
-              const float4 kk = D.rk[d0][s];
-              if (kk.w == 0.f) continue;
-#pragma unroll
-              for (int j = 0; j < 4; j++) {
-                const float dJ = buffer_dj(kk.x, kk.y, kk.z, val[s][j], val[0][j]);
-                out[s][j] = __fadd_rn(out[s][j], dJ);
-                out[0][j] = __fsub_rn(out[0][j], dJ);
-              }
-            }
-          } else {
+        for (int s = 0; s < MS; s++) {
+          f2_split(o2[s][0], out[s][0], out[s][1]);
+          f2_split(o2[s][1], out[s][2], out[s][3]);
+        }
+        if (si.react && !si.react_fast) {
+          {
 #pragma unroll
             for (int j = 0; j < 4; j++) {
               float vj[MS], oj[MS];
