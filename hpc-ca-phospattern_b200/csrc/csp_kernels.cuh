@@ -319,7 +319,7 @@ __device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int
 // (evaluate_RyR_stochastically, boundaryfluxes.c:295-359) and the flux of every pair that
 // touches the voxel, summed in pair order (Species_step_boundary_fluxes,
 // species.c:1704-1907), added to the voxel's new value.
-__global__ void __launch_bounds__(256) k_boundaries(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
+__global__ void __launch_bounds__(256, 4) k_boundaries(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                      const FluxRow* __restrict__ rows, int nrows,
                                                      const FluxEntry* __restrict__ entries,
                                                      const FluxPair* __restrict__ pairs,
