@@ -290,14 +290,16 @@ __device__ __forceinline__ int gate(const FluxParams& fp, int state, double c0, 
 
 // Flux of one pair at this step, with the channel gated first (a discrete pair flows
 // only when its channel is open after this step's gating).  The owner side of a channel
-// stores its new state.  Returns false when the pair carries no flux this step.
+// stores its new state.  Returns false when the pair carries no flux this step.  CH =
+// false: the caller's rows hold density pairs only (no channel code is compiled).
+template <bool CH>
 __device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int r, int kind, int dsi,
                                           int channel, int local_channel, int boundary, int owner, long long v0,
                                           long long v1, const FluxParams& fp, const float* __restrict__ uold,
                                           const float* __restrict__ ca, unsigned char* __restrict__ states, int nch,
                                           long long k, bool stoch, double& J) {
   const long long ti = k + 1;
-  if (channel >= 0) {
+  if (CH && channel >= 0) {
     const int s_old = states[(k & 1) * (long long)nch + channel];
     int s_new = s_old;
     if (stoch && kind != FLUX_SERCA)
@@ -318,8 +320,13 @@ __device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int
 // One thread per flux row (a voxel receiving boundary flux): channel gating
 // (evaluate_RyR_stochastically, boundaryfluxes.c:295-359) and the flux of every pair that
 // touches the voxel, summed in pair order (Species_step_boundary_fluxes,
-// species.c:1704-1907), added to the voxel's new value.
-__global__ void __launch_bounds__(256, 4) k_boundaries(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
+// species.c:1704-1907), added to the voxel's new value.  The rows are split by the host:
+// CH = true for voxels touched by a discrete (channel) pair, CH = false for voxels touched
+// by density pairs only (SERCA sheets: most rows), which run without the gating code and
+// its registers, at higher occupancy.  Every voxel has one row, so the two launches write
+// disjoint voxels.
+template <bool CH>
+__global__ void __launch_bounds__(256, CH ? 4 : 8) k_boundaries(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                      const FluxRow* __restrict__ rows, int nrows,
                                                      const FluxEntry* __restrict__ entries,
                                                      const FluxPair* __restrict__ pairs,
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(256, 4) k_boundaries(const RealDesc* __restric
   const float* __restrict__ ca = D.u[cur & 1u][0];
   double acc = 0.0, J;
   bool any = false;
-  if (pair_step(D, &ctl[row.r], row.r, row.kind, row.dsi, row.channel, row.local_channel, row.boundary,
+  if (pair_step<CH>(D, &ctl[row.r], row.r, row.kind, row.dsi, row.channel, row.local_channel, row.boundary,
                 row.owner, row.v0, row.v1, params[row.param], uold, ca, states, nch, k, stoch, J)) {
     acc += (double)row.sign * J;
     any = true;
@@ -350,7 +357,7 @@ __global__ void __launch_bounds__(256, 4) k_boundaries(const RealDesc* __restric
   for (int e = row.more_begin; e < row.more_end; e++) {
     const FluxEntry en = entries[e];
     const FluxPair pr = pairs[en.pair];
-    if (pair_step(D, &ctl[row.r], row.r, pr.kind, pr.dsi, pr.channel, pr.local_channel, pr.boundary, en.owner,
+    if (pair_step<CH>(D, &ctl[row.r], row.r, pr.kind, pr.dsi, pr.channel, pr.local_channel, pr.boundary, en.owner,
                   pr.v0, pr.v1, params[pr.param], uold, ca, states, nch, k, stoch, J)) {
       acc += (double)en.sign * J;
       any = true;

@@ -130,6 +130,7 @@ struct csp_handle {
   double* d_red = nullptr;
   double* d_red_out = nullptr;
   int nrows = 0, nch = 0;
+  int nrows_density = 0;             // rows [0, nrows_density) have density pairs only
   int max_plane_vox = 0;
   long long max_vox = 0;
   int kernel = 0;                 // 0 staged, 1 direct
@@ -771,6 +772,16 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     i = j;
   }
   h->nrows = (int)rows.size();
+  // rows touched by density pairs only first (gating-free launch), channel rows after
+  auto has_channel = [&](const FluxRow& rw) {
+    if (rw.channel >= 0) return true;
+    for (int e = rw.more_begin; e < rw.more_end; e++)
+      if (pairs[entries[e].pair].channel >= 0) return true;
+    return false;
+  };
+  std::stable_partition(rows.begin(), rows.end(), [&](const FluxRow& rw) { return !has_channel(rw); });
+  h->nrows_density = 0;
+  while (h->nrows_density < h->nrows && !has_channel(rows[h->nrows_density])) h->nrows_density++;
   auto upload = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (bytes == 0) bytes = 16;
     if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
@@ -829,10 +840,15 @@ static void launch_voxels(csp_handle* h) {
 }
 
 static void launch_boundaries(csp_handle* h) {
-  if (h->nrows > 0)
-    k_boundaries<<<(h->nrows + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, h->nrows,
-                                                                h->d_entries, h->d_pairs, h->d_params, h->d_states,
-                                                                std::max(h->nch, 1));
+  const int nd = h->nrows_density, nc = h->nrows - h->nrows_density;
+  if (nd > 0)
+    k_boundaries<false><<<(nd + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, nd, h->d_entries,
+                                                                  h->d_pairs, h->d_params, h->d_states,
+                                                                  std::max(h->nch, 1));
+  if (nc > 0)
+    k_boundaries<true><<<(nc + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows + nd, nc, h->d_entries,
+                                                                 h->d_pairs, h->d_params, h->d_states,
+                                                                 std::max(h->nch, 1));
   k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->n);
 }
 
