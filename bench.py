@@ -16,8 +16,10 @@ buffers: initial fields uploaded from host memory, K calls of csp_advance(1) eac
 returning the per-realisation stop flags, final fields downloaded.  The state (5.1 GB
 per GPU) is larger than L2, so no flush is needed between steps.
 
---impl reference times the reference's CPU implementation of the step on the host cores
-(the FP64 port of the reference in oracle/; one realisation per step sample).
+cpu_baseline and --impl reference time the reference program itself (oracle/_ref: the
+reference's fvm_mpi sources built with a single-rank MPI stub and the project's HDF5
+subset, FP64, OpenMP on every physical core) on one realisation of the workload, from its
+own main-loop timer; the FP64 port in oracle/ stands in only when oracle/_ref is absent.
 """
 import argparse
 import ctypes as C
@@ -134,6 +136,23 @@ def shard_workload(rank, world, nreal):
     return specs, opts
 
 
+def pinned_copy(a):
+    """A copy of a numpy array in page-locked host memory (torch's pinned allocator), so
+    that the state copies of the e2e leg run at full PCIe speed; a plain copy without torch."""
+    try:
+        import torch
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=torch.cuda.is_available())
+        out = t.numpy()
+        out[...] = a
+        _PINNED.append(t)          # keeps the pinned block alive with the array
+        return out
+    except ImportError:
+        return a.copy()
+
+
+_PINNED = []
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -165,24 +184,92 @@ def cpu_port_rate(steps, spec, opts):
     return nvox * steps / dt, dt
 
 
+def host_cores():
+    """Physical cores of this host (the reference's OpenMP threads)."""
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return int(n)
+    except ImportError:
+        pass
+    return os.cpu_count() or 1
+
+
+def reference_binary():
+    from oracle import refrun
+    return refrun.ref_binary()
+
+
+def reference_run(spec, opts, nsteps, threads, workdir):
+    """One run of the reference program (oracle/_ref) for nsteps time steps; returns
+    (time steps taken, seconds of its MAINLOOP timer, calcium_sparks.c:188-229)."""
+    from oracle import refrun
+    h = float(opts.get("h", spec["h"]))
+    dt = 0.95 * h * h / (6 * 220000.0)           # the workload's automatic dt (sigma_max = 220000 nm^2/ms)
+    o = dict(opts)
+    o["tstop"] = nsteps * dt
+    o["dt_save"] = o["tstop"]
+    res = refrun.run(spec, o, workdir, threads=threads, verbose=True)
+    steps = max(out["time_index"] for out in res["outputs"])
+    if not res["mainloop_s"]:
+        raise RuntimeError("reference printed no MAINLOOP time")
+    return steps, res["mainloop_s"]
+
+
+def reference_rate(spec, opts, target_s, threads, workdir, steps_hint=None):
+    """voxel-steps/s of the reference program on `threads` host cores, on a sample of
+    about target_s seconds of its main loop (sized by a short calibration run)."""
+    nvox = int(np.prod(spec["voxels"].shape))
+    s0, t0 = reference_run(spec, opts, 300, threads, workdir)
+    est = nvox * s0 / max(t0, 0.05)
+    nsteps = steps_hint or max(300, int(target_s * est / nvox))
+    steps, secs = reference_run(spec, opts, nsteps, threads, workdir)
+    return nvox * steps / secs, steps, secs
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference's step on the host cores, rank 0 only."""
+    """--impl reference: the reference program's step on the host cores (rank 0 only).
+
+    oracle/_ref is the reference's own FP64 OpenMP build (fvm_mpi sources, single-rank
+    MPI stub, HDF5 subset), run on one realisation of the workload with every physical
+    core; one "step" of this arm is m time steps of that realisation, m sized so the K
+    timed steps take about 30 s of the reference's main loop."""
     synth = importlib.import_module("hpc-ca-phospattern_b200.synth")
     if rank != 0:
         return 0
     specs, opts = synth.config3(n=1)
-    steps = max(1, args.steps)
-    rate, dt = cpu_port_rate(steps, specs[0], opts[0])
+    K = max(1, args.steps)
     unit = "voxel-steps/s"
+    nvox = int(np.prod(SHAPE))
+    config = {"workload": "batched ensemble (config 3): realisations of 100x100x50 voxels at 6 nm, RyR/pRyR "
+                          "clusters + SERCA; the CPU arm runs one realisation at a time",
+              "realisations_per_gpu": N_REAL, "voxels_per_realisation": nvox, "parallelism": "OpenMP"}
+    if reference_binary():
+        import tempfile
+        cores = host_cores()
+        wd = tempfile.mkdtemp(prefix="csp_ref_")
+        s0, t0 = reference_run(specs[0], opts[0], 300, cores, wd)          # warm-up + calibration
+        est = nvox * s0 / max(t0, 0.05)
+        m = max(1, int(30.0 * est / (nvox * K)))
+        steps, secs = reference_run(specs[0], opts[0], m * K, cores, wd)
+        rate = nvox * steps / secs
+        kind = "reference"
+        sample = (f"{steps} time steps ({K} samples of {m}) of one 100x100x50 realisation of the workload, "
+                  f"{secs:.1f} s of the reference's main loop (oracle/_ref: its own FP64 OpenMP build), "
+                  f"{cores} threads")
+        ms_per_step = 1e3 * secs / K
+    else:
+        cores = 1
+        rate, dt = cpu_port_rate(K, specs[0], opts[0])
+        kind = "port"
+        sample = f"{K} steps of one 100x100x50 realisation, FP64 port of the reference (oracle/_ref not built)"
+        ms_per_step = 1e3 * dt / K
     line = {"impl": "reference", "metric": "ensemble voxel-steps/s", "value": rate, "unit": unit,
-            "n_gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps,
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": "batched ensemble, realisation 100x100x50 voxels at 6 nm (config 3); "
-                                   "CPU arm samples one realisation per step", "realisations": N_REAL,
-                       "voxels_per_realisation": int(np.prod(SHAPE))},
-            "cpu_baseline": {"value": rate, "unit": unit, "cores": 1, "kind": "port",
-                             "sample": f"{steps} steps of one 100x100x50 realisation, FP64 port of the reference"},
+            "data": "synthetic", "config": config,
+            "cpu_baseline": {"value": rate, "unit": unit, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": rate, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -195,7 +282,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--realisations", type=int, default=N_REAL)
-    ap.add_argument("--cpu-steps", type=int, default=200)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="length of the CPU baseline sample (0: skip)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -234,7 +322,8 @@ def main():
 
     # ---- e2e through the C ABI with host buffers ----
     sim2 = pkg.Simulation(specs, opts)
-    host = [sim2.state(r) for r in range(nreal)]
+    host = [pinned_copy(sim2.state(r)) for r in range(nreal)]
+    outb = [pinned_copy(h) for h in host]
     lib = sim2.lib
     flags = np.zeros(nreal, dtype=np.int32)
     fp = flags.ctypes.data_as(C.POINTER(C.c_int32))
@@ -246,23 +335,35 @@ def main():
         rc = lib.csp_advance(sim2.h, 1, fp)
         if rc:
             raise RuntimeError(f"csp_advance failed: {rc}")
-    out = [sim2.state(r) for r in range(nreal)]
+    for r in range(nreal):
+        sim2.state_into(outb[r], r)
+    out = outb
     e2e_s = time.perf_counter() - t0
     e2e_s = D.reduce(e2e_s, "max")
     e2e = vox_total * K / e2e_s
     ns = len(specs[0]["species"])
-    field_bytes = 4 * ns * nvox                     # FP32 fields copied per direction
+    field_bytes = 8 * ns * nvox                     # FP64 host state copied per direction (rounded on the device)
     h2d = field_bytes / K
     d2h = (field_bytes + K * nreal * 48) / K        # final fields + per-step progress / stop flags
     assert all(np.isfinite(o).all() for o in out)
 
     # ---- CPU baseline (rank 0, N=1 only): FP64 port of the reference ----
     cpu = None
-    if world == 1 and rank == 0 and args.cpu_steps > 0:
-        rate, dt = cpu_port_rate(args.cpu_steps, specs[0], opts[0])
-        cpu = {"value": rate, "unit": "voxel-steps/s", "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_steps} steps of one 100x100x50 realisation of the workload "
-                         f"({dt:.1f} s), FP64 port of the reference"}
+    if world == 1 and rank == 0 and args.cpu_seconds > 0:
+        if reference_binary():
+            import tempfile
+            cores = host_cores()
+            rate, steps, secs = reference_rate(specs[0], opts[0], args.cpu_seconds, cores,
+                                               tempfile.mkdtemp(prefix="csp_ref_"))
+            cpu = {"value": rate, "unit": "voxel-steps/s", "cores": cores, "kind": "reference",
+                   "sample": f"{steps} time steps of one 100x100x50 realisation of the workload, {secs:.1f} s "
+                             f"of the reference's main loop (its own FP64 OpenMP build, oracle/_ref)"}
+        else:
+            steps = 200
+            rate, dt = cpu_port_rate(steps, specs[0], opts[0])
+            cpu = {"value": rate, "unit": "voxel-steps/s", "cores": 1, "kind": "port",
+                   "sample": f"{steps} steps of one 100x100x50 realisation of the workload "
+                             f"({dt:.1f} s), FP64 port of the reference"}
 
     # per step: voxel kernel, density-row flux kernel, channel-row gating/flux kernel, step
     # epilogue (the workload has both kinds of flux rows)

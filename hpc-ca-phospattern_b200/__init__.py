@@ -99,6 +99,13 @@ class Simulation:
         self._check(self.lib.csp_download_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
         return u
 
+    def state_into(self, u, r=0):
+        """Download realisation r into a caller-owned C-contiguous float64 array."""
+        if u.dtype != np.float64 or not u.flags.c_contiguous or u.shape != self.shape(r):
+            raise ValueError("state_into needs a C-contiguous float64 array of the state shape")
+        self._check(self.lib.csp_download_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
+        return u
+
     def set_state(self, u, r=0):
         u = np.ascontiguousarray(u, dtype=np.float64)
         if u.shape != self.shape(r):

@@ -129,6 +129,8 @@ struct csp_handle {
   int* d_err = nullptr;
   double* d_red = nullptr;
   double* d_red_out = nullptr;
+  double* d_stage = nullptr;         // FP64 state staging of upload / download (one realisation)
+  size_t stage_elems = 0;
   int nrows = 0, nch = 0;
   int nrows_density = 0;             // rows [0, nrows_density) have density pairs only
   int max_plane_vox = 0;
@@ -952,51 +954,91 @@ extern "C" int csp_get_info(const csp_handle* h, int32_t r, csp_info* info) {
   return CSP_OK;
 }
 
-extern "C" int csp_upload_state(csp_handle* h, int32_t r, const double* u) {
-  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
-  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+// Physical-order FP64 state <-> device-order FP32 fields of one realisation: one thread
+// per (species, physical voxel); the physical index is linear (coalesced FP64 side), the
+// device index follows the realisation's axis order.
+struct StateMap {
+  float* f[NS];                      // current buffer of each species
+  int n[3];                          // physical voxels per axis
+  long long stride[3];               // device index stride of each physical axis
+  long long nvox;
+  int ns;
+};
+
+__global__ void k_state_in(const double* __restrict__ src, StateMap m) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m.nvox * m.ns) return;
+  const int s = (int)(i / m.nvox);
+  const long long v = i - (long long)s * m.nvox;
+  const int z = (int)(v % m.n[2]);
+  const long long xy = v / m.n[2];
+  const int y = (int)(xy % m.n[1]), x = (int)(xy / m.n[1]);
+  m.f[s][x * m.stride[0] + y * m.stride[1] + z * m.stride[2]] = __double2float_rn(src[i]);
+}
+
+__global__ void k_state_out(double* __restrict__ dst, StateMap m) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m.nvox * m.ns) return;
+  const int s = (int)(i / m.nvox);
+  const long long v = i - (long long)s * m.nvox;
+  const int z = (int)(v % m.n[2]);
+  const long long xy = v / m.n[2];
+  const int y = (int)(xy % m.n[1]), x = (int)(xy / m.n[1]);
+  dst[i] = (double)m.f[s][x * m.stride[0] + y * m.stride[1] + z * m.stride[2]];
+}
+
+static int state_map(csp_handle* h, int r, StateMap& m) {
   RealCtl c;
   int rc = read_ctl(h, r, c);
   if (rc) return rc;
   const HostReal& hr = h->real[r];
   const RealDesc& D = hr.desc;
   const unsigned cur = c.cur_mask[c.step & 1];
-  const int nx = hr.nphys[0], ny = hr.nphys[1], nz = hr.nphys[2];
-  const size_t nvox = (size_t)nx * ny * nz;
-  std::vector<float> tmp(hr.field_elems, 0.f);
-  for (int s = 0; s < D.ns; s++) {
-    const double* us = u + (size_t)s * nvox;
-    for (int x = 0; x < nx; x++)
-      for (int y = 0; y < ny; y++)
-        for (int z = 0; z < nz; z++) tmp[hr.dev_index(x, y, z)] = (float)us[((size_t)x * ny + y) * nz + z];
-    CUDA_TRY(h, cudaMemcpyAsync(D.u[(cur >> s) & 1u][s], tmp.data(), hr.field_elems * sizeof(float),
-                                cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  memset(&m, 0, sizeof m);
+  m.ns = D.ns;
+  for (int s = 0; s < D.ns; s++) m.f[s] = D.u[(cur >> s) & 1u][s];
+  for (int a = 0; a < 3; a++) m.n[a] = hr.nphys[a];
+  // device axis i holds physical axis perm[i]; device strides P, nz, 1
+  const long long dstr[3] = {(long long)D.P, (long long)D.nz, 1};
+  for (int i = 0; i < 3; i++) m.stride[hr.perm[i]] = dstr[i];
+  m.nvox = (long long)m.n[0] * m.n[1] * m.n[2];
+  const size_t need = (size_t)m.nvox * m.ns;
+  if (need > h->stage_elems) {
+    cudaFree(h->d_stage);
+    h->d_stage = nullptr;
+    h->stage_elems = 0;
+    if (cudaMalloc(&h->d_stage, need * sizeof(double)) != cudaSuccess)
+      return fail(h, CSP_ENOMEM, "state staging buffer of %.1f MB", need * 8.0 / 1e6);
+    h->stage_elems = need;
   }
+  return CSP_OK;
+}
+
+extern "C" int csp_upload_state(csp_handle* h, int32_t r, const double* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  StateMap m;
+  int rc = state_map(h, r, m);
+  if (rc) return rc;
+  const long long n = m.nvox * m.ns;
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, u, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  k_state_in<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, m);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return CSP_OK;
 }
 
 extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
   if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
   if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
-  RealCtl c;
-  int rc = read_ctl(h, r, c);
+  StateMap m;
+  int rc = state_map(h, r, m);
   if (rc) return rc;
-  const HostReal& hr = h->real[r];
-  const RealDesc& D = hr.desc;
-  const unsigned cur = c.cur_mask[c.step & 1];
-  const int nx = hr.nphys[0], ny = hr.nphys[1], nz = hr.nphys[2];
-  const size_t nvox = (size_t)nx * ny * nz;
-  std::vector<float> tmp(hr.field_elems);
-  for (int s = 0; s < D.ns; s++) {
-    CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), D.u[(cur >> s) & 1u][s], hr.field_elems * sizeof(float),
-                                cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    double* us = u + (size_t)s * nvox;
-    for (int x = 0; x < nx; x++)
-      for (int y = 0; y < ny; y++)
-        for (int z = 0; z < nz; z++) us[((size_t)x * ny + y) * nz + z] = (double)tmp[hr.dev_index(x, y, z)];
-  }
+  const long long n = m.nvox * m.ns;
+  k_state_out<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, m);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaMemcpyAsync(u, h->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return CSP_OK;
 }
 
@@ -1108,6 +1150,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   cudaFree(h->d_fields); cudaFree(h->d_dom); cudaFree(h->d_cls); cudaFree(h->d_desc); cudaFree(h->d_ctl);
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
   cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
+  cudaFree(h->d_stage);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);
