@@ -99,6 +99,17 @@ class Simulation:
         self._check(self.lib.csp_download_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
         return u
 
+    def linescan(self, species, axis, offsets_nm, conv, num_domains=0, r=0):
+        """Gaussian linescan of one species along one axis (csp_linescan)."""
+        n = self.info(r).n[axis]
+        out = np.zeros(n, dtype=np.float64)
+        off = np.ascontiguousarray(offsets_nm, dtype=np.float64)
+        cv = np.ascontiguousarray(conv, dtype=np.float64)
+        P = C.POINTER(C.c_double)
+        self._check(self.lib.csp_linescan(self.h, r, int(species), int(axis), off.ctypes.data_as(P),
+                                          cv.ctypes.data_as(P), int(num_domains), out.ctypes.data_as(P)))
+        return out
+
     def state_into(self, u, r=0):
         """Download realisation r into a caller-owned C-contiguous float64 array."""
         if u.dtype != np.float64 or not u.flags.c_contiguous or u.shape != self.shape(r):

@@ -229,6 +229,8 @@ def declare(lib):
         "csp_advance": (C.c_int, [h, C.c_int64, P(C.c_int32)]),
         "csp_reduce_outputs": (C.c_int, [h, C.c_int32, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int32)]),
         "csp_get_channel_states": (C.c_int, [h, C.c_int32, C.c_int32, P(C.c_int32)]),
+        "csp_linescan": (C.c_int, [h, C.c_int32, C.c_int32, C.c_int32, P(C.c_double), P(C.c_double), C.c_int32,
+                                   P(C.c_double)]),
         "csp_set_channel_states": (C.c_int, [h, C.c_int32, C.c_int32, P(C.c_int32)]),
         "csp_status": (C.c_int, [h, C.c_char_p, C.c_size_t]),
         "csp_get_stream": (C.c_int, [h, P(C.c_void_p)]),

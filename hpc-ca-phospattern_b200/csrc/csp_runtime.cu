@@ -1079,6 +1079,115 @@ extern "C" int csp_set_channel_states(csp_handle* h, int32_t r, int32_t boundary
   return CSP_OK;
 }
 
+// ---- linescan: convolution of one species with a 3-D Gaussian along one axis
+// (Species_compute_convolution_with_gaussian_function_locally, species.c:1960-2037) ----
+//
+// The reference sums, for every position a of the scanned axis A,
+//   u(x,y,z) * g(o_x - x h) * g(o_y - y h) * g(o_z - z h)   with o_A = a h
+// over all species voxels (or over voxels whose domain id is below num_domains, the
+// reference's domain test, species.c:2013-2024).  The weight factorises, so one pass
+// over the field builds S[i] = sum over the other two axes of u * w_B * w_C for every
+// index i of A (FP64 bins in shared memory, then one global add per bin and block), and
+// the host finishes out[a] = sum_i S[i] g((a - i) h).
+struct LinescanMap {
+  const float* f;
+  const unsigned char* dom;
+  int nd[3];                 // device extents (n0, n1, n2)
+  int P;
+  int phys_of_dev[3];        // physical axis of each device axis
+  int axis;                  // scanned physical axis
+  int num_domains;           // > 0: only voxels with domain id < num_domains
+  const double* w[3];        // per physical axis weights (the scanned axis: unused)
+  int nbins;
+};
+
+__global__ void k_linescan_bins(LinescanMap m, double* __restrict__ bins) {
+  extern __shared__ double sb[];
+  for (int i = threadIdx.x; i < m.nbins; i += blockDim.x) sb[i] = 0.0;
+  __syncthreads();
+  const long long plane = (long long)m.nd[1] * m.nd[2];
+  const long long total = (long long)m.nd[0] * plane;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
+       v += (long long)gridDim.x * blockDim.x) {
+    const int c0 = (int)(v / plane);
+    const long long rem = v - c0 * plane;
+    const int c1 = (int)(rem / m.nd[2]), c2 = (int)(rem - (long long)c1 * m.nd[2]);
+    const long long dv = (long long)c0 * m.P + rem;
+    const int dom = m.dom[dv] & DOMAIN_BITS;
+    if (m.num_domains > 0 && dom >= m.num_domains) continue;
+    int pc[3];
+    pc[m.phys_of_dev[0]] = c0; pc[m.phys_of_dev[1]] = c1; pc[m.phys_of_dev[2]] = c2;
+    double w = (double)m.f[dv];
+    for (int a = 0; a < 3; a++)
+      if (a != m.axis) w *= m.w[a][pc[a]];
+    atomicAdd(&sb[pc[m.axis]], w);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < m.nbins; i += blockDim.x)
+    if (sb[i] != 0.0) atomicAdd(&bins[i], sb[i]);
+}
+
+static double gauss_weight(double x, double sigma) {   // utils.c:209-213
+  return 1.0 / std::sqrt(2.0 * M_PI * sigma) * std::exp(-x * x / 2.0 / sigma);
+}
+
+extern "C" int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t axis, const double* offsets_nm,
+                            const double* conv, int32_t num_domains, double* out) {
+  if (!h || !offsets_nm || !conv || !out) return fail(h, CSP_EINVAL, "NULL argument");
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  const HostReal& hr = h->real[r];
+  const RealDesc& D = hr.desc;
+  if (species < 0 || species >= D.ns) return fail(h, CSP_ERANGE, "species %d out of range", species);
+  if (axis < 0 || axis > 2) return fail(h, CSP_ERANGE, "axis %d out of range", axis);
+  const int nA = hr.nphys[axis];
+  if ((size_t)nA * sizeof(double) > 48 * 1024) return fail(h, CSP_ENOTSUP, "linescan axis of %d voxels", nA);
+  RealCtl c;
+  int rc = read_ctl(h, r, c);
+  if (rc) return rc;
+  const unsigned cur = c.cur_mask[c.step & 1];
+  const double hs = hr.info.h;
+  // weights of the two fixed axes, then one device buffer: [w0 | w1 | w2 | bins]
+  std::vector<double> host;
+  size_t woff[3];
+  for (int a = 0; a < 3; a++) {
+    woff[a] = host.size();
+    for (int i = 0; i < hr.nphys[a]; i++)
+      host.push_back(a == axis ? 0.0 : gauss_weight(offsets_nm[a] - i * hs, conv[a]));
+  }
+  const size_t boff = host.size();
+  host.resize(boff + nA, 0.0);
+  double* dbuf = nullptr;
+  if (cudaMalloc(&dbuf, host.size() * sizeof(double)) != cudaSuccess)
+    return fail(h, CSP_ENOMEM, "linescan buffer");
+  LinescanMap m;
+  m.f = D.u[(cur >> species) & 1u][species];
+  m.dom = D.dom;
+  m.nd[0] = D.nx; m.nd[1] = D.ny; m.nd[2] = D.nz;
+  m.P = D.P;
+  for (int i = 0; i < 3; i++) m.phys_of_dev[i] = hr.perm[i];
+  m.axis = axis;
+  m.num_domains = num_domains;
+  for (int a = 0; a < 3; a++) m.w[a] = dbuf + woff[a];
+  m.nbins = nA;
+  cudaError_t e = cudaMemcpyAsync(dbuf, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    k_linescan_bins<<<592, 256, nA * sizeof(double), h->stream>>>(m, dbuf + boff);
+    e = cudaGetLastError();
+  }
+  std::vector<double> bins(nA);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(bins.data(), dbuf + boff, nA * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dbuf);
+  if (e != cudaSuccess) return fail(h, CSP_ECUDA, "linescan: %s", cudaGetErrorString(e));
+  for (int a = 0; a < nA; a++) {
+    double acc = 0.0;
+    for (int i = 0; i < nA; i++) acc += bins[i] * gauss_weight((a - i) * hs, conv[axis]);
+    out[a] = acc;
+  }
+  return CSP_OK;
+}
+
 extern "C" int csp_reduce_outputs(csp_handle* h, int32_t r, double* min_values, double* max_values,
                                   double* total_values, int32_t* openness) {
   if (!h) return CSP_EINVAL;

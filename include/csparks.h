@@ -231,6 +231,16 @@ int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_ms, float* b
  * 1 = direct (one thread per voxel, global loads).  Both give bitwise equal results. */
 int csp_set_kernel(csp_handle* h, int32_t which);
 
+/* Linescan of species `species` of realisation r along physical axis `axis` (0 x, 1 y,
+ * 2 z): out[a] = sum over species voxels of u * g(o_x - x h) g(o_y - y h) g(o_z - z h) with
+ * o_axis = a*h, the other two offsets_nm[] fixed (nm), g(d, s) = exp(-d^2/2s)/sqrt(2 pi s)
+ * with s = conv[axis of d] (the species file's convolution_constants).  num_domains > 0
+ * keeps only voxels whose domain id is below num_domains, the reference's test.  out has
+ * n[axis] entries.  Replaces Species_compute_convolution_with_gaussian_function_locally
+ * (species.c:1960-2037; gauss, utils.c:209-213). */
+int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t axis, const double* offsets_nm,
+                 const double* conv, int32_t num_domains, double* out);
+
 void csp_destroy(csp_handle* h);
 
 /* ---- allocation-free reduction ----
