@@ -41,6 +41,30 @@ def _status(lib, h):
     return buf.value.decode(errors="replace")
 
 
+def mlp_init(seed=1):
+    """Initial surrogate parameters (csp_mlp_init)."""
+    lib = load()
+    p = np.zeros(abi.MLP_NPARAM, dtype=np.float32)
+    lib.csp_mlp_init(int(seed), p.ctypes.data_as(C.POINTER(C.c_float)))
+    return p
+
+
+def mlp_gradient(params, x, t):
+    """(loss, grad) of the mean squared error from the device training kernels."""
+    lib = load()
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    t = np.ascontiguousarray(t, dtype=np.float32)
+    g = np.zeros(abi.MLP_NPARAM, dtype=np.float32)
+    loss = C.c_float()
+    P = C.POINTER(C.c_float)
+    rc = lib.csp_mlp_gradient(p.ctypes.data_as(P), x.ctypes.data_as(P), t.ctypes.data_as(P), int(x.shape[0]),
+                              g.ctypes.data_as(P), C.byref(loss))
+    if rc != 0:
+        raise CspError(rc, _status(lib, None))
+    return loss.value, g
+
+
 def set_device(device):
     """Select the CUDA device for the handles created next by this thread."""
     lib = load()
@@ -109,6 +133,31 @@ class Simulation:
         self._check(self.lib.csp_linescan(self.h, r, int(species), int(axis), off.ctypes.data_as(P),
                                           cv.ctypes.data_as(P), int(num_domains), out.ctypes.data_as(P)))
         return out
+
+    # ---- learned reaction surrogate ----
+    def mlp_train(self, params=None, r=0, samples=1_000_000, val_samples=65536, epochs=10, batch=16384, lr=1e-3,
+                  tol=1e-4, seed=1):
+        """Train the reaction surrogate on device (csp_mlp_train); returns (params, report dict)."""
+        p = mlp_init(seed) if params is None else np.array(params, dtype=np.float32)
+        cfg = abi.csp_mlp_config(samples=samples, val_samples=val_samples, epochs=epochs, batch=batch, lr=lr,
+                                 tol=tol, seed=seed)
+        rep = abi.csp_mlp_report()
+        self._check(self.lib.csp_mlp_train(self.h, r, C.byref(cfg), p.ctypes.data_as(C.POINTER(C.c_float)),
+                                           C.byref(rep)))
+        return p, {f: getattr(rep, f) for f, _ in abi.csp_mlp_report._fields_}
+
+    def set_surrogate(self, params, tol=1e-4):
+        """Use the surrogate with these parameters on reaction steps (None: switch off)."""
+        if params is None:
+            self._check(self.lib.csp_set_surrogate(self.h, None, float(tol)))
+            return
+        self._mlp = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.csp_set_surrogate(self.h, self._mlp.ctypes.data_as(C.POINTER(C.c_float)), float(tol)))
+
+    def surrogate_counts(self):
+        ev, fb = C.c_int64(), C.c_int64()
+        self._check(self.lib.csp_surrogate_counts(self.h, C.byref(ev), C.byref(fb)))
+        return ev.value, fb.value
 
     def state_into(self, u, r=0):
         """Download realisation r into a caller-owned C-contiguous float64 array."""

@@ -102,6 +102,19 @@ class csp_info(C.Structure):
                 ("fused_pairs", C.c_int64), ("flux_rows", C.c_int64)]
 
 
+MLP_NPARAM = 5061
+
+
+class csp_mlp_config(C.Structure):
+    _fields_ = [("samples", C.c_int64), ("val_samples", C.c_int64), ("epochs", C.c_int32), ("batch", C.c_int32),
+                ("lr", C.c_float), ("tol", C.c_double), ("seed", C.c_uint64)]
+
+
+class csp_mlp_report(C.Structure):
+    _fields_ = [("val_loss_first", C.c_float), ("val_loss_last", C.c_float), ("val_accept_rate", C.c_double),
+                ("train_ms", C.c_float), ("steps", C.c_int32), ("samples", C.c_int64)]
+
+
 def _name(s):
     b = s.encode()
     if len(b) >= NAME_LEN:
@@ -239,6 +252,12 @@ def declare(lib):
         "csp_profile_advance": (C.c_int, [h, C.c_int64, P(C.c_float), P(C.c_float)]),
         "csp_reduce_field_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_double,
                                                C.c_void_p, C.c_void_p]),
+        "csp_mlp_init": (None, [C.c_uint64, P(C.c_float)]),
+        "csp_mlp_train": (C.c_int, [h, C.c_int32, P(csp_mlp_config), P(C.c_float), P(csp_mlp_report)]),
+        "csp_mlp_gradient": (C.c_int, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64, P(C.c_float),
+                                       P(C.c_float)]),
+        "csp_set_surrogate": (C.c_int, [h, P(C.c_float), C.c_double]),
+        "csp_surrogate_counts": (C.c_int, [h, P(C.c_int64), P(C.c_int64)]),
         "csp_destroy": (None, [h]),
     }
     for name, (res, args) in sig.items():

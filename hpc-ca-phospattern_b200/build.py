@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
 
 LIB_SOURCES = ["csp_runtime.cu", "csp_noalloc.cu"]
-LIB_DEPS = ["csp_runtime.cu", "csp_noalloc.cu", "csp_device.cuh", "csp_kernels.cuh", "csp_staged.cuh",
+LIB_DEPS = ["csp_runtime.cu", "csp_noalloc.cu", "csp_device.cuh", "csp_kernels.cuh", "csp_staged.cuh", "csp_mlp.cuh",
             os.path.join("..", "..", "include", "csparks.h")]
 
 

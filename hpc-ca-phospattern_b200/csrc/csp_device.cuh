@@ -46,6 +46,8 @@ struct RealDesc {
   signed char dsi_of[NS];            // diffusive index of species s, or -1
   signed char rtab[ND][NS];          // fast reaction table: buffer index bi with bsp0 = s in domain d, or -1
   int react_fast;                    // every buffer binds species 0 and bound species are distinct per domain
+  int react_external;                // reaction increments come from the surrogate kernel (csp_mlp.cuh)
+  unsigned mlp_domains;              // bit d: domain d's reactions are mild enough for the surrogate
   // Density-boundary fluxes evaluated inside the voxel kernels.  A voxel's domain byte
   // holds the domain id in bits 0-2 and a flux pattern index in bits 3-7 (0 = none).
   // fpat[pattern][k] for neighbour direction k: 0 = no flux, else (slot + 1), with bit 7

@@ -123,7 +123,7 @@ __host__ __device__ inline StepInfo step_info(const RealDesc& D, long long time_
   StepInfo si;
   unsigned diffusing;
   step_masks(D, time_ind, si.pre, si.updated, diffusing);
-  si.react = (D.nbuf > 0 && time_ind % D.reaction_substep == 0) ? 1 : 0;
+  si.react = (D.nbuf > 0 && time_ind % D.reaction_substep == 0 && !D.react_external) ? 1 : 0;
   si.react_fast = (si.react && D.react_fast && (si.pre & 1u)) ? 1 : 0;
   return si;
 }

@@ -1,0 +1,491 @@
+// csp_mlp.cuh -- learned surrogate of the buffer-binding substep.
+//
+// With dt_update_react = n*dt the reference advances the buffer reactions once every n
+// steps by one explicit step of dt_r = n*dt from the voxel's old state
+// (Species_step_reaction, species.c:1653-1702: du += dt_r * J(u)).  The surrogate
+// replaces that increment by a learned one.  For one voxel of domain d with Ca = c and
+// bound buffer concentrations b_s (s = species 1..5, the slots of the buffers bound to
+// Ca in d):
+//   plain integrator (training target and fallback): n explicit steps of h = dt_r/n of
+//     db_s/dt = g_s = k_on,s (tot_s - b_s) c - k_off,s b_s,  dc/dt = -sum_s g_s
+//     (the reference's own reaction update applied at its native step dt, FP64);
+//   network: x = [log10(c)/3, b_1/tot_1 .. b_5/tot_5, log10(dt_r)/4, d/4] (8 inputs),
+//     two ReLU layers of 64, 5 outputs t_s; the increment is
+//     df_s = dt_r g_s / tot_s + S_s t_s,
+//     S_s = dt_r^2 / 2 (lambda_s |g_s| + k_on,s (tot_s - b_s) |G|) / tot_s,
+//     lambda_s = k_off,s + k_on,s c, G = sum_q g_q (S_s is the size of the second-order
+//     term of the exact solution, so t_s stays within about +-1 and the correction
+//     vanishes at equilibrium), db_s = tot_s df_s, dc = -sum_s db_s (total Ca conserved by
+//     construction): the network learns the correction of the single explicit step
+//     towards the plain integrator; an untrained (zero) output layer is the reference's
+//     own update;
+//   eligible domains: dt_r (sum_s k_on,s tot_s + max_s (k_off,s + 500 k_on,s)) <= 0.25, i.e.
+//     the reaction is far from stiff at dt_r over the network's Ca range; voxels of other
+//     domains (SR with millimolar CSQN) always take the plain integrator and the network
+//     is neither trained nor evaluated there;
+//   acceptance: the increment must satisfy the trapezoidal rule of the ODE,
+//     max_s |db_s - dt_r/2 (g_s(y0) + g_s(y0 + dy))| / tot_s <= tol (1e-4 by default);
+//     otherwise the voxel takes the plain integrator.
+// All FP32 except the plain integrator (FP64).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "csp_device.cuh"
+
+namespace csp {
+
+constexpr int MLP_IN = 8, MLP_H = 64, MLP_OUT = 5, MLP_SLOTS = 5;
+constexpr int MLP_NPARAM = MLP_IN * MLP_H + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H * MLP_OUT + MLP_OUT;
+
+// parameter layout (row-major, input index first): w1[8][64] b1[64] w2[64][64] b2[64] w3[64][5] b3[5]
+struct MlpW {
+  float w1[MLP_IN * MLP_H];
+  float b1[MLP_H];
+  float w2[MLP_H * MLP_H];
+  float b2[MLP_H];
+  float w3[MLP_H * MLP_OUT];
+  float b3[MLP_OUT];
+};
+static_assert(sizeof(MlpW) == MLP_NPARAM * sizeof(float), "MLP parameter layout");
+
+// buffer constants of one domain by slot (species 1..5), zero for absent slots
+struct RxConst {
+  float kon[MLP_SLOTS], koff[MLP_SLOTS], tot[MLP_SLOTS];
+};
+
+constexpr double MLP_STIFF_LIMIT = 0.25, MLP_CA_MAX = 500.0;
+
+// Domains whose buffer reactions the network serves (see the header comment).
+inline unsigned mlp_eligible_domains(const RealDesc& D);
+
+__host__ __device__ inline RxConst rx_const(const RealDesc& D, int d) {
+  RxConst k;
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    const int s = q + 1;
+    const bool on = s < NS && D.rtab[d][s] >= 0;
+    const int t = on ? D.rtab[d][s] * D.nd + d : 0;
+    const double dtr = D.dt_r;
+    // the device tables hold the rates times dt_r
+    k.kon[q] = on ? (float)(D.kon_dt[t] / dtr) : 0.f;
+    k.koff[q] = on ? (float)(D.koff_dt[t] / dtr) : 0.f;
+    k.tot[q] = on ? D.tot[t] : 0.f;
+  }
+  return k;
+}
+
+inline unsigned mlp_eligible_domains(const RealDesc& D) {
+  unsigned mask = 0;
+  const double dtr = D.dt * D.reaction_substep;
+  for (int d = 0; d < D.nd; d++) {
+    const RxConst k = rx_const(D, d);
+    double sum = 0.0, lam = 0.0;
+    bool any = false;
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      if (k.tot[q] <= 0.f) continue;
+      any = true;
+      sum += (double)k.kon[q] * k.tot[q];
+      lam = fmax(lam, (double)k.koff[q] + MLP_CA_MAX * k.kon[q]);
+    }
+    if (any && dtr * (sum + lam) <= MLP_STIFF_LIMIT) mask |= 1u << d;
+  }
+  return mask;
+}
+
+template <class T>
+__host__ __device__ inline T rx_g(const RxConst& k, int q, T c, T b) {
+  return (T)k.kon[q] * ((T)k.tot[q] - b) * c - (T)k.koff[q] * b;
+}
+
+// Scale S_s of the network's correction (see the header comment).
+template <class T>
+__host__ __device__ inline void rx_scale(const RxConst& k, T dtr, T c, const T* b, T* S) {
+  T G = 0;
+  for (int q = 0; q < MLP_SLOTS; q++)
+    if (k.tot[q] > 0.f) G += rx_g<T>(k, q, c, b[q]);
+  const T aG = G < 0 ? -G : G;
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (k.tot[q] <= 0.f) { S[q] = 0; continue; }
+    const T g = rx_g<T>(k, q, c, b[q]);
+    const T lam = (T)k.koff[q] + (T)k.kon[q] * c;
+    S[q] = (T)0.5 * dtr * dtr * (lam * (g < 0 ? -g : g) + (T)k.kon[q] * ((T)k.tot[q] - b[q]) * aG) / (T)k.tot[q];
+  }
+}
+
+// The plain integrator: n explicit steps of h, FP64.  In: c, b[]; out: increments.
+__host__ __device__ inline void rx_plain(const RxConst& k, int n, double h, double c, const double* b0, double& dc,
+                                         double* db) {
+  double b[MLP_SLOTS];
+  for (int q = 0; q < MLP_SLOTS; q++) b[q] = b0[q];
+  double cc = c;
+  for (int i = 0; i < n; i++) {
+    double g[MLP_SLOTS], sg = 0.0;
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      g[q] = k.tot[q] > 0.f ? rx_g<double>(k, q, cc, b[q]) : 0.0;
+      sg += g[q];
+    }
+    for (int q = 0; q < MLP_SLOTS; q++) b[q] += h * g[q];
+    cc -= h * sg;
+  }
+  for (int q = 0; q < MLP_SLOTS; q++) db[q] = b[q] - b0[q];
+  dc = cc - c;
+}
+
+__host__ __device__ inline void rx_features(const RxConst& k, int d, float dtr, float c, const float* b,
+                                            float* x) {
+  x[0] = log10f(fmaxf(c, 1e-3f)) * (1.f / 3.f);
+  for (int q = 0; q < MLP_SLOTS; q++) x[1 + q] = k.tot[q] > 0.f ? b[q] / k.tot[q] : 0.f;
+  x[6] = log10f(dtr) * 0.25f;
+  x[7] = 0.25f * (float)d;
+}
+
+// Training target of one sample: the correction t_s that turns the single explicit step
+// into the plain integrator's increment (0 for absent slots or S_s = 0), clipped to +-20.
+__host__ __device__ inline void rx_target(const RxConst& k, float dtr, float c, const float* b, const double* db_plain,
+                                          float* t) {
+  double bd[MLP_SLOTS], S[MLP_SLOTS];
+  for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
+  rx_scale<double>(k, (double)dtr, (double)c, bd, S);
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (k.tot[q] <= 0.f || !(S[q] > 1e-30)) { t[q] = 0.f; continue; }
+    const double g = rx_g<double>(k, q, (double)c, bd[q]);
+    double v = (db_plain[q] / k.tot[q] - dtr * g / k.tot[q]) / S[q];
+    v = v > 20.0 ? 20.0 : (v < -20.0 ? -20.0 : v);
+    t[q] = (float)v;
+  }
+}
+
+// Network forward pass of one sample; W in shared memory (broadcast reads).
+__device__ __forceinline__ void mlp_forward(const MlpW& W, const float* x, float* y) {
+  float h1[MLP_H];
+#pragma unroll
+  for (int j = 0; j < MLP_H; j++) {
+    float a = W.b1[j];
+#pragma unroll
+    for (int i = 0; i < MLP_IN; i++) a = fmaf(x[i], W.w1[i * MLP_H + j], a);
+    h1[j] = fmaxf(a, 0.f);
+  }
+  float o[MLP_OUT];
+#pragma unroll
+  for (int q = 0; q < MLP_OUT; q++) o[q] = W.b3[q];
+  // second layer in chunks of 16 units, each folded into the outputs at once
+#pragma unroll 1
+  for (int j0 = 0; j0 < MLP_H; j0 += 16) {
+    float a[16];
+#pragma unroll
+    for (int j = 0; j < 16; j++) a[j] = W.b2[j0 + j];
+#pragma unroll
+    for (int k = 0; k < MLP_H; k++) {
+#pragma unroll
+      for (int j = 0; j < 16; j++) a[j] = fmaf(h1[k], W.w2[k * MLP_H + j0 + j], a[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      const float h2 = fmaxf(a[j], 0.f);
+#pragma unroll
+      for (int q = 0; q < MLP_OUT; q++) o[q] = fmaf(h2, W.w3[(j0 + j) * MLP_OUT + q], o[q]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < MLP_OUT; q++) y[q] = o[q];
+}
+
+// Surrogate increment of one voxel with acceptance test; returns true when accepted.
+__device__ __forceinline__ bool rx_surrogate(const MlpW& W, const RxConst& k, int d, float dtr, float c,
+                                             const float* b, float tol, float& dc, float* db) {
+  float x[MLP_IN], t[MLP_OUT];
+  rx_features(k, d, dtr, c, b, x);
+  mlp_forward(W, x, t);
+  float S[MLP_SLOTS];
+  rx_scale<float>(k, dtr, c, b, S);
+  float sdb = 0.f;
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (k.tot[q] <= 0.f) { db[q] = 0.f; continue; }
+    const float g = rx_g<float>(k, q, c, b[q]);
+    const float df = dtr * g / k.tot[q] + S[q] * t[q];
+    db[q] = k.tot[q] * df;
+    sdb += db[q];
+  }
+  dc = -sdb;
+  // trapezoidal-rule residual
+  const float c1 = c + dc;
+  float worst = 0.f;
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (k.tot[q] <= 0.f) continue;
+    const float g0 = rx_g<float>(k, q, c, b[q]), g1 = rx_g<float>(k, q, c1, b[q] + db[q]);
+    worst = fmaxf(worst, fabsf(db[q] - 0.5f * dtr * (g0 + g1)) / k.tot[q]);
+  }
+  return worst <= tol && isfinite(worst);
+}
+
+}  // namespace csp
+
+namespace csp {
+
+// ---- deployment: the reaction increments of a reaction step, after the voxel kernel
+// (run with its reaction switched off) and the boundary kernels.  One thread per voxel;
+// blockIdx.y = realisation.  Reads the old state, adds into the new one; species fixed
+// in the voxel's domain and, with -f, species 0 on the outer faces keep the values the
+// voxel kernel gave them.  counters[0] += evaluated voxels, counters[1] += fallbacks.
+__global__ void __launch_bounds__(256) k_react_surrogate(const RealDesc* __restrict__ descs,
+                                                         const RealCtl* __restrict__ ctl,
+                                                         const float* __restrict__ params, float tol,
+                                                         unsigned long long* __restrict__ counters) {
+  __shared__ MlpW W;
+  __shared__ unsigned s_eval, s_fall;
+  {
+    float* w = reinterpret_cast<float*>(&W);
+    for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) w[i] = params[i];
+    if (threadIdx.x == 0) { s_eval = 0; s_fall = 0; }
+  }
+  __syncthreads();
+  const RealDesc& D = descs[blockIdx.y];
+  const RealCtl& C = ctl[blockIdx.y];
+  const long long k = C.step, ti = k + 1;
+  const bool active = !C.stopped && D.react_external && D.nbuf > 0 && ti % D.reaction_substep == 0;
+  const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long p = active ? v % D.P : 0;
+  bool mine = active && v < (long long)D.nx * D.P && p < D.plane;
+  int d = 0;
+  if (mine) {
+    d = D.dom[v] & DOMAIN_BITS;
+    bool any = false;
+    for (int s = 1; s <= MLP_SLOTS && s < NS; s++) any = any || D.rtab[d][s] >= 0;
+    mine = any;
+  }
+  if (mine) {
+    const unsigned cur = C.cur_mask[k & 1];
+    const RxConst kc = rx_const(D, d);
+    float b[MLP_SLOTS], db[MLP_SLOTS], dc;
+    const float c = D.u[cur & 1u][0][v];
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      const int s = q + 1;
+      b[q] = (kc.tot[q] > 0.f) ? D.u[(cur >> s) & 1u][s][v] : 0.f;
+    }
+    const float dtr = (float)(D.dt * D.reaction_substep);
+    const bool ok = ((D.mlp_domains >> d) & 1u) && rx_surrogate(W, kc, d, dtr, c, b, tol, dc, db);
+    atomicAdd(&s_eval, 1u);
+    if (!ok) {
+      atomicAdd(&s_fall, 1u);
+      double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
+      for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
+      rx_plain(kc, D.reaction_substep, D.dt, (double)c, bd, dcd, dbd);
+      for (int q = 0; q < MLP_SLOTS; q++) db[q] = (float)dbd[q];
+      dc = (float)dcd;
+    }
+    const unsigned fm = D.fixed_mask[d];
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      const int s = q + 1;
+      if (kc.tot[q] <= 0.f || (fm >> s & 1u)) continue;
+      float* un = D.u[((cur >> s) & 1u) ^ 1u][s];
+      un[v] = __fadd_rn(un[v], db[q]);
+    }
+    bool face = false;
+    if (D.dirichlet) {
+      const long long c0 = v / D.P;
+      const int c1 = (int)(p / D.nz), c2 = (int)(p % D.nz);
+      face = c0 == 0 || c0 == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
+    }
+    if (!(fm & 1u) && !face) {
+      float* un = D.u[(cur & 1u) ^ 1u][0];
+      un[v] = __fadd_rn(un[v], dc);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_eval) {
+    atomicAdd(&counters[0], (unsigned long long)s_eval);
+    atomicAdd(&counters[1], (unsigned long long)s_fall);
+  }
+}
+
+// ---- training ----
+
+// Voxel-state pairs for one realisation's buffer constants: Ca log-uniform over
+// [0.1, 500] uM in cytosolic domains (initial Ca < 100 uM) and [10, 2000] uM in SR
+// domains; bound fractions at equilibrium with a log-normally perturbed Ca (20 %:
+// uniform in [0, 1]); dt_r = dt * reaction_substep.  x[n][8] features, t[n][5] targets.
+__global__ void k_mlp_pairs(const RealDesc* __restrict__ desc, unsigned long long seed, long long n,
+                            const int* __restrict__ doms, int ndoms, float* __restrict__ x, float* __restrict__ t) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RealDesc& D = *desc;
+  unsigned ctr[4] = {(unsigned)i, (unsigned)(i >> 32), 0x6d6c70u, 0u}, r[4], r2[4];
+  philox4x32(ctr, (unsigned)seed, (unsigned)(seed >> 32) ^ 0x5eedu, r);
+  ctr[3] = 1u;
+  philox4x32(ctr, (unsigned)seed, (unsigned)(seed >> 32) ^ 0x5eedu, r2);
+  auto u01 = [](unsigned a) { return ((double)a + 0.5) * (1.0 / 4294967296.0); };
+  const int d = doms[r[0] % (unsigned)ndoms];
+  const bool sr = D.init[d][0] >= 100.f;
+  const double lo = sr ? 10.0 : 0.1, hi = sr ? 2000.0 : 500.0;
+  const double c = lo * exp(u01(r[1]) * log(hi / lo));
+  // Box-Muller normal for the perturbation of the equilibrium Ca
+  const double z = sqrt(-2.0 * log(u01(r[2]))) * cos(6.283185307179586 * u01(r[3]));
+  const double ce = c * exp(z);
+  const RxConst kc = rx_const(D, d);
+  float b[MLP_SLOTS];
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (kc.tot[q] <= 0.f) { b[q] = 0.f; continue; }
+    double f = kc.kon[q] * ce / (kc.kon[q] * ce + kc.koff[q]);
+    if (u01(r2[q & 3] ^ (unsigned)(q * 0x9E3779B9u)) < 0.2) f = u01(r2[(q + 1) & 3] * 2654435761u);
+    b[q] = (float)(f * kc.tot[q]);
+  }
+  const float dtr = (float)(D.dt * D.reaction_substep);
+  double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
+  for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
+  rx_plain(kc, D.reaction_substep, D.dt, (double)(float)c, bd, dcd, dbd);
+  float xf[MLP_IN], tf[MLP_OUT];
+  rx_features(kc, d, dtr, (float)c, b, xf);
+  rx_target(kc, dtr, (float)c, b, dbd, tf);
+  for (int j = 0; j < MLP_IN; j++) x[i * MLP_IN + j] = xf[j];
+  for (int j = 0; j < MLP_OUT; j++) t[i * MLP_OUT + j] = tf[j];
+}
+
+constexpr int MLP_TB = 128;           // samples (threads) per CTA of the gradient kernel
+constexpr int MLP_LD = MLP_H + 1;     // padded row length of the activation tiles
+
+// Loss and gradient of the mean squared error over samples [0, n): every CTA takes
+// MLP_TB samples, runs the forward and backward pass per sample (thread) into shared
+// tiles, forms its weight gradients as small GEMMs over its samples and adds them (and
+// its loss sum) to grad[MLP_NPARAM] / loss[0] with atomics.  scale = 1 / (n * MLP_OUT).
+__global__ void __launch_bounds__(MLP_TB) k_mlp_grad(const float* __restrict__ params, const float* __restrict__ x,
+                                                     const float* __restrict__ t, long long n, float scale,
+                                                     float* __restrict__ grad, float* __restrict__ loss) {
+  extern __shared__ float sm[];
+  MlpW& W = *reinterpret_cast<MlpW*>(sm);
+  float* X = sm + MLP_NPARAM;                  // [TB][8]
+  float* H1 = X + MLP_TB * MLP_IN;             // [TB][LD] relu(layer 1)
+  float* H2 = H1 + MLP_TB * MLP_LD;            // [TB][LD] relu(layer 2)
+  float* D2 = H2 + MLP_TB * MLP_LD;            // [TB][LD] dL/d(pre-activation 2)
+  float* D1 = D2 + MLP_TB * MLP_LD;            // [TB][LD] dL/d(pre-activation 1)
+  float* DY = D1 + MLP_TB * MLP_LD;            // [TB][5]
+  __shared__ float s_loss;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < MLP_NPARAM; i += MLP_TB) sm[i] = params[i];
+  if (tid == 0) s_loss = 0.f;
+  const long long i0 = (long long)blockIdx.x * MLP_TB;
+  const long long i = i0 + tid;
+  const bool valid = i < n;
+  for (int j = 0; j < MLP_IN; j++) X[tid * MLP_IN + j] = valid ? x[i * MLP_IN + j] : 0.f;
+  __syncthreads();
+  // forward
+  float* h1 = H1 + tid * MLP_LD;
+  float* h2 = H2 + tid * MLP_LD;
+  for (int j = 0; j < MLP_H; j++) {
+    float a = W.b1[j];
+    for (int q = 0; q < MLP_IN; q++) a = fmaf(X[tid * MLP_IN + q], W.w1[q * MLP_H + j], a);
+    h1[j] = fmaxf(a, 0.f);
+  }
+  for (int j = 0; j < MLP_H; j++) {
+    float a = W.b2[j];
+    for (int q = 0; q < MLP_H; q++) a = fmaf(h1[q], W.w2[q * MLP_H + j], a);
+    h2[j] = fmaxf(a, 0.f);
+  }
+  float l = 0.f;
+  for (int q = 0; q < MLP_OUT; q++) {
+    float y = W.b3[q];
+    for (int j = 0; j < MLP_H; j++) y = fmaf(h2[j], W.w3[j * MLP_OUT + q], y);
+    const float e = valid ? y - t[i * MLP_OUT + q] : 0.f;
+    l += e * e;
+    DY[tid * MLP_OUT + q] = 2.f * e * scale;
+  }
+  atomicAdd(&s_loss, l * scale);
+  // backward to the pre-activations
+  float* d2 = D2 + tid * MLP_LD;
+  float* d1 = D1 + tid * MLP_LD;
+  for (int j = 0; j < MLP_H; j++) {
+    float a = 0.f;
+    for (int q = 0; q < MLP_OUT; q++) a = fmaf(W.w3[j * MLP_OUT + q], DY[tid * MLP_OUT + q], a);
+    d2[j] = h2[j] > 0.f ? a : 0.f;
+  }
+  for (int k = 0; k < MLP_H; k++) {
+    float a = 0.f;
+    for (int j = 0; j < MLP_H; j++) a = fmaf(W.w2[k * MLP_H + j], d2[j], a);
+    d1[k] = h1[k] > 0.f ? a : 0.f;
+  }
+  __syncthreads();
+  // weight gradients: sums over the CTA's samples
+  float* gw1 = grad;
+  float* gb1 = gw1 + MLP_IN * MLP_H;
+  float* gw2 = gb1 + MLP_H;
+  float* gb2 = gw2 + MLP_H * MLP_H;
+  float* gw3 = gb2 + MLP_H;
+  float* gb3 = gw3 + MLP_H * MLP_OUT;
+  {
+    // w2[k][j] = sum_b H1[b][k] D2[b][j]: thread -> k = tid % 64, j in one half
+    const int kk = tid % MLP_H, jh = (tid / MLP_H) * (MLP_H / 2);
+    float acc[MLP_H / 2];
+    for (int j = 0; j < MLP_H / 2; j++) acc[j] = 0.f;
+    for (int b = 0; b < MLP_TB; b++) {
+      const float hk = H1[b * MLP_LD + kk];
+      for (int j = 0; j < MLP_H / 2; j++) acc[j] = fmaf(hk, D2[b * MLP_LD + jh + j], acc[j]);
+    }
+    for (int j = 0; j < MLP_H / 2; j++) atomicAdd(&gw2[kk * MLP_H + jh + j], acc[j]);
+  }
+  for (int e = tid; e < MLP_IN * MLP_H + 2 * MLP_H + MLP_H * MLP_OUT + MLP_OUT; e += MLP_TB) {
+    float acc = 0.f;
+    if (e < MLP_IN * MLP_H) {                                   // w1[q][k]
+      const int q = e / MLP_H, kk = e % MLP_H;
+      for (int b = 0; b < MLP_TB; b++) acc = fmaf(X[b * MLP_IN + q], D1[b * MLP_LD + kk], acc);
+      atomicAdd(&gw1[e], acc);
+    } else if (e < MLP_IN * MLP_H + MLP_H) {                    // b1[k]
+      const int kk = e - MLP_IN * MLP_H;
+      for (int b = 0; b < MLP_TB; b++) acc += D1[b * MLP_LD + kk];
+      atomicAdd(&gb1[kk], acc);
+    } else if (e < MLP_IN * MLP_H + 2 * MLP_H) {                // b2[j]
+      const int j = e - MLP_IN * MLP_H - MLP_H;
+      for (int b = 0; b < MLP_TB; b++) acc += D2[b * MLP_LD + j];
+      atomicAdd(&gb2[j], acc);
+    } else if (e < MLP_IN * MLP_H + 2 * MLP_H + MLP_H * MLP_OUT) {   // w3[j][q]
+      const int f = e - MLP_IN * MLP_H - 2 * MLP_H;
+      const int j = f / MLP_OUT, q = f % MLP_OUT;
+      for (int b = 0; b < MLP_TB; b++) acc = fmaf(H2[b * MLP_LD + j], DY[b * MLP_OUT + q], acc);
+      atomicAdd(&gw3[f], acc);
+    } else {                                                    // b3[q]
+      const int q = e - MLP_IN * MLP_H - 2 * MLP_H - MLP_H * MLP_OUT;
+      for (int b = 0; b < MLP_TB; b++) acc += DY[b * MLP_OUT + q];
+      atomicAdd(&gb3[q], acc);
+    }
+  }
+  __syncthreads();
+  if (tid == 0) atomicAdd(loss, s_loss);
+}
+
+constexpr size_t MLP_GRAD_SMEM =
+    sizeof(float) * ((size_t)MLP_NPARAM + MLP_TB * MLP_IN + 4 * (size_t)MLP_TB * MLP_LD + MLP_TB * MLP_OUT);
+
+// Adam step (Kingma & Ba, 2015) on every parameter; clears the gradient.
+__global__ void k_mlp_adam(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                           int n, float lr, float b1, float b2, float eps, int step) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / (1.f - powf(b1, (float)step)), vh = vi / (1.f - powf(b2, (float)step));
+  p[i] -= lr * mh / (sqrtf(vh) + eps);
+  g[i] = 0.f;
+}
+
+// Acceptance rate of the network on samples: rebuilds each voxel state from its features
+// and applies the surrogate's acceptance test.  counts[0] += accepted.
+__global__ void __launch_bounds__(256) k_mlp_accept(const RealDesc* __restrict__ desc, const float* __restrict__ params,
+                                                    const float* __restrict__ x, long long n, float tol,
+                                                    unsigned long long* __restrict__ counts) {
+  __shared__ MlpW W;
+  for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) reinterpret_cast<float*>(&W)[i] = params[i];
+  __syncthreads();
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const RealDesc& D = *desc;
+  const float* xi = x + i * MLP_IN;
+  const int d = (int)lrintf(xi[7] * 4.f);
+  const RxConst kc = rx_const(D, d);
+  const float c = powf(10.f, 3.f * xi[0]);
+  float b[MLP_SLOTS], db[MLP_SLOTS], dc;
+  for (int q = 0; q < MLP_SLOTS; q++) b[q] = xi[1 + q] * kc.tot[q];
+  const float dtr = (float)(D.dt * D.reaction_substep);
+  if (rx_surrogate(W, kc, d, dtr, c, b, tol, dc, db)) atomicAdd(&counts[0], 1ull);
+}
+
+}  // namespace csp

@@ -18,11 +18,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <ctime>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "csp_kernels.cuh"
 #include "csp_staged.cuh"
+#include "csp_mlp.cuh"
 
 using namespace csp;
 
@@ -139,6 +141,12 @@ struct csp_handle {
   StagedPlan plan;
   cudaGraphExec_t graph = nullptr;
   int graph_kernel = -1;
+  int graph_surrogate = 0;
+  // learned reaction surrogate (csp_set_surrogate)
+  int surrogate = 0;
+  float surrogate_tol = 1e-4f;
+  float* d_mlp = nullptr;                   // MLP_NPARAM parameters
+  unsigned long long* d_mlp_cnt = nullptr;  // evaluated voxels, fallbacks
   std::string msg;
 };
 
@@ -851,6 +859,10 @@ static void launch_boundaries(csp_handle* h) {
     k_boundaries<true><<<(nc + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows + nd, nc, h->d_entries,
                                                                  h->d_pairs, h->d_params, h->d_states,
                                                                  std::max(h->nch, 1));
+  if (h->surrogate) {
+    dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)h->n);
+    k_react_surrogate<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_mlp, h->surrogate_tol, h->d_mlp_cnt);
+  }
   k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->n);
 }
 
@@ -861,7 +873,7 @@ static cudaError_t launch_step(csp_handle* h) {
 }
 
 static int ensure_graph(csp_handle* h) {
-  if (h->graph && h->graph_kernel == h->kernel) return CSP_OK;
+  if (h->graph && h->graph_kernel == h->kernel && h->graph_surrogate == h->surrogate) return CSP_OK;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   cudaGraph_t g;
   CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -877,6 +889,7 @@ static int ensure_graph(csp_handle* h) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { h->graph = nullptr; return fail(h, CSP_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
   h->graph_kernel = h->kernel;
+  h->graph_surrogate = h->surrogate;
   return CSP_OK;
 }
 
@@ -1251,6 +1264,209 @@ extern "C" int csp_set_kernel(csp_handle* h, int32_t which) {
   return CSP_OK;
 }
 
+// ---- learned reaction surrogate (csp_mlp.cuh) ----
+
+extern "C" void csp_mlp_init(uint64_t seed, float* params) {
+  // He-uniform hidden layers, zero biases, zero output layer: an untrained network gives
+  // the reference's single explicit reaction step.
+  std::mt19937_64 g(seed);
+  std::uniform_real_distribution<float> u(-1.f, 1.f);
+  float* p = params;
+  const float a1 = std::sqrt(6.f / MLP_IN), a2 = std::sqrt(6.f / MLP_H);
+  for (int i = 0; i < MLP_IN * MLP_H; i++) *p++ = a1 * u(g);
+  for (int i = 0; i < MLP_H; i++) *p++ = 0.f;
+  for (int i = 0; i < MLP_H * MLP_H; i++) *p++ = a2 * u(g);
+  for (int i = 0; i < MLP_H; i++) *p++ = 0.f;
+  for (int i = 0; i < MLP_H * MLP_OUT + MLP_OUT; i++) *p++ = 0.f;
+}
+
+static int surrogate_supported(csp_handle* h) {
+  for (int r = 0; r < h->n; r++) {
+    const RealDesc& D = h->real[r].desc;
+    if (D.nbuf == 0) continue;
+    if (!D.react_fast) return fail(h, CSP_ENOTSUP, "realisation %d: the surrogate needs every buffer bound to species 0", r);
+    for (int d = 0; d < D.nd; d++)
+      for (int s = MLP_SLOTS + 1; s < NS; s++)
+        if (D.rtab[d][s] >= 0) return fail(h, CSP_ENOTSUP, "realisation %d: buffer species %d beyond the 5 slots", r, s);
+  }
+  return CSP_OK;
+}
+
+extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol) {
+  if (!h) return CSP_EINVAL;
+  const int on = params != nullptr;
+  if (on) {
+    int rc = surrogate_supported(h);
+    if (rc) return rc;
+    if (!h->d_mlp) {
+      if (cudaMalloc(&h->d_mlp, MLP_NPARAM * sizeof(float)) != cudaSuccess ||
+          cudaMalloc(&h->d_mlp_cnt, 2 * sizeof(unsigned long long)) != cudaSuccess)
+        return fail(h, CSP_ENOMEM, "surrogate buffers");
+      CUDA_TRY(h, cudaMemsetAsync(h->d_mlp_cnt, 0, 2 * sizeof(unsigned long long), h->stream));
+    }
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    h->surrogate_tol = (float)tol;
+  }
+  h->surrogate = on;
+  std::vector<RealDesc> descs(h->n);
+  for (int r = 0; r < h->n; r++) {
+    h->real[r].desc.react_external = on;
+    h->real[r].desc.mlp_domains = mlp_eligible_domains(h->real[r].desc);
+    descs[r] = h->real[r].desc;
+  }
+  CUDA_TRY(h, cudaMemcpyAsync(h->d_desc, descs.data(), h->n * sizeof(RealDesc), cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+extern "C" int csp_surrogate_counts(const csp_handle* hc, int64_t* evaluated, int64_t* fallbacks) {
+  csp_handle* h = const_cast<csp_handle*>(hc);
+  if (!h || !evaluated || !fallbacks) return CSP_EINVAL;
+  unsigned long long c[2] = {0, 0};
+  if (h->d_mlp_cnt) {
+    CUDA_TRY(h, cudaMemcpyAsync(c, h->d_mlp_cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  }
+  *evaluated = (int64_t)c[0];
+  *fallbacks = (int64_t)c[1];
+  return CSP_OK;
+}
+
+static cudaError_t mlp_grad_launch(const float* dp, const float* dx, const float* dt, long long n, float* dg,
+                                   float* dl, cudaStream_t st) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MLP_GRAD_SMEM);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const unsigned blocks = (unsigned)((n + MLP_TB - 1) / MLP_TB);
+  k_mlp_grad<<<blocks, MLP_TB, MLP_GRAD_SMEM, st>>>(dp, dx, dt, n, 1.f / (float)(n * MLP_OUT), dg, dl);
+  return cudaGetLastError();
+}
+
+extern "C" int csp_mlp_gradient(const float* params, const float* x, const float* t, int64_t n, float* grad,
+                                float* loss) {
+  if (!params || !x || !t || !grad || !loss || n <= 0) return fail(nullptr, CSP_EINVAL, "bad argument");
+  float *dp = nullptr, *dx = nullptr, *dt = nullptr, *dg = nullptr;
+  const size_t nb = (MLP_NPARAM + 1) * sizeof(float);
+  cudaError_t e = cudaMalloc(&dp, nb);
+  if (e == cudaSuccess) e = cudaMalloc(&dx, n * MLP_IN * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dt, n * MLP_OUT * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dg, nb);
+  if (e == cudaSuccess) e = cudaMemcpy(dp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dt, t, n * MLP_OUT * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(dg, 0, nb);
+  if (e == cudaSuccess) e = mlp_grad_launch(dp, dx, dt, n, dg, dg + MLP_NPARAM, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(grad, dg, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(loss, dg + MLP_NPARAM, sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dx); cudaFree(dt); cudaFree(dg);
+  if (e != cudaSuccess) return fail(nullptr, CSP_ECUDA, "mlp gradient: %s", cudaGetErrorString(e));
+  return CSP_OK;
+}
+
+extern "C" int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg, float* params,
+                             csp_mlp_report* rep) {
+  if (!h || !cfg || !params) return CSP_EINVAL;
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  int rc = surrogate_supported(h);
+  if (rc) return rc;
+  const RealDesc& D = h->real[r].desc;
+  std::vector<int> doms;
+  const unsigned elig = mlp_eligible_domains(D);
+  for (int d = 0; d < D.nd; d++)
+    if ((elig >> d) & 1u) doms.push_back(d);
+  if (doms.empty()) return fail(h, CSP_EINVAL, "realisation %d has no domain the surrogate can serve", r);
+  const long long nt = cfg->samples > 0 ? cfg->samples : 1000000, nv = cfg->val_samples > 0 ? cfg->val_samples : 65536;
+  const int batch = cfg->batch > 0 ? cfg->batch : 16384, epochs = cfg->epochs > 0 ? cfg->epochs : 10;
+  const long long ntot = nt + nv;
+  float *dx = nullptr, *dtg = nullptr, *dp = nullptr, *dg = nullptr, *dm = nullptr, *dv = nullptr;
+  int* dd = nullptr;
+  unsigned long long* dcnt = nullptr;
+  RealDesc* ddesc = nullptr;
+  const size_t pb = (MLP_NPARAM + 1) * sizeof(float);
+  cudaError_t e = cudaMalloc(&dx, ntot * MLP_IN * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dtg, ntot * MLP_OUT * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dp, pb);
+  if (e == cudaSuccess) e = cudaMalloc(&dg, pb);
+  if (e == cudaSuccess) e = cudaMalloc(&dm, pb);
+  if (e == cudaSuccess) e = cudaMalloc(&dv, pb);
+  if (e == cudaSuccess) e = cudaMalloc(&dd, doms.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&dcnt, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&ddesc, sizeof(RealDesc));
+  cudaStream_t st = h->stream;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ddesc, &D, sizeof(RealDesc), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dd, doms.data(), doms.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, pb, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dm, 0, pb, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dv, 0, pb, st);
+  if (e == cudaSuccess) {
+    k_mlp_pairs<<<(unsigned)((ntot + 255) / 256), 256, 0, st>>>(ddesc, cfg->seed, ntot, dd, (int)doms.size(), dx, dtg);
+    e = cudaGetLastError();
+  }
+  float val_first = 0.f, val_last = 0.f;
+  auto val_loss = [&](float& out) -> cudaError_t {
+    cudaError_t ee = cudaMemsetAsync(dg, 0, pb, st);
+    if (ee == cudaSuccess) ee = mlp_grad_launch(dp, dx + nt * MLP_IN, dtg + nt * MLP_OUT, nv, dg, dg + MLP_NPARAM, st);
+    if (ee == cudaSuccess) ee = cudaMemcpyAsync(&out, dg + MLP_NPARAM, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (ee == cudaSuccess) ee = cudaStreamSynchronize(st);
+    if (ee == cudaSuccess) ee = cudaMemsetAsync(dg, 0, pb, st);
+    return ee;
+  };
+  if (e == cudaSuccess) e = val_loss(val_first);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  int step = 0;
+  const float lr0 = cfg->lr > 0 ? cfg->lr : 1e-3f;
+  const long long nbatches = (nt + batch - 1) / batch;
+  for (int ep = 0; ep < epochs && e == cudaSuccess; ep++) {
+    // cosine learning-rate decay over the run
+    for (long long bi = 0; bi < nbatches && e == cudaSuccess; bi++) {
+      const long long s0 = bi * batch, nb = std::min<long long>(batch, nt - s0);
+      const double prog = (double)step / (double)(epochs * nbatches);
+      const float lr = (float)(lr0 * 0.5 * (1.0 + std::cos(M_PI * prog)));
+      e = mlp_grad_launch(dp, dx + s0 * MLP_IN, dtg + s0 * MLP_OUT, nb, dg, dg + MLP_NPARAM, st);
+      step++;
+      if (e == cudaSuccess) {
+        k_mlp_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, st>>>(dp, dg, dm, dv, MLP_NPARAM, lr, 0.9f, 0.999f, 1e-8f, step);
+        e = cudaGetLastError();
+      }
+    }
+  }
+  cudaEventRecord(e1, st);
+  if (e == cudaSuccess) e = val_loss(val_last);
+  unsigned long long acc = 0;
+  if (e == cudaSuccess) e = cudaMemsetAsync(dcnt, 0, sizeof acc, st);
+  if (e == cudaSuccess) {
+    k_mlp_accept<<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(ddesc, dp, dx + nt * MLP_IN, nv,
+                                                               cfg->tol > 0 ? (float)cfg->tol : 1e-4f, dcnt);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&acc, dcnt, sizeof acc, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(params, dp, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dx); cudaFree(dtg); cudaFree(dp); cudaFree(dg); cudaFree(dm); cudaFree(dv); cudaFree(dd);
+  cudaFree(dcnt); cudaFree(ddesc);
+  if (e != cudaSuccess) return fail(h, CSP_ECUDA, "mlp training: %s", cudaGetErrorString(e));
+  if (rep) {
+    rep->val_loss_first = val_first;
+    rep->val_loss_last = val_last;
+    rep->val_accept_rate = (double)acc / (double)nv;
+    rep->train_ms = ms;
+    rep->steps = step;
+    rep->samples = nt;
+  }
+  return CSP_OK;
+}
+
 extern "C" void csp_destroy(csp_handle* h) {
   if (!h) return;
   if (h->stream) cudaStreamSynchronize(h->stream);
@@ -1260,6 +1476,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
   cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
   cudaFree(h->d_stage);
+  cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -241,6 +241,51 @@ int csp_set_kernel(csp_handle* h, int32_t which);
 int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t axis, const double* offsets_nm,
                  const double* conv, int32_t num_domains, double* out);
 
+/* ---- learned reaction surrogate ----
+ * With dt_update_react = n*dt the reference advances the buffer reactions every n steps
+ * by one explicit step of dt_r = n*dt (Species_step_reaction, species.c:1653-1702).  The
+ * surrogate replaces that increment by a small MLP (8 inputs: log Ca, the bound fractions
+ * of the buffer species 1..5, log dt_r, the domain id; two ReLU layers of 64; 5 outputs)
+ * that predicts the correction of the explicit step towards the plain integrator (the
+ * same reaction update taken n times at the step dt).  Every voxel's increment must pass
+ * a trapezoidal-rule residual test (relative to the buffer totals, tolerance tol), else
+ * the voxel takes the plain integrator.  Needs every buffer bound to species 0 and bound
+ * species among 1..5. */
+#define CSP_MLP_NPARAM 5061   /* w1[8][64] b1[64] w2[64][64] b2[64] w3[64][5] b3[5] */
+
+typedef struct csp_mlp_config {
+  int64_t samples;          /* training pairs (default 1e6) */
+  int64_t val_samples;      /* held-out pairs (default 65536) */
+  int32_t epochs;           /* default 10 */
+  int32_t batch;            /* default 16384 */
+  float lr;                 /* Adam learning rate, cosine decay (default 1e-3) */
+  double tol;               /* acceptance tolerance reported on the held-out pairs (default 1e-4) */
+  uint64_t seed;            /* Philox key of the pair sampler */
+} csp_mlp_config;
+
+typedef struct csp_mlp_report {
+  float val_loss_first, val_loss_last;   /* held-out mean squared error before / after */
+  double val_accept_rate;                /* held-out pairs passing the residual test */
+  float train_ms;                        /* device time of the training loop */
+  int32_t steps;
+  int64_t samples;
+} csp_mlp_report;
+
+/* Initial parameters: He-uniform hidden layers from `seed`, zero output layer (the
+ * untrained network reproduces the single explicit step). */
+void csp_mlp_init(uint64_t seed, float* params);
+/* Train on device: pairs sampled from realisation r's buffer constants (Ca log-uniform in
+ * 0.1-500 uM in the cytosol, 10-2000 uM in SR domains; targets from the plain integrator),
+ * Adam on the mean squared error; params in (start) / out (trained). */
+int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg, float* params, csp_mlp_report* rep);
+/* Loss and gradient of the mean squared error of params on n host pairs x[n][8], t[n][5]
+ * with the device kernels used in training (for checks against a CPU implementation). */
+int csp_mlp_gradient(const float* params, const float* x, const float* t, int64_t n, float* grad, float* loss);
+/* Use params (NULL: switch off) for the reaction steps of every realisation. */
+int csp_set_surrogate(csp_handle* h, const float* params, double tol);
+/* Voxel increments evaluated by the surrogate so far, and those that fell back. */
+int csp_surrogate_counts(const csp_handle* h, int64_t* evaluated, int64_t* fallbacks);
+
 void csp_destroy(csp_handle* h);
 
 /* ---- allocation-free reduction ----

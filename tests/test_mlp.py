@@ -1,0 +1,187 @@
+"""The learned reaction surrogate: oracle pins, gradients, training, gain and deployment.
+
+CPU (no GPU):
+  * the numpy restatement's gradient (oracle/mlp.py) against central finite differences;
+  * its plain integrator against the FP64 oracle of the whole step (pinned to the
+    reference program) on a spatially uniform field, where the step is the reaction alone.
+GPU:
+  * loss and gradient of the device training kernel against the numpy oracle (FP32 vs
+    FP64: relative error <= 1e-4);
+  * training on device lowers the held-out loss and the trained network is accepted on
+    most held-out pairs;
+  * gain: on voxel states of a spark simulation, the network's increment over
+    dt_update_react = 10 dt is much closer to the plain integrator than the reference's
+    single explicit step (the method without the network);
+  * deployment: a simulation with the surrogate stays as close to the run that reacts
+    every step as the plain 10 dt run, or closer, and conserves total calcium.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp as om
+
+RNG = np.random.default_rng(11)
+DT = 0.95 * 36 / (6 * 220000.0)
+
+
+def random_params(rng, scale_out=0.3):
+    p = np.zeros(om.NPARAM)
+    p[:] = rng.normal(0, 0.3, om.NPARAM)
+    return p
+
+
+def test_oracle_gradient_finite_differences():
+    p = random_params(RNG)
+    x = RNG.normal(0, 1, (7, om.NIN))
+    t = RNG.normal(0, 1, (7, om.NOUT))
+    loss, grad = om.loss_grad(p, x, t)
+    idx = RNG.choice(om.NPARAM, 60, replace=False)
+    eps = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += eps
+        lp, _ = om.loss_grad(q, x, t)
+        q[i] -= 2 * eps
+        lm, _ = om.loss_grad(q, x, t)
+        fd = (lp - lm) / (2 * eps)
+        assert abs(fd - grad[i]) <= 1e-6 * max(1.0, abs(fd)), (i, fd, grad[i])
+
+
+def test_plain_integrator_pinned_to_oracle(synth):
+    """Uniform field, no channels: the whole step is the buffer reaction."""
+    from oracle.oracle import Oracle
+    spec = synth.tiny((6, 6, 6), serca=False, pryr=False)
+    spec["voxels"][:] = 0                              # all cytosol
+    spec["boundaries"] = []
+    spec.pop("ryr", None)
+    opts = dict(h=6.0, tstop=1.0, seed=1)
+    orc = Oracle(spec, opts)
+    u = orc.state()
+    k = om.constants(spec, 0)
+    c0 = 37.0
+    b0 = 0.3 * k[2]
+    u[0] = c0
+    for q in range(4):
+        u[q + 1] = b0[q]
+    orc.set_state(u)
+    n = 10
+    orc.step(n)
+    got = orc.state()[:, 3, 3, 3]
+    dc, db = om.plain(k, n, DT, c0, b0)
+    np.testing.assert_allclose(got[0], c0 + dc, rtol=1e-12)
+    np.testing.assert_allclose(got[1:5], b0[:4] + db[:4], rtol=1e-12)
+
+
+@pytest.mark.gpu
+def test_device_gradient_matches_oracle(pkg):
+    p = (pkg.mlp_init(3).astype(np.float64) + RNG.normal(0, 0.05, om.NPARAM)).astype(np.float32)
+    x = RNG.uniform(-1, 1, (1000, om.NIN)).astype(np.float32)
+    t = RNG.normal(0, 1, (1000, om.NOUT)).astype(np.float32)
+    loss, grad = pkg.mlp_gradient(p, x, t)
+    lref, gref = om.loss_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss - lref) <= 1e-4 * abs(lref)
+    err = np.max(np.abs(grad - gref)) / np.max(np.abs(gref))
+    assert err <= 1e-4, f"gradient rel err {err:.2e}"
+
+
+def spark_case(synth, n_real=4, react_every=10):
+    spec = synth.tiny((16, 16, 20))
+    opts = dict(h=6.0, tstop=1.0, seed=7, open_states={"ryr": [0, 4]}, t_close={"ryr": 1.0},
+                dt_update_react=react_every * DT if react_every > 1 else -1.0)
+    return spec, opts
+
+
+_TRAINED = {}
+
+
+def trained(pkg, synth):
+    if "p" not in _TRAINED:
+        spec, opts = spark_case(synth)
+        sim = pkg.Simulation(spec, opts)
+        p, rep = sim.mlp_train(samples=4_000_000, val_samples=65536, epochs=20, batch=8192, lr=2e-3, seed=5)
+        sim.close()
+        _TRAINED["p"], _TRAINED["rep"] = p, rep
+    return _TRAINED["p"], _TRAINED["rep"]
+
+
+@pytest.mark.gpu
+def test_training_lowers_loss(pkg, synth):
+    p, rep = trained(pkg, synth)
+    print(rep)
+    assert rep["val_loss_last"] < 0.15 * rep["val_loss_first"], rep
+    assert rep["val_accept_rate"] > 0.95, rep
+
+
+@pytest.mark.gpu
+def test_network_gain_over_single_explicit_step(pkg, synth):
+    """Per-voxel increment error against the plain integrator, on states of a spark."""
+    p, _ = trained(pkg, synth)
+    spec, opts = spark_case(synth)
+    sim = pkg.Simulation(spec, opts)
+    sim.advance(400)
+    u = sim.state()
+    n = sim.info().reaction_substep
+    dtr = n * DT
+    sim.close()
+    vox = spec["voxels"]
+    idx = np.argwhere(np.isin(vox, [0, 1]))                    # cytosol and cleft voxels
+    sel = idx[RNG.choice(len(idx), 3000, replace=False)]
+    e_plain_step, e_net, accepted = [], [], 0
+    pp = p.astype(np.float64)
+    for (i, j, l) in sel:
+        d = int(vox[i, j, l])
+        k = om.constants(spec, d)
+        c = float(np.float32(u[0, i, j, l]))
+        b = np.zeros(om.NSLOT)
+        b[:4] = u[1:5, i, j, l].astype(np.float32)
+        dc_ref, db_ref = om.plain(k, n, DT, c, b)
+        dc_e, db_e = om.plain(k, 1, dtr, c, b)                 # the reference's update at -T 10 dt
+        dc_n, db_n, ok = om.surrogate(pp, k, d, dtr, c, b, 1e-4)
+        accepted += ok
+        if not ok:
+            dc_n, db_n = dc_ref, db_ref                        # fallback: the plain integrator
+        tot = np.where(k[2] > 0, k[2], 1.0)
+        e_plain_step.append(np.max(np.abs(db_e - db_ref) / tot))
+        e_net.append(np.max(np.abs(db_n - db_ref) / tot))
+    e_plain_step, e_net = np.array(e_plain_step), np.array(e_net)
+    print(f"accepted {accepted / len(sel):.3f}; error/tot vs plain integrator: single explicit step median "
+          f"{np.median(e_plain_step):.2e} max {e_plain_step.max():.2e}; network median {np.median(e_net):.2e} "
+          f"max {e_net.max():.2e}")
+    rms = lambda e: float(np.sqrt(np.mean(e * e)))
+    print(f"rms: single explicit step {rms(e_plain_step):.2e}, network {rms(e_net):.2e}")
+    assert accepted / len(sel) > 0.95
+    assert np.median(e_net) < 0.2 * np.median(e_plain_step)
+    assert rms(e_net) < 0.5 * rms(e_plain_step)
+    assert e_net.max() < e_plain_step.max()
+
+
+@pytest.mark.gpu
+def test_surrogate_deployed_in_simulation(pkg, synth):
+    p, _ = trained(pkg, synth)
+    spec, opts = spark_case(synth)
+    fine_spec, fine_opts = spark_case(synth, react_every=1)
+    steps = 600
+    fine = pkg.Simulation(fine_spec, fine_opts)
+    fine.advance(steps)
+    uf = fine.state()
+    fine.close()
+    plain = pkg.Simulation(spec, opts)
+    plain.advance(steps)
+    up = plain.state()
+    plain.close()
+    sur = pkg.Simulation(spec, opts)
+    sur.set_surrogate(p, 1e-4)
+    sur.advance(steps)
+    us = sur.state()
+    ev, fb = sur.surrogate_counts()
+    sur.close()
+    assert np.all(np.isfinite(us))
+    assert ev > 0
+    scale = np.max(np.abs(uf), axis=(1, 2, 3))
+    err_plain = np.max(np.abs(up - uf), axis=(1, 2, 3)) / scale
+    err_sur = np.max(np.abs(us - uf), axis=(1, 2, 3)) / scale
+    print(f"evaluated {ev}, fallbacks {fb} ({fb / ev:.3f}); max error vs reacting every step: plain -T 10dt "
+          f"{err_plain.max():.2e}, surrogate {err_sur.max():.2e}")
+    assert err_sur.max() <= 1.05 * err_plain.max() + 1e-6
