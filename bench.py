@@ -79,6 +79,17 @@ class Dist:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX if op == "max" else self.dist.ReduceOp.SUM)
         return float(t.item())
 
+    def gather_summaries(self, sim, nreal):
+        """Steps taken and stop flag of every realisation of every rank, gathered to rank 0
+        (all_gather over NCCL with N GPUs); returns the number of realisations gathered."""
+        rows = np.array([[sim.info(r).step, sim.info(r).stopped] for r in range(nreal)], dtype=np.float64)
+        if not self.dist:
+            return rows.shape[0]
+        t = self.torch.tensor(rows, device=self.dev)
+        out = [self.torch.empty_like(t) for _ in range(self.world)]
+        self.dist.all_gather(out, t)
+        return int(sum(o.shape[0] for o in out))
+
     def close(self):
         if self.dist:
             self.dist.destroy_process_group()
@@ -275,6 +286,27 @@ def run_reference(args, rank, world):
     return 0
 
 
+def surrogate_run(pkg, specs, opts, W, K):
+    """The workload with dt_update_react = 10 dt and the learned reaction surrogate: the
+    network trained on device from the first realisation's constants, then the ensemble
+    timed like the main run."""
+    dt = 0.95 * 36 / (6 * 220000.0)
+    o10 = [dict(o, dt_update_react=10 * dt) for o in opts]
+    sim = pkg.Simulation(specs, o10)
+    params, rep = sim.mlp_train(samples=4_000_000, epochs=20, batch=8192, lr=2e-3, seed=5)
+    sim.set_surrogate(params, 1e-4)
+    sim.advance(W)
+    sim.advance(K)
+    ms = sim.last_ms()
+    vx, ev, fb = sim.surrogate_counts()
+    nvox = sum(int(np.prod(s["voxels"].shape)) for s in specs)
+    sim.close()
+    return {"value": nvox * K / (ms / 1e3), "unit": "voxel-steps/s", "dt_update_react": "10 dt",
+            "train_ms": rep["train_ms"], "val_accept_rate": rep["val_accept_rate"],
+            "voxel_increments": vx, "network_fraction": ev / vx if vx else None,
+            "fallback_fraction": fb / vx if vx else None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -282,6 +314,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--realisations", type=int, default=N_REAL)
+    ap.add_argument("--extras", type=int, default=1,
+                    help="also time the plain single-realisation path and the surrogate run (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="length of the CPU baseline sample (0: skip)")
     args = ap.parse_args()
@@ -311,6 +345,8 @@ def main():
     ms_max = D.reduce(ms, "max")
     vox_total = D.reduce(nvox, "sum")
     value = vox_total * K / (ms_max / 1e3)
+    # per-realisation summaries (steps taken, stopped) of every rank to rank 0: one gather
+    gathered = D.gather_summaries(sim, nreal)
 
     # ---- roofline of the dominant kernel: per-launch CUDA events ----
     nprof = min(K, 100)
@@ -346,6 +382,17 @@ def main():
     h2d = field_bytes / K
     d2h = (field_bytes + K * nreal * 48) / K        # final fields + per-step progress / stop flags
     assert all(np.isfinite(o).all() for o in out)
+
+    # ---- plain path: one realisation of the same workload on the same kernels ----
+    plain_single, sur = None, None
+    if args.extras:
+        single = pkg.Simulation(specs[:1], opts[:1])
+        single.advance(W)
+        single.advance(K)
+        plain_single = int(np.prod(specs[0]["voxels"].shape)) * K / (single.last_ms() / 1e3)
+        single.close()
+        # ---- learned reaction surrogate (dt_update_react = 10 dt): train, deploy, time ----
+        sur = surrogate_run(pkg, specs, opts, W, K)
 
     # ---- CPU baseline (rank 0, N=1 only): FP64 port of the reference ----
     cpu = None
@@ -386,6 +433,11 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": kernels,
+            "plain_single_realisation": None if plain_single is None else {
+                "value": plain_single, "unit": "voxel-steps/s",
+                "workload": "one 100x100x50 realisation of the workload, same kernels"},
+            "surrogate": sur,
+            "gathered_realisations": gathered,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -65,6 +65,20 @@ def mlp_gradient(params, x, t):
     return loss.value, g
 
 
+def mlp_forward(params, x, tensor_cores=False):
+    """Network outputs on device (csp_mlp_forward): FP32 or TF32 tensor cores."""
+    lib = load()
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.zeros((x.shape[0], 5), dtype=np.float32)
+    P = C.POINTER(C.c_float)
+    rc = lib.csp_mlp_forward(p.ctypes.data_as(P), x.ctypes.data_as(P), int(x.shape[0]), 1 if tensor_cores else 0,
+                             y.ctypes.data_as(P))
+    if rc != 0:
+        raise CspError(rc, _status(lib, None))
+    return y
+
+
 def set_device(device):
     """Select the CUDA device for the handles created next by this thread."""
     lib = load()
@@ -155,9 +169,10 @@ class Simulation:
         self._check(self.lib.csp_set_surrogate(self.h, self._mlp.ctypes.data_as(C.POINTER(C.c_float)), float(tol)))
 
     def surrogate_counts(self):
-        ev, fb = C.c_int64(), C.c_int64()
-        self._check(self.lib.csp_surrogate_counts(self.h, C.byref(ev), C.byref(fb)))
-        return ev.value, fb.value
+        """(voxel increments, network evaluations, plain-integrator fallbacks)."""
+        vx, ev, fb = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self.lib.csp_surrogate_counts(self.h, C.byref(vx), C.byref(ev), C.byref(fb)))
+        return vx.value, ev.value, fb.value
 
     def state_into(self, u, r=0):
         """Download realisation r into a caller-owned C-contiguous float64 array."""

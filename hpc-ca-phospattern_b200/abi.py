@@ -256,8 +256,9 @@ def declare(lib):
         "csp_mlp_train": (C.c_int, [h, C.c_int32, P(csp_mlp_config), P(C.c_float), P(csp_mlp_report)]),
         "csp_mlp_gradient": (C.c_int, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64, P(C.c_float),
                                        P(C.c_float)]),
+        "csp_mlp_forward": (C.c_int, [P(C.c_float), P(C.c_float), C.c_int64, C.c_int32, P(C.c_float)]),
         "csp_set_surrogate": (C.c_int, [h, P(C.c_float), C.c_double]),
-        "csp_surrogate_counts": (C.c_int, [h, P(C.c_int64), P(C.c_int64)]),
+        "csp_surrogate_counts": (C.c_int, [h, P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
         "csp_destroy": (None, [h]),
     }
     for name, (res, args) in sig.items():

@@ -23,6 +23,9 @@
 //     the reaction is far from stiff at dt_r over the network's Ca range; voxels of other
 //     domains (SR with millimolar CSQN) always take the plain integrator and the network
 //     is neither trained nor evaluated there;
+//   near equilibrium: where max_s S_s <= MLP_SKIP (1e-8) the correction cannot exceed
+//     ~2e-8 of the buffer totals (|t_s| <= 2 on the training data), below FP32
+//     resolution, so the network is not evaluated and the increment is the explicit one;
 //   acceptance: the increment must satisfy the trapezoidal rule of the ODE,
 //     max_s |db_s - dt_r/2 (g_s(y0) + g_s(y0 + dy))| / tot_s <= tol (1e-4 by default);
 //     otherwise the voxel takes the plain integrator.
@@ -54,6 +57,7 @@ struct RxConst {
 };
 
 constexpr double MLP_STIFF_LIMIT = 0.25, MLP_CA_MAX = 500.0;
+constexpr float MLP_SKIP = 1e-8f;
 
 // Domains whose buffer reactions the network serves (see the header comment).
 inline unsigned mlp_eligible_domains(const RealDesc& D);
@@ -189,24 +193,125 @@ __device__ __forceinline__ void mlp_forward(const MlpW& W, const float* x, float
   for (int q = 0; q < MLP_OUT; q++) y[q] = o[q];
 }
 
-// Surrogate increment of one voxel with acceptance test; returns true when accepted.
-__device__ __forceinline__ bool rx_surrogate(const MlpW& W, const RxConst& k, int d, float dtr, float c,
-                                             const float* b, float tol, float& dc, float* db) {
-  float x[MLP_IN], t[MLP_OUT];
-  rx_features(k, d, dtr, c, b, x);
-  mlp_forward(W, x, t);
+// ---- tensor-core forward pass: one warp, 32 samples (one per lane), two tiles of 16
+// rows through mma.sync m16n8k8 (TF32 inputs, FP32 accumulation).  Fragment layouts of
+// the PTX ISA for m16n8k8 .tf32 (g = lane / 4, q = lane % 4):
+//   A (16x8, row): a0 (g, q), a1 (g+8, q), a2 (g, q+4), a3 (g+8, q+4)
+//   B (8x8, col):  b0 (q, g), b1 (q+4, g)
+//   C (16x8):      c0 (g, 2q), c1 (g, 2q+1), c2 (g+8, 2q), c3 (g+8, 2q+1)
+// Weights sit in shared memory with padded rows (MLP_TC_LD) so that the fragment loads
+// hit 32 different banks; activations are staged per warp in a [32][MLP_TC_LD] tile.
+constexpr int MLP_TC_LD = MLP_H + 4;     // padded row length (floats)
+constexpr int MLP_TC_N3 = 8;             // output layer padded to one n-tile
+struct MlpTC {
+  float w1[MLP_IN * MLP_TC_LD];
+  float w2[MLP_H * MLP_TC_LD];
+  float w3[MLP_H * MLP_TC_LD];           // [64][8 used of LD], columns 5..7 zero
+  float b1[MLP_H], b2[MLP_H], b3[MLP_TC_N3];
+};
+constexpr int MLP_TC_STAGE = 32 * MLP_TC_LD;   // floats of one warp's activation tile
+
+__device__ __forceinline__ void mlp_tc_load(MlpTC& T, const float* __restrict__ p) {
+  const MlpW& W = *reinterpret_cast<const MlpW*>(p);
+  for (int i = threadIdx.x; i < MLP_IN * MLP_H; i += blockDim.x) T.w1[(i / MLP_H) * MLP_TC_LD + i % MLP_H] = W.w1[i];
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) T.w2[(i / MLP_H) * MLP_TC_LD + i % MLP_H] = W.w2[i];
+  for (int i = threadIdx.x; i < MLP_H * MLP_TC_N3; i += blockDim.x) {
+    const int k = i / MLP_TC_N3, n = i % MLP_TC_N3;
+    T.w3[k * MLP_TC_LD + n] = n < MLP_OUT ? W.w3[k * MLP_OUT + n] : 0.f;
+  }
+  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+    T.b1[i] = W.b1[i];
+    T.b2[i] = W.b2[i];
+  }
+  for (int i = threadIdx.x; i < MLP_TC_N3; i += blockDim.x) T.b3[i] = i < MLP_OUT ? W.b3[i] : 0.f;
+}
+
+__device__ __forceinline__ unsigned tf32_bits(float f) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// out[32][NT*8] = act(in[32][K] W[K][NT*8] + bias), in / out: [32][MLP_TC_LD] warp tiles
+// (out may be in: every read of a tile precedes its writes, and mma.sync converges the warp)
+template <int K, int NT, bool RELU>
+__device__ __forceinline__ void mlp_tc_layer(const float* in, const float* W, const float* bias, float* out,
+                                             int lane) {
+  const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++) {
+    float acc[NT][4];
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++) {
+      acc[nt][0] = acc[nt][2] = bias[nt * 8 + 2 * q];
+      acc[nt][1] = acc[nt][3] = bias[nt * 8 + 2 * q + 1];
+    }
+    const float* r0 = in + (mt * 16 + g) * MLP_TC_LD;
+    const float* r1 = r0 + 8 * MLP_TC_LD;
+#pragma unroll
+    for (int k0 = 0; k0 < K; k0 += 8) {
+      const unsigned a[4] = {tf32_bits(r0[k0 + q]), tf32_bits(r1[k0 + q]), tf32_bits(r0[k0 + q + 4]),
+                             tf32_bits(r1[k0 + q + 4])};
+#pragma unroll
+      for (int nt = 0; nt < NT; nt++) {
+        const unsigned b[2] = {tf32_bits(W[(k0 + q) * MLP_TC_LD + nt * 8 + g]),
+                               tf32_bits(W[(k0 + q + 4) * MLP_TC_LD + nt * 8 + g])};
+        mma_tf32(acc[nt], a, b);
+      }
+    }
+    __syncwarp();
+    float* o0 = out + (mt * 16 + g) * MLP_TC_LD;
+    float* o1 = o0 + 8 * MLP_TC_LD;
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++) {
+      float v[4] = {acc[nt][0], acc[nt][1], acc[nt][2], acc[nt][3]};
+      if (RELU)
+        for (int i = 0; i < 4; i++) v[i] = fmaxf(v[i], 0.f);
+      o0[nt * 8 + 2 * q] = v[0];
+      o0[nt * 8 + 2 * q + 1] = v[1];
+      o1[nt * 8 + 2 * q] = v[2];
+      o1[nt * 8 + 2 * q + 1] = v[3];
+    }
+    __syncwarp();
+  }
+}
+
+// Forward pass of the 32 lanes' samples; every lane of the warp must call it.
+__device__ __forceinline__ void mlp_forward_tc(const MlpTC& T, float* stage, const float* x, float* y) {
+  const int lane = threadIdx.x & 31;
+  float* row = stage + lane * MLP_TC_LD;
+#pragma unroll
+  for (int i = 0; i < MLP_IN; i++) row[i] = x[i];
+  __syncwarp();
+  mlp_tc_layer<MLP_IN, MLP_H / 8, true>(stage, T.w1, T.b1, stage, lane);
+  mlp_tc_layer<MLP_H, MLP_H / 8, true>(stage, T.w2, T.b2, stage, lane);
+  mlp_tc_layer<MLP_H, 1, false>(stage, T.w3, T.b3, stage, lane);
+#pragma unroll
+  for (int i = 0; i < MLP_OUT; i++) y[i] = row[i];
+  __syncwarp();
+}
+
+// Increment of the network output t, with the acceptance test (see the header comment).
+__device__ __forceinline__ bool rx_apply_output(const RxConst& k, float dtr, float c, const float* b, const float* t,
+                                                float tol, float& dc, float* db) {
   float S[MLP_SLOTS];
   rx_scale<float>(k, dtr, c, b, S);
   float sdb = 0.f;
   for (int q = 0; q < MLP_SLOTS; q++) {
     if (k.tot[q] <= 0.f) { db[q] = 0.f; continue; }
     const float g = rx_g<float>(k, q, c, b[q]);
-    const float df = dtr * g / k.tot[q] + S[q] * t[q];
-    db[q] = k.tot[q] * df;
+    db[q] = k.tot[q] * (dtr * g / k.tot[q] + S[q] * t[q]);
     sdb += db[q];
   }
   dc = -sdb;
-  // trapezoidal-rule residual
   const float c1 = c + dc;
   float worst = 0.f;
   for (int q = 0; q < MLP_SLOTS; q++) {
@@ -217,6 +322,16 @@ __device__ __forceinline__ bool rx_surrogate(const MlpW& W, const RxConst& k, in
   return worst <= tol && isfinite(worst);
 }
 
+// Surrogate increment of one voxel with acceptance test (FP32 forward pass); returns
+// true when accepted.
+__device__ __forceinline__ bool rx_surrogate(const MlpW& W, const RxConst& k, int d, float dtr, float c,
+                                             const float* b, float tol, float& dc, float* db) {
+  float x[MLP_IN], t[MLP_OUT];
+  rx_features(k, d, dtr, c, b, x);
+  mlp_forward(W, x, t);
+  return rx_apply_output(k, dtr, c, b, t, tol, dc, db);
+}
+
 }  // namespace csp
 
 namespace csp {
@@ -225,47 +340,87 @@ namespace csp {
 // (run with its reaction switched off) and the boundary kernels.  One thread per voxel;
 // blockIdx.y = realisation.  Reads the old state, adds into the new one; species fixed
 // in the voxel's domain and, with -f, species 0 on the outer faces keep the values the
-// voxel kernel gave them.  counters[0] += evaluated voxels, counters[1] += fallbacks.
-__global__ void __launch_bounds__(256) k_react_surrogate(const RealDesc* __restrict__ descs,
-                                                         const RealCtl* __restrict__ ctl,
-                                                         const float* __restrict__ params, float tol,
-                                                         unsigned long long* __restrict__ counters) {
-  __shared__ MlpW W;
-  __shared__ unsigned s_eval, s_fall;
-  {
-    float* w = reinterpret_cast<float*>(&W);
-    for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) w[i] = params[i];
-    if (threadIdx.x == 0) { s_eval = 0; s_fall = 0; }
-  }
-  __syncthreads();
+// voxel kernel gave them.  The network runs on the tensor cores for a whole warp when
+// any of its voxels needs it.  counters[0] += voxels, counters[1] += voxels the network
+// ran for, counters[2] += voxels that took the plain integrator.
+constexpr int MLP_DEPLOY_T = 256;
+constexpr int MLP_DEPLOY_VPT = 32;       // voxels per thread (grid-stride within the realisation)
+constexpr size_t MLP_DEPLOY_SMEM = sizeof(MlpTC) + sizeof(float) * (size_t)MLP_TC_STAGE * (MLP_DEPLOY_T / 32);
+
+__global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
+                                                                  const RealCtl* __restrict__ ctl,
+                                                                  const float* __restrict__ params, float tol,
+                                                                  unsigned long long* __restrict__ counters) {
+  extern __shared__ __align__(16) float dsm[];
+  MlpTC& T = *reinterpret_cast<MlpTC*>(dsm);
+  float* stage = dsm + sizeof(MlpTC) / sizeof(float) + (threadIdx.x >> 5) * MLP_TC_STAGE;
+  __shared__ RxConst sk[ND];
+  __shared__ unsigned s_vox, s_net, s_fall;
   const RealDesc& D = descs[blockIdx.y];
   const RealCtl& C = ctl[blockIdx.y];
   const long long k = C.step, ti = k + 1;
   const bool active = !C.stopped && D.react_external && D.nbuf > 0 && ti % D.reaction_substep == 0;
-  const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long p = active ? v % D.P : 0;
-  bool mine = active && v < (long long)D.nx * D.P && p < D.plane;
-  int d = 0;
-  if (mine) {
-    d = D.dom[v] & DOMAIN_BITS;
-    bool any = false;
-    for (int s = 1; s <= MLP_SLOTS && s < NS; s++) any = any || D.rtab[d][s] >= 0;
-    mine = any;
-  }
-  if (mine) {
-    const unsigned cur = C.cur_mask[k & 1];
-    const RxConst kc = rx_const(D, d);
-    float b[MLP_SLOTS], db[MLP_SLOTS], dc;
-    const float c = D.u[cur & 1u][0][v];
-    for (int q = 0; q < MLP_SLOTS; q++) {
-      const int s = q + 1;
-      b[q] = (kc.tot[q] > 0.f) ? D.u[(cur >> s) & 1u][s][v] : 0.f;
+  if (!active) return;                              // uniform over the block
+  const long long nvox = (long long)D.nx * D.P;
+  const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
+  if ((long long)blockIdx.x * span >= nvox) return;  // uniform over the block
+  mlp_tc_load(T, params);
+  if (threadIdx.x < ND) sk[threadIdx.x] = rx_const(D, threadIdx.x < D.nd ? threadIdx.x : 0);
+  if (threadIdx.x == 0) { s_vox = 0; s_net = 0; s_fall = 0; }
+  __syncthreads();
+  const unsigned cur = C.cur_mask[k & 1];
+  const float dtr = (float)(D.dt * D.reaction_substep);
+  unsigned n_vox = 0, n_net = 0, n_fall = 0;
+  for (int it = 0; it < MLP_DEPLOY_VPT; it++) {
+    const long long v = (long long)blockIdx.x * span + (long long)it * MLP_DEPLOY_T + threadIdx.x;
+    const long long p = v % D.P;
+    bool mine = v < nvox && p < D.plane;
+    int d = 0;
+    if (mine) {
+      d = D.dom[v] & DOMAIN_BITS;
+      bool any = false;
+      for (int q = 0; q < MLP_SLOTS; q++) any = any || sk[d].tot[q] > 0.f;
+      mine = any;
     }
-    const float dtr = (float)(D.dt * D.reaction_substep);
-    const bool ok = ((D.mlp_domains >> d) & 1u) && rx_surrogate(W, kc, d, dtr, c, b, tol, dc, db);
-    atomicAdd(&s_eval, 1u);
+    const RxConst& kc = sk[d];
+    float b[MLP_SLOTS], db[MLP_SLOTS], dc = 0.f, c = 0.f, x[MLP_IN], t[MLP_OUT];
+    for (int q = 0; q < MLP_SLOTS; q++) b[q] = 0.f;
+    bool elig = false, skip = false;
+    if (mine) {
+      c = D.u[cur & 1u][0][v];
+      for (int q = 0; q < MLP_SLOTS; q++) {
+        const int s = q + 1;
+        b[q] = (kc.tot[q] > 0.f) ? D.u[(cur >> s) & 1u][s][v] : 0.f;
+      }
+      elig = (D.mlp_domains >> d) & 1u;
+      float S[MLP_SLOTS], smax = 0.f;
+      rx_scale<float>(kc, dtr, c, b, S);
+      for (int q = 0; q < MLP_SLOTS; q++) smax = fmaxf(smax, S[q]);
+      skip = elig && smax <= MLP_SKIP;
+    }
+    const bool net = mine && elig && !skip;
+    if (net) rx_features(kc, d, dtr, c, b, x);
+    else
+      for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
+    if (__any_sync(0xffffffffu, net)) mlp_forward_tc(T, stage, x, t);   // the whole warp
+    if (!mine) continue;
+    bool ok;
+    n_vox++;
+    if (skip) {
+      // near equilibrium: the explicit increment
+      float sdb = 0.f;
+      for (int q = 0; q < MLP_SLOTS; q++) {
+        db[q] = kc.tot[q] > 0.f ? dtr * rx_g<float>(kc, q, c, b[q]) : 0.f;
+        sdb += db[q];
+      }
+      dc = -sdb;
+      ok = true;
+    } else {
+      ok = net && rx_apply_output(kc, dtr, c, b, t, tol, dc, db);
+      n_net += net;
+    }
     if (!ok) {
-      atomicAdd(&s_fall, 1u);
+      n_fall++;
       double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
       for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
       rx_plain(kc, D.reaction_substep, D.dt, (double)c, bd, dcd, dbd);
@@ -290,12 +445,37 @@ __global__ void __launch_bounds__(256) k_react_surrogate(const RealDesc* __restr
       un[v] = __fadd_rn(un[v], dc);
     }
   }
+  if (n_vox) atomicAdd(&s_vox, n_vox);
+  if (n_net) atomicAdd(&s_net, n_net);
+  if (n_fall) atomicAdd(&s_fall, n_fall);
   __syncthreads();
-  if (threadIdx.x == 0 && s_eval) {
-    atomicAdd(&counters[0], (unsigned long long)s_eval);
-    atomicAdd(&counters[1], (unsigned long long)s_fall);
+  if (threadIdx.x == 0 && s_vox) {
+    atomicAdd(&counters[0], (unsigned long long)s_vox);
+    atomicAdd(&counters[1], (unsigned long long)s_net);
+    atomicAdd(&counters[2], (unsigned long long)s_fall);
   }
 }
+
+// Forward passes for checks: y[n][5] of x[n][8], FP32 (tc = 0) or tensor cores (tc = 1).
+__global__ void __launch_bounds__(MLP_DEPLOY_T) k_mlp_forward(const float* __restrict__ params,
+                                                              const float* __restrict__ x, long long n, int tc,
+                                                              float* __restrict__ y) {
+  extern __shared__ __align__(16) float dsm[];
+  MlpTC& T = *reinterpret_cast<MlpTC*>(dsm);
+  MlpW& W = *reinterpret_cast<MlpW*>(dsm + sizeof(MlpTC) / sizeof(float) + (size_t)MLP_TC_STAGE * (MLP_DEPLOY_T / 32));
+  float* stage = dsm + sizeof(MlpTC) / sizeof(float) + (threadIdx.x >> 5) * MLP_TC_STAGE;
+  mlp_tc_load(T, params);
+  for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) reinterpret_cast<float*>(&W)[i] = params[i];
+  __syncthreads();
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  float xi[MLP_IN], yi[MLP_OUT];
+  for (int j = 0; j < MLP_IN; j++) xi[j] = i < n ? x[i * MLP_IN + j] : 0.f;
+  if (tc) mlp_forward_tc(T, stage, xi, yi);
+  else mlp_forward(W, xi, yi);
+  if (i < n)
+    for (int j = 0; j < MLP_OUT; j++) y[i * MLP_OUT + j] = yi[j];
+}
+constexpr size_t MLP_FORWARD_SMEM = MLP_DEPLOY_SMEM + sizeof(MlpW);
 
 // ---- training ----
 

@@ -146,7 +146,7 @@ struct csp_handle {
   int surrogate = 0;
   float surrogate_tol = 1e-4f;
   float* d_mlp = nullptr;                   // MLP_NPARAM parameters
-  unsigned long long* d_mlp_cnt = nullptr;  // evaluated voxels, fallbacks
+  unsigned long long* d_mlp_cnt = nullptr;  // voxels, network evaluations, fallbacks
   std::string msg;
 };
 
@@ -860,8 +860,10 @@ static void launch_boundaries(csp_handle* h) {
                                                                  h->d_pairs, h->d_params, h->d_states,
                                                                  std::max(h->nch, 1));
   if (h->surrogate) {
-    dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)h->n);
-    k_react_surrogate<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_mlp, h->surrogate_tol, h->d_mlp_cnt);
+    const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
+    dim3 grid((unsigned)((h->max_vox + span - 1) / span), (unsigned)h->n);
+    k_react_surrogate<<<grid, MLP_DEPLOY_T, MLP_DEPLOY_SMEM, h->stream>>>(h->d_desc, h->d_ctl, h->d_mlp,
+                                                                          h->surrogate_tol, h->d_mlp_cnt);
   }
   k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->n);
 }
@@ -1300,10 +1302,12 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
     if (rc) return rc;
     if (!h->d_mlp) {
       if (cudaMalloc(&h->d_mlp, MLP_NPARAM * sizeof(float)) != cudaSuccess ||
-          cudaMalloc(&h->d_mlp_cnt, 2 * sizeof(unsigned long long)) != cudaSuccess)
+          cudaMalloc(&h->d_mlp_cnt, 3 * sizeof(unsigned long long)) != cudaSuccess)
         return fail(h, CSP_ENOMEM, "surrogate buffers");
-      CUDA_TRY(h, cudaMemsetAsync(h->d_mlp_cnt, 0, 2 * sizeof(unsigned long long), h->stream));
+      CUDA_TRY(h, cudaMemsetAsync(h->d_mlp_cnt, 0, 3 * sizeof(unsigned long long), h->stream));
     }
+    CUDA_TRY(h, cudaFuncSetAttribute(k_react_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)MLP_DEPLOY_SMEM));
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     h->surrogate_tol = (float)tol;
   }
@@ -1319,16 +1323,17 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
   return CSP_OK;
 }
 
-extern "C" int csp_surrogate_counts(const csp_handle* hc, int64_t* evaluated, int64_t* fallbacks) {
+extern "C" int csp_surrogate_counts(const csp_handle* hc, int64_t* voxels, int64_t* network, int64_t* fallbacks) {
   csp_handle* h = const_cast<csp_handle*>(hc);
-  if (!h || !evaluated || !fallbacks) return CSP_EINVAL;
-  unsigned long long c[2] = {0, 0};
+  if (!h || !voxels || !network || !fallbacks) return CSP_EINVAL;
+  unsigned long long c[3] = {0, 0, 0};
   if (h->d_mlp_cnt) {
     CUDA_TRY(h, cudaMemcpyAsync(c, h->d_mlp_cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   }
-  *evaluated = (int64_t)c[0];
-  *fallbacks = (int64_t)c[1];
+  *voxels = (int64_t)c[0];
+  *network = (int64_t)c[1];
+  *fallbacks = (int64_t)c[2];
   return CSP_OK;
 }
 
@@ -1363,6 +1368,27 @@ extern "C" int csp_mlp_gradient(const float* params, const float* x, const float
   if (e == cudaSuccess) e = cudaMemcpy(loss, dg + MLP_NPARAM, sizeof(float), cudaMemcpyDeviceToHost);
   cudaFree(dp); cudaFree(dx); cudaFree(dt); cudaFree(dg);
   if (e != cudaSuccess) return fail(nullptr, CSP_ECUDA, "mlp gradient: %s", cudaGetErrorString(e));
+  return CSP_OK;
+}
+
+extern "C" int csp_mlp_forward(const float* params, const float* x, int64_t n, int32_t tensor_cores, float* y) {
+  if (!params || !x || !y || n <= 0) return fail(nullptr, CSP_EINVAL, "bad argument");
+  float *dp = nullptr, *dx = nullptr, *dy = nullptr;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)MLP_FORWARD_SMEM);
+  if (e == cudaSuccess) e = cudaMalloc(&dp, MLP_NPARAM * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dx, n * MLP_IN * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dy, n * MLP_OUT * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(dp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dx, x, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_mlp_forward<<<(unsigned)((n + MLP_DEPLOY_T - 1) / MLP_DEPLOY_T), MLP_DEPLOY_T, MLP_FORWARD_SMEM>>>(
+        dp, dx, n, tensor_cores ? 1 : 0, dy);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(y, dy, n * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dx); cudaFree(dy);
+  if (e != cudaSuccess) return fail(nullptr, CSP_ECUDA, "mlp forward: %s", cudaGetErrorString(e));
   return CSP_OK;
 }
 

@@ -249,7 +249,8 @@ int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t axis, const 
  * that predicts the correction of the explicit step towards the plain integrator (the
  * same reaction update taken n times at the step dt).  Every voxel's increment must pass
  * a trapezoidal-rule residual test (relative to the buffer totals, tolerance tol), else
- * the voxel takes the plain integrator.  Needs every buffer bound to species 0 and bound
+ * the voxel takes the plain integrator; voxels within 1e-8 of equilibrium take the
+ * explicit step without evaluating the network.  Needs every buffer bound to species 0 and bound
  * species among 1..5. */
 #define CSP_MLP_NPARAM 5061   /* w1[8][64] b1[64] w2[64][64] b2[64] w3[64][5] b3[5] */
 
@@ -281,10 +282,15 @@ int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg, float* pa
 /* Loss and gradient of the mean squared error of params on n host pairs x[n][8], t[n][5]
  * with the device kernels used in training (for checks against a CPU implementation). */
 int csp_mlp_gradient(const float* params, const float* x, const float* t, int64_t n, float* grad, float* loss);
+/* Network outputs y[n][5] of inputs x[n][8]: the FP32 pass of training (tensor_cores = 0)
+ * or the TF32 tensor-core pass the simulation uses (tensor_cores = 1). */
+int csp_mlp_forward(const float* params, const float* x, int64_t n, int32_t tensor_cores, float* y);
 /* Use params (NULL: switch off) for the reaction steps of every realisation. */
 int csp_set_surrogate(csp_handle* h, const float* params, double tol);
-/* Voxel increments evaluated by the surrogate so far, and those that fell back. */
-int csp_surrogate_counts(const csp_handle* h, int64_t* evaluated, int64_t* fallbacks);
+/* Since csp_set_surrogate: voxel reaction increments taken, those the network was
+ * evaluated for (the others were at equilibrium to within 1e-8 of their buffer totals, or
+ * in a stiff domain), and those that took the plain integrator. */
+int csp_surrogate_counts(const csp_handle* h, int64_t* voxels, int64_t* network, int64_t* fallbacks);
 
 void csp_destroy(csp_handle* h);
 

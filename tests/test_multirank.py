@@ -2,7 +2,8 @@
 
 Realisations shard across ranks with no exchange on the data path: each rank builds its
 own realisations (disjoint seeds), the only collectives are the barrier and the
-max / sum reductions of the timing and voxel counts.
+max / sum reductions of the timing and voxel counts, and one gather of the
+per-realisation summaries after the timed region.
 """
 import os
 import socket
@@ -32,7 +33,13 @@ def _worker(rank, world, port, q):
     d.barrier()
     total = d.reduce(nvox, "sum")
     slowest = d.reduce(1.0 + rank, "max")
-    q.put((rank, seeds, nvox, total, slowest))
+
+    class FakeSim:                      # per-realisation progress, as csp_get_info reports it
+        def info(self, r):
+            return type("I", (), {"step": 10 * rank + r, "stopped": r % 2})()
+
+    gathered = d.gather_summaries(FakeSim(), 4)
+    q.put((rank, seeds, nvox, total, slowest, gathered))
     d.close()
 
 
@@ -48,7 +55,9 @@ def test_two_ranks_shard_realisations_without_exchange():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, s0, n0, t0, m0), (r1, s1, n1, t1, m1) = res
+    (r0, s0, n0, t0, m0, g0), (r1, s1, n1, t1, m1, g1) = res
+    assert g0 == g1 == 8, "every rank's realisation summaries reach every rank"
+
     assert set(s0).isdisjoint(s1), "ranks must draw different realisations"
     assert t0 == t1 == n0 + n1
     assert m0 == m1 == 2.0
