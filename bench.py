@@ -333,6 +333,9 @@ def main():
     nvox = sum(int(np.prod(s["voxels"].shape)) for s in specs)
     W, K = max(3, args.warmup), args.steps
 
+    # ---- tile shape of the staged voxel kernel: the autotuner's pick ----
+    tune = sim.autotune(repeats=3)
+
     # ---- device-timed steps (graph replay, CUDA events on the handle stream) ----
     sim.advance(W)
     D.barrier()
@@ -424,7 +427,9 @@ def main():
             "config": {"workload": f"batched ensemble (config 3): {nreal} realisations of 100x100x50 voxels at 6 nm "
                                    "per GPU, RyR/pRyR clusters + SERCA, FP32 fields",
                        "realisations_per_gpu": nreal, "voxels_per_gpu": nvox,
-                       "l2": "state 5.1 GB per GPU > L2, no flush needed", "parallelism": f"ensemble x{world}"},
+                       "l2": "state 5.1 GB per GPU > L2, no flush needed", "parallelism": f"ensemble x{world}",
+                       "tile": {"threads": tune["chosen"]["threads"], "x_planes_per_unit": tune["chosen"]["segment"],
+                                "autotuned_from": len(tune["candidates"])}},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "k_voxels_staged", "launch_ms": t_launch * 1e3,

@@ -148,6 +148,13 @@ class Simulation:
                                           cv.ctypes.data_as(P), int(num_domains), out.ctypes.data_as(P)))
         return out
 
+    def autotune(self, repeats=3):
+        """Pick the staged kernel's tile shape by timing (csp_autotune); returns a dict."""
+        rep = abi.csp_tune_report()
+        self._check(self.lib.csp_autotune(self.h, int(repeats), C.byref(rep)))
+        cands = [dict(threads=rep.threads[i], segment=rep.segment[i], ms=rep.ms[i]) for i in range(rep.n)]
+        return {"chosen": cands[rep.chosen], "candidates": cands}
+
     # ---- learned reaction surrogate ----
     def mlp_train(self, params=None, r=0, samples=1_000_000, val_samples=65536, epochs=10, batch=16384, lr=1e-3,
                   tol=1e-4, seed=1):

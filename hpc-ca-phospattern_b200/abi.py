@@ -115,6 +115,11 @@ class csp_mlp_report(C.Structure):
                 ("train_ms", C.c_float), ("steps", C.c_int32), ("samples", C.c_int64)]
 
 
+class csp_tune_report(C.Structure):
+    _fields_ = [("n", C.c_int32), ("threads", C.c_int32 * 8), ("segment", C.c_int32 * 8), ("ms", C.c_float * 8),
+                ("chosen", C.c_int32)]
+
+
 def _name(s):
     b = s.encode()
     if len(b) >= NAME_LEN:
@@ -259,6 +264,7 @@ def declare(lib):
         "csp_mlp_forward": (C.c_int, [P(C.c_float), P(C.c_float), C.c_int64, C.c_int32, P(C.c_float)]),
         "csp_set_surrogate": (C.c_int, [h, P(C.c_float), C.c_double]),
         "csp_surrogate_counts": (C.c_int, [h, P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
+        "csp_autotune": (C.c_int, [h, C.c_int32, P(csp_tune_report)]),
         "csp_destroy": (None, [h]),
     }
     for name, (res, args) in sig.items():

@@ -141,6 +141,8 @@ struct csp_handle {
   StagedPlan plan;
   cudaGraphExec_t graph = nullptr;
   int graph_kernel = -1;
+  int graph_plan = -1;
+  int plan_epoch = 0;                       // bumped when the autotuner replaces the plan
   int graph_surrogate = 0;
   // learned reaction surrogate (csp_set_surrogate)
   int surrogate = 0;
@@ -875,7 +877,8 @@ static cudaError_t launch_step(csp_handle* h) {
 }
 
 static int ensure_graph(csp_handle* h) {
-  if (h->graph && h->graph_kernel == h->kernel && h->graph_surrogate == h->surrogate) return CSP_OK;
+  if (h->graph && h->graph_kernel == h->kernel && h->graph_surrogate == h->surrogate && h->graph_plan == h->plan_epoch)
+    return CSP_OK;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   cudaGraph_t g;
   CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -891,6 +894,7 @@ static int ensure_graph(csp_handle* h) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { h->graph = nullptr; return fail(h, CSP_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
   h->graph_kernel = h->kernel;
+  h->graph_plan = h->plan_epoch;
   h->graph_surrogate = h->surrogate;
   return CSP_OK;
 }
@@ -1263,6 +1267,77 @@ extern "C" int csp_set_kernel(csp_handle* h, int32_t which) {
   if (!h || which < 0 || which > 1) return CSP_EINVAL;
   if (which == 0 && !h->plan.ok) return fail(h, CSP_ENOTSUP, "staged kernel unavailable for this batch");
   h->kernel = which;
+  return CSP_OK;
+}
+
+// ---- autotuner of the staged kernel's tile shape ----
+// Candidates: threads per CTA (positions per chunk = 4 x threads) and x planes per work
+// unit.  Each candidate's voxel kernel runs `repeats` times at the current step: the
+// kernel reads the current buffers and writes the next ones, so repeating it is free of
+// side effects (the real step writes the same values), and every tiling gives bitwise
+// equal fields.  The fastest plan replaces the current one.
+extern "C" int csp_autotune(csp_handle* h, int32_t repeats, csp_tune_report* rep) {
+  if (!h) return CSP_EINVAL;
+  if (repeats < 1) repeats = 3;
+  std::vector<RealDesc> descs(h->n);
+  for (int r = 0; r < h->n; r++) descs[r] = h->real[r].desc;
+  const int cand[][2] = {{256, 0}, {256, 16}, {256, 32}, {256, 1 << 20}, {128, 0}, {128, 32}};
+  const int ncand = (int)(sizeof cand / sizeof cand[0]);
+  cudaEvent_t e0, e1;
+  CUDA_TRY(h, cudaEventCreate(&e0));
+  CUDA_TRY(h, cudaEventCreate(&e1));
+  int best = -1;
+  float best_ms = 0.f;
+  StagedPlan best_plan;
+  csp_tune_report local;
+  memset(&local, 0, sizeof local);
+  for (int i = 0; i < ncand && i < CSP_TUNE_MAX; i++) {
+    StagedPlan pl = staged_plan(descs, cand[i][0], cand[i][1]);
+    local.threads[local.n] = cand[i][0];
+    local.segment[local.n] = pl.g.seg;
+    local.ms[local.n] = -1.f;
+    if (staged_prepare(pl) != cudaSuccess) {
+      staged_release(pl);
+      local.n++;
+      continue;
+    }
+    staged_launch(pl, h->d_desc, h->d_ctl, h->d_err, h->stream);      // warm-up
+    cudaEventRecord(e0, h->stream);
+    for (int k = 0; k < repeats; k++) staged_launch(pl, h->d_desc, h->d_ctl, h->d_err, h->stream);
+    cudaEventRecord(e1, h->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      staged_release(pl);
+      if (best >= 0) staged_release(best_plan);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(h, CSP_ECUDA, "autotune: %s", cudaGetErrorString(e));
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= repeats;
+    local.ms[local.n] = ms;
+    if (best < 0 || ms < best_ms) {
+      if (best >= 0) staged_release(best_plan);
+      best = local.n;
+      best_ms = ms;
+      best_plan = pl;
+    } else {
+      staged_release(pl);
+    }
+    local.n++;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best < 0) return fail(h, CSP_ENOTSUP, "autotune: no staged plan fits this batch");
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  staged_release(h->plan);
+  h->plan = best_plan;
+  h->plan_epoch++;
+  h->kernel = 0;
+  local.chosen = best;
+  if (rep) *rep = local;
   return CSP_OK;
 }
 

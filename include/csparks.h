@@ -292,6 +292,20 @@ int csp_set_surrogate(csp_handle* h, const float* params, double tol);
  * in a stiff domain), and those that took the plain integrator. */
 int csp_surrogate_counts(const csp_handle* h, int64_t* voxels, int64_t* network, int64_t* fallbacks);
 
+/* ---- autotuner ----
+ * Times candidate tile shapes of the staged voxel kernel (threads per CTA, x planes per
+ * work unit) at the current step and keeps the fastest; fields are the same for every
+ * shape.  No counterpart in the reference (its OpenMP loops have no tile parameters). */
+#define CSP_TUNE_MAX 8
+typedef struct csp_tune_report {
+  int32_t n;                       /* candidates tried */
+  int32_t threads[CSP_TUNE_MAX];
+  int32_t segment[CSP_TUNE_MAX];   /* x planes per work unit */
+  float ms[CSP_TUNE_MAX];          /* voxel-kernel time per launch (-1: did not fit) */
+  int32_t chosen;                  /* index of the plan in use */
+} csp_tune_report;
+int csp_autotune(csp_handle* h, int32_t repeats, csp_tune_report* report);
+
 void csp_destroy(csp_handle* h);
 
 /* ---- allocation-free reduction ----

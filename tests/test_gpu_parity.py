@@ -274,3 +274,45 @@ def test_density_pair_bookkeeping(pkg, synth):
     assert 2 * nch <= inf.flux_rows <= 2 * nch + 2 * unfused
     if inf.fused_pairs == 0:
         assert inf.flux_rows > nserca
+
+
+def test_autotune_keeps_fields_bitwise(pkg, synth):
+    """The autotuner only changes the staged kernel's tiling: fields stay bitwise equal."""
+    specs = [synth.tiny((16, 14, 20)), synth.tiny((12, 12, 16))]
+    opts = [dict(h=6.0, tstop=5.0, seed=3, open_states={"ryr": [0, 2]}, t_close={"ryr": 5.0})] * 2
+    a = pkg.Simulation(specs, opts)
+    b = pkg.Simulation(specs, opts)
+    a.advance(30)
+    b.advance(30)
+    rep = b.autotune(repeats=2)
+    assert rep["chosen"]["ms"] > 0 and len(rep["candidates"]) >= 4
+    a.advance(50)
+    b.advance(50)
+    for r in range(2):
+        np.testing.assert_array_equal(a.state(r), b.state(r))
+
+
+def test_uneven_ensemble_matches_oracle(pkg, oracle_mod, synth):
+    """Config 4 in small: different shapes and resolutions (so different dt and step
+    counts) in one batch, dt_update_react = 5 dt; every realisation against its own oracle,
+    run to its own last step."""
+    cases = [((14, 12, 18), 6.0), ((10, 16, 12), 8.5), ((12, 10, 14), 10.0)]
+    specs, opts = [], []
+    for k, (shape, h) in enumerate(cases):
+        spec = synth.tiny(shape, pryr=(k != 1))
+        spec["h"] = h
+        dt = 0.95 * h * h / (6 * 220000.0)
+        specs.append(spec)
+        opts.append(dict(h=h, tstop=0.004, seed=21, dt_update_react=5 * dt, open_states={"ryr": [k]},
+                         t_close={"ryr": 0.003}))
+    sim = pkg.Simulation(specs, opts)
+    totals = [sim.info(r).total_steps for r in range(3)]
+    assert len(set(totals)) == 3, totals
+    flags = sim.advance(max(totals) + 10)
+    assert all(flags)
+    for r in range(3):
+        assert sim.info(r).step == totals[r]
+        orc = oracle_mod.Oracle(specs[r], opts[r], realisation=r)
+        orc.step(totals[r])
+        assert_close(sim.state(r), orc.state(), what=f"uneven r={r}")
+        np.testing.assert_array_equal(sim.channels(0, r), orc.channels(0))
