@@ -149,6 +149,12 @@ RYR_FIELDS = ("Kd_open", "k_min_open", "k_max_open", "n_open", "Kd_close", "k_mi
 
 def write_model(spec, geometry_file, species_file):
     """Write a model description as the reference's geometry and species files."""
+    write_geometry(spec, geometry_file)
+    write_species(spec, species_file)
+
+
+def write_geometry(spec, geometry_file):
+    """The geometry file (geometry.c:96-344): root h / global_size, /domains, /boundaries."""
     doms = spec["domains"]
     with H5(geometry_file, "w") as g:
         g.put_attr("/", "h", float(spec["h"]), np.float64)
@@ -168,6 +174,11 @@ def write_model(spec, geometry_file, species_file):
             g.put_attr("/boundaries", f"name_{i}", b["name"])
             g.put_attr("/boundaries", f"type_{i}", b["type"])
             g.put_dset(f"/boundaries/{b['name']}", np.asarray(b["pairs"]).reshape(-1, 6), np.uint16)
+
+
+def write_species(spec, species_file):
+    """The species file (species.c:103-258, boundaryfluxes.c:377-527)."""
+    doms = spec["domains"]
     with H5(species_file, "w") as s:
         sp = spec["species"]
         s.put_attr("/", "num_domains", len(doms), np.uint8)
@@ -215,50 +226,65 @@ def write_model(spec, geometry_file, species_file):
             s.put_attr("/serca", "boundary", spec["serca"]["boundary"])
 
 
-def read_model(geometry_file, species_file):
-    """Read the reference's geometry and species files into a model description."""
+def _float(v):
+    """One attribute value as a float (attributes are written as 1-element arrays)."""
+    return float(np.ravel(v)[0])
+
+
+def _int(v):
+    return int(np.ravel(v)[0])
+
+
+def read_geometry(geometry_file):
+    """The geometry part of a model description."""
     spec = {}
     with H5(geometry_file) as g:
-        spec["h"] = float(g.attr("/", "h"))
+        spec["h"] = _float(g.attr("/", "h"))
         spec["global_size"] = [float(v) for v in np.atleast_1d(g.attr("/", "global_size"))]
-        nd = int(g.attr("domains", "num"))
+        nd = _int(g.attr("domains", "num"))
         spec["domains"] = [g.attr("domains", f"name_{i}") for i in range(nd)]
         spec["voxels"] = g.dset("/domains/voxels").astype(np.uint8)
         spec["domain_connections"] = g.dset("/domains/domain_connections").astype(np.uint8)
-        nb = int(g.attr("boundaries", "num"))
+        nb = _int(g.attr("boundaries", "num"))
         spec["boundaries"] = []
         for i in range(nb):
             name = g.attr("boundaries", f"name_{i}")
             spec["boundaries"].append(dict(name=name, type=g.attr("boundaries", f"type_{i}"),
                                            pairs=g.dset(f"/boundaries/{name}").astype(np.uint16).reshape(-1, 6)))
+    return spec
+
+
+def read_model(geometry_file, species_file):
+    """Read the reference's geometry and species files into a model description."""
+    spec = read_geometry(geometry_file)
     with H5(species_file) as s:
-        ns = int(s.attr("/", "num_species"))
+        ns = _int(s.attr("/", "num_species"))
         spec["species"] = [s.attr("/", f"species_name_{i}") for i in range(ns)]
         spec["domain_species"] = {}
         for d in spec["domains"]:
             ds = {"init": [float(v) for v in np.atleast_1d(s.attr(d, "init"))]}
-            ndiff = int(s.attr(d, "num_diffusive"))
+            ndiff = _int(s.attr(d, "num_diffusive"))
             ds["diffusive"] = [int(v) for v in np.atleast_1d(s.attr(d, "diffusive"))] if ndiff else []
             ds["sigma"] = [float(v) for v in np.atleast_1d(s.attr(d, "sigma"))] if ndiff else []
             ds["buffers"] = []
-            for bi in range(int(s.attr(d, "num_buffers"))):
+            for bi in range(_int(s.attr(d, "num_buffers"))):
                 grp = f"/{d}/buffer_{bi}/"
-                ds["buffers"].append(dict(k_off=float(s.attr(grp, "k_off")), k_on=float(s.attr(grp, "k_on")),
-                                          tot=float(s.attr(grp, "tot")),
+                ds["buffers"].append(dict(k_off=_float(s.attr(grp, "k_off")), k_on=_float(s.attr(grp, "k_on")),
+                                          tot=_float(s.attr(grp, "tot")),
                                           species=[int(v) for v in np.atleast_1d(s.attr(grp, "species"))]))
             spec["domain_species"][d] = ds
-        nf = int(s.attr("/", "num_fixed_domain_species"))
+        nf = _int(s.attr("/", "num_fixed_domain_species"))
         fx = np.atleast_1d(s.attr("/", "fixed_domain_species")) if nf else []
         spec["fixed_domain_species"] = [(int(fx[2 * i]), int(fx[2 * i + 1])) for i in range(nf)]
         spec["convolution_constants"] = [float(v) for v in np.atleast_1d(s.attr("/", "convolution_constants"))]
         for key in ("ryr", "p_ryr"):
-            if int(s.attr("/", f"use_{key}")):
-                p = {f: float(s.attr("/" + key, f)) for f in RYR_FIELDS}
+            if _int(s.attr("/", f"use_{key}")):
+                p = {f: _float(s.attr("/" + key, f)) for f in RYR_FIELDS}
                 p["boundary"] = s.attr("/" + key, "boundary")
                 p["species"] = s.attr("/" + key, "species")
                 spec[key] = p
-        if int(s.attr("/", "use_serca")):
-            p = {f: float(s.attr("/serca", f)) for f in ("v_cyt_to_A_sr", "density", "scale")}
+        if _int(s.attr("/", "use_serca")):
+            p = {f: _float(s.attr("/serca", f)) for f in ("v_cyt_to_A_sr", "density", "scale")}
             p["boundary"] = s.attr("/serca", "boundary")
             # the reference takes the SERCA species from the /ryr group (boundaryfluxes.c:511)
             p["species"] = s.attr("/ryr", "species")
