@@ -254,7 +254,11 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
               ((wyp ^ dw) & ymask_p) == 0u;
       }
 
-      if (__builtin_expect(uni, 1)) {
+      // the uniform path only when every in-range group of the warp takes it: a warp with
+      // a few mixed groups would otherwise run both paths one after the other; the mixed
+      // path gives uniform groups the same rounded values
+      const bool uni_w = __all_sync(__activemask(), uni || !all_in);
+      if (__builtin_expect(uni && uni_w, 1)) {
         // ---- uniform group: constants once per group, one species at a time, voxel
         // pairs (0,1) and (2,3) in two-lane FP32 ----
         float val[MS][4];
@@ -418,13 +422,57 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           slot++;
           if (!(si.pre >> s & 1u)) continue;
           const float* cs = D.coef[D.dsi_of[s]];
-          float4 vp = make_float4(0.f, 0.f, 0.f, 0.f), vn = vp;
-          if (has_prev) vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
-          if (has_next) vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
+          // out-of-box neighbours are read at the voxel itself (as in the uniform path)
+          const float4 vp = *reinterpret_cast<const float4*>(fp + so_s + p0);
+          const float4 vn = *reinterpret_cast<const float4*>(fn + so_s + p0);
           const float pv[4] = {vp.x, vp.y, vp.z, vp.w};
           const float nv[4] = {vn.x, vn.y, vn.z, vn.w};
           const float zm = fc[so_s + ((vzy[0] & 1u) ? p0 - 1 : p0)];
           const float zp = fc[so_s + ((vzy[3] & 2u) ? p0 + 4 : p0 + 3)];
+#ifndef CSP_FUSE_DENSITY
+          // two voxels per instruction: the uniform form and the per-neighbour-coefficient
+          // form (diffuse_coef6) on the pair, then per voxel the one its neighbourhood calls
+          // for -- each lane rounds exactly as the scalar functions do
+          float unbv[4][6];
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const unsigned valid = vzy[j] | xval;
+            const float u = val[s][j];
+            unbv[j][0] = j > 0 ? val[s][j > 0 ? j - 1 : 0] : zm;
+            unbv[j][1] = j < 3 ? val[s][j < 3 ? j + 1 : 3] : zp;
+            if (!yvec) {
+              unbv[j][0] = (valid & 1u) ? unbv[j][0] : u;
+              unbv[j][1] = (valid & 2u) ? unbv[j][1] : u;
+            }
+            unbv[j][2] = fc[so_s + ((valid & 4u) ? p0 + j - nz : p0 + j)];
+            unbv[j][3] = fc[so_s + ((valid & 8u) ? p0 + j + nz : p0 + j)];
+            unbv[j][4] = pv[j];
+            unbv[j][5] = nv[j];
+          }
+          const F2 m2 = f2(-2.f, -2.f), zero2 = f2(0.f, 0.f);
+#pragma unroll
+          for (int q = 0; q < 2; q++) {
+            const int ja = 2 * q, jb = 2 * q + 1;
+            const F2 u2 = f2(val[s][ja], val[s][jb]);
+            const float* ca = cs + dj[ja] * ND;
+            const float* cb = cs + dj[jb] * ND;
+            const F2 cu = f2(ca[dj[ja]], cb[dj[jb]]);
+            const F2 zs = f2(__fadd_rn(unbv[ja][0], unbv[ja][1]), __fadd_rn(unbv[jb][0], unbv[jb][1]));
+            const F2 ys = f2_add(f2(unbv[ja][2], unbv[jb][2]), f2(unbv[ja][3], unbv[jb][3]));
+            const F2 xs = f2_add(f2(unbv[ja][4], unbv[jb][4]), f2(unbv[ja][5], unbv[jb][5]));
+            const F2 ru = diffuse_uniform2(cu, m2, u2, zs, ys, xs);
+            F2 a = zero2;
+#pragma unroll
+            for (int kk = 0; kk < 6; kk++)
+              a = f2_fma(f2(ca[dnb[ja][kk]], cb[dnb[jb][kk]]), f2_sub(f2(unbv[ja][kk], unbv[jb][kk]), u2), a);
+            const F2 rg = f2_add(u2, a);
+            float ua, ub, ga, gb;
+            f2_split(ru, ua, ub);
+            f2_split(rg, ga, gb);
+            out[s][ja] = unij[ja] ? ua : ga;
+            out[s][jb] = unij[jb] ? ub : gb;
+          }
+#else
 #pragma unroll
           for (int j = 0; j < 4; j++) {
             const unsigned valid = vzy[j] | xval;
@@ -434,9 +482,11 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             float unb[6];
             unb[0] = j > 0 ? val[s][j > 0 ? j - 1 : 0] : zm;
             unb[1] = j < 3 ? val[s][j < 3 ? j + 1 : 3] : zp;
+            if (!yvec) {   // the group may straddle a row end: in-group z neighbours per voxel
+              unb[0] = (valid & 1u) ? unb[0] : u;
+              unb[1] = (valid & 2u) ? unb[1] : u;
+            }
             unb[2] = ym; unb[3] = yp; unb[4] = pv[j]; unb[5] = nv[j];
-#pragma unroll
-            for (int kk = 0; kk < 6; kk++) unb[kk] = (valid >> kk & 1u) ? unb[kk] : u;
             const float* c = cs + dj[j] * ND;
             out[s][j] = unij[j] ? diffuse_uniform(c[dj[j]], u, unb) : diffuse_general(c, dnb[j], u, unb);
 #ifdef CSP_FUSE_DENSITY
@@ -459,11 +509,42 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             }
 #endif
           }
+#endif
+        }
+        // the four voxels in one domain (usual next to a domain sheet): the group form of
+        // the buffer reactions, as in the uniform path
+        const bool one_dom = dj[0] == dj[1] && dj[1] == dj[2] && dj[2] == dj[3];
+        if (si.react && si.react_fast && one_dom) {
+          const int d = dj[0];
+          F2 o2[MS][2];
+#pragma unroll
+          for (int s = 0; s < MS; s++) {
+            o2[s][0] = f2(out[s][0], out[s][1]);
+            o2[s][1] = f2(out[s][2], out[s][3]);
+          }
+          const F2 ca0 = f2(val[0][0], val[0][1]), ca1 = f2(val[0][2], val[0][3]);
+#pragma unroll
+          for (int s = 1; s < MS; s++) {
+            const float4 kk = D.rk[d][s];
+            if (kk.w == 0.f) continue;
+            const F2 kon = f2(kk.x, kk.x), nkoff = f2(-kk.y, -kk.y), tot = f2(kk.z, kk.z);
+            const F2 dj0 = buffer_dj2(kon, nkoff, tot, f2(val[s][0], val[s][1]), ca0);
+            const F2 dj1 = buffer_dj2(kon, nkoff, tot, f2(val[s][2], val[s][3]), ca1);
+            o2[s][0] = f2_add(o2[s][0], dj0);
+            o2[s][1] = f2_add(o2[s][1], dj1);
+            o2[0][0] = f2_sub(o2[0][0], dj0);
+            o2[0][1] = f2_sub(o2[0][1], dj1);
+          }
+#pragma unroll
+          for (int s = 0; s < MS; s++) {
+            f2_split(o2[s][0], out[s][0], out[s][1]);
+            f2_split(o2[s][1], out[s][2], out[s][3]);
+          }
         }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
           const int d = dj[j];
-          if (si.react) {
+          if (si.react && !(si.react_fast && one_dom)) {
             if (si.react_fast) {
 #pragma unroll
               for (int s = 1; s < MS; s++) {
