@@ -79,6 +79,29 @@ struct RealCtl {
   double last_closed;                // abort rule bookkeeping
 };
 
+// What a realisation's running step does, for the density-row kernel: written at creation
+// and by the step epilogue for the next step (one 16-byte load per row).
+struct alignas(16) StepRec {
+  unsigned active;                   // not stopped
+  unsigned cur;                      // bit s: index of the current buffer of species s
+  unsigned updated;                  // species written by the step
+  unsigned sub;                      // bit dsi: diffusive index dsi takes its substep (and its fluxes)
+};
+
+// A density-boundary row in 32 bytes (two 16-byte loads): the receiving voxel, the other
+// voxel of its first pair, the first pair's law with the SERCA scale inline, and the
+// entries of any further pairs.
+enum : unsigned { DROW_APPLY = 1u, DROW_TO = 2u, DROW_SERCA = 4u };
+struct alignas(16) DensityRow {
+  int v, vo;                         // receiving voxel, other voxel of the first pair (field indices)
+  int r;                             // realisation
+  int more_begin;                    // further pairs: entries[more_begin .. more_begin + nmore)
+  double scale;                      // first pair, kind SERCA: the flux scale (FluxParams::p[9])
+  unsigned meta0;                    // first pair's parameter block (bits 0-15), species (16-23), dsi (24-31)
+  unsigned meta1;                    // DROW_* flags (bits 0-7), nmore (8-15)
+};
+static_assert(sizeof(DensityRow) == 32, "density row");
+
 // One boundary pair (species voxels), with the law applied across it.
 struct FluxPair {
   int r;                  // realisation

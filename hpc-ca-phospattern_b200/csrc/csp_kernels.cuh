@@ -369,10 +369,71 @@ __global__ void __launch_bounds__(256, CH ? 4 : 8) k_boundaries(const RealDesc* 
   }
 }
 
+// The step record of a realisation's running step (see StepRec).
+__host__ __device__ inline void write_steprec(const RealDesc& D, const RealCtl& C, StepRec& R) {
+  unsigned pre, updated, sub;
+  step_masks(D, C.step + 1, pre, updated, sub);
+  R.active = C.stopped ? 0u : 1u;
+  R.cur = C.cur_mask[C.step & 1];
+  R.updated = updated;
+  R.sub = sub;
+}
+
+// Density-boundary rows (voxels touched by density pairs only: the SERCA sheets), one
+// thread per row: what k_boundaries<false> computes -- the flux of every pair of the row
+// in pair order, summed in FP64, added to the voxel's new value with one rounding -- from
+// a 32-byte row, the realisation's step record and the voxel's new value loaded together
+// with the pair's old values (three dependent loads instead of five).
+__global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restrict__ descs,
+                                                          const StepRec* __restrict__ rec,
+                                                          const DensityRow* __restrict__ rows, int nrows,
+                                                          const FluxEntry* __restrict__ entries,
+                                                          const FluxPair* __restrict__ pairs,
+                                                          const FluxParams* __restrict__ params) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nrows) return;
+  const int4 a = __ldg(reinterpret_cast<const int4*>(rows + i));          // v, vo, r, more_begin
+  const int4 b = __ldg(reinterpret_cast<const int4*>(rows + i) + 1);      // scale, meta0, meta1
+  const uint4 R = __ldg(reinterpret_cast<const uint4*>(rec + a.z));       // active, cur, updated, sub
+  if (!R.x) return;
+  const RealDesc& D = descs[a.z];
+  const unsigned meta0 = (unsigned)b.z, meta1 = (unsigned)b.w;
+  const int sp = (int)((meta0 >> 16) & 0xffu), dsi = (int)(meta0 >> 24);
+  const unsigned sel = (R.y >> sp) & 1u;
+  const float* __restrict__ uold = D.u[sel][sp];
+  float* __restrict__ unew = D.u[sel ^ 1u][sp];
+  const bool write = (meta1 & DROW_APPLY) && (R.z >> sp & 1u);
+  const float nv = write ? unew[a.x] : 0.f;
+  double acc = 0.0;
+  bool any = false;
+  if (R.w >> dsi & 1u) {
+    const double us = (double)__ldg(uold + a.x), uo = (double)__ldg(uold + a.y);
+    const bool to = meta1 & DROW_TO;
+    const double u0 = to ? uo : us, u1 = to ? us : uo;
+    const double J = (meta1 & DROW_SERCA) ? serca_flux_fast(u0, u1, __hiloint2double(b.y, b.x))
+                                          : ryr_flux(D.dt, D.h, u0, u1, params[meta0 & 0xffffu].p);
+    acc += to ? J : -J;
+    any = true;
+  }
+  const int nmore = (int)((meta1 >> 8) & 0xffu);
+  for (int e = a.w; e < a.w + nmore; e++) {
+    const FluxEntry en = entries[e];
+    const FluxPair pr = pairs[en.pair];
+    if (!(R.w >> pr.dsi & 1u)) continue;
+    const FluxParams& fp = params[pr.param];
+    const double u0 = (double)__ldg(uold + pr.v0), u1 = (double)__ldg(uold + pr.v1);
+    const double J = pr.kind == FLUX_SERCA ? serca_flux_fast(u0, u1, fp.p[9]) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
+    acc += (double)en.sign * J;
+    any = true;
+  }
+  if (any && write) unew[a.x] = (float)((double)nv + acc);
+}
+
 // Step epilogue, one thread per realisation, after the boundary kernel: advance the
 // step counter, apply the abort rule (species.c:3476-3486) on the openness counted by
 // the boundary kernel, stop at the last step.
-__global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl, int nreal) {
+__global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl, StepRec* __restrict__ rec,
+                           int nreal) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nreal) return;
   RealCtl& C = ctl[r];
@@ -393,6 +454,7 @@ __global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restri
     }
   }
   if (C.step >= D.total_steps) C.stopped = 1;
+  write_steprec(D, C, rec[r]);
 }
 
 // Output reductions: partial min / max / sum over a block for one species of one

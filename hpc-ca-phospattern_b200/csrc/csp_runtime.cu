@@ -135,6 +135,8 @@ struct csp_handle {
   size_t stage_elems = 0;
   int nrows = 0, nch = 0;
   int nrows_density = 0;             // rows [0, nrows_density) have density pairs only
+  DensityRow* d_drows = nullptr;     // the density rows in 32 bytes (null: k_boundaries<false>)
+  StepRec* d_rec = nullptr;          // per realisation: what its running step does
   int max_plane_vox = 0;
   long long max_vox = 0;
   int kernel = 0;                 // 0 staged, 1 direct
@@ -794,6 +796,30 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
   std::stable_partition(rows.begin(), rows.end(), [&](const FluxRow& rw) { return !has_channel(rw); });
   h->nrows_density = 0;
   while (h->nrows_density < h->nrows && !has_channel(rows[h->nrows_density])) h->nrows_density++;
+  // the density rows in 32 bytes, when every one fits the compact form
+  std::vector<DensityRow> drows;
+  for (int i = 0; i < h->nrows_density; i++) {
+    const FluxRow& rw = rows[i];
+    const RealDesc& D = h->real[rw.r].desc;
+    const long long lim = 0x7fffffffll;
+    const bool to = rw.v == rw.v1 && rw.sign > 0.f, from = rw.v == rw.v0 && rw.sign < 0.f;
+    const long long vo = to ? rw.v0 : rw.v1;
+    if (!(to || from) || rw.v > lim || vo > lim || rw.v < 0 || vo < 0 || rw.param < 0 || rw.param > 0xffff ||
+        rw.species >= NS || rw.dsi >= D.ndiff || rw.more_end - rw.more_begin > 0xff) {
+      drows.clear();
+      break;
+    }
+    DensityRow d;
+    d.v = (int)rw.v;
+    d.vo = (int)vo;
+    d.r = rw.r;
+    d.more_begin = rw.more_begin;
+    d.scale = rw.kind == FLUX_SERCA ? params[rw.param].p[9] : 0.0;
+    d.meta0 = (unsigned)rw.param | ((unsigned)rw.species << 16) | ((unsigned)rw.dsi << 24);
+    d.meta1 = (rw.apply ? DROW_APPLY : 0u) | (to ? DROW_TO : 0u) | (rw.kind == FLUX_SERCA ? DROW_SERCA : 0u) |
+              ((unsigned)(rw.more_end - rw.more_begin) << 8);
+    drows.push_back(d);
+  }
   auto upload = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (bytes == 0) bytes = 16;
     if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
@@ -817,7 +843,11 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     off += (int)h->real[r].cls.size();
     descs[r] = h->real[r].desc;
   }
-  bool ok = upload((void**)&h->d_rows, rows.empty() ? nullptr : rows.data(), rows.size() * sizeof(FluxRow)) &&
+  std::vector<StepRec> recs(n);
+  for (int r = 0; r < n; r++) write_steprec(descs[r], ctl[r], recs[r]);
+  bool ok = upload((void**)&h->d_rec, recs.data(), recs.size() * sizeof(StepRec)) &&
+            (drows.empty() || upload((void**)&h->d_drows, drows.data(), drows.size() * sizeof(DensityRow))) &&
+            upload((void**)&h->d_rows, rows.empty() ? nullptr : rows.data(), rows.size() * sizeof(FluxRow)) &&
             upload((void**)&h->d_entries, entries.empty() ? nullptr : entries.data(), entries.size() * sizeof(FluxEntry)) &&
             upload((void**)&h->d_pairs, pairs.empty() ? nullptr : pairs.data(), pairs.size() * sizeof(FluxPair)) &&
             upload((void**)&h->d_params, params.empty() ? nullptr : params.data(), params.size() * sizeof(FluxParams)) &&
@@ -853,7 +883,10 @@ static void launch_voxels(csp_handle* h) {
 
 static void launch_boundaries(csp_handle* h) {
   const int nd = h->nrows_density, nc = h->nrows - h->nrows_density;
-  if (nd > 0)
+  if (nd > 0 && h->d_drows)
+    k_density_rows<<<(nd + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_rec, h->d_drows, nd, h->d_entries,
+                                                            h->d_pairs, h->d_params);
+  else if (nd > 0)
     k_boundaries<false><<<(nd + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, nd, h->d_entries,
                                                                   h->d_pairs, h->d_params, h->d_states,
                                                                   std::max(h->nch, 1));
@@ -867,7 +900,7 @@ static void launch_boundaries(csp_handle* h) {
     k_react_surrogate<<<grid, MLP_DEPLOY_T, MLP_DEPLOY_SMEM, h->stream>>>(h->d_desc, h->d_ctl, h->d_mlp,
                                                                           h->surrogate_tol, h->d_mlp_cnt);
   }
-  k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->n);
+  k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rec, h->n);
 }
 
 static cudaError_t launch_step(csp_handle* h) {
@@ -1574,6 +1607,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   staged_release(h->plan);
   cudaFree(h->d_fields); cudaFree(h->d_dom); cudaFree(h->d_cls); cudaFree(h->d_desc); cudaFree(h->d_ctl);
+  cudaFree(h->d_rec); cudaFree(h->d_drows);
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
   cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
   cudaFree(h->d_stage);
