@@ -90,8 +90,10 @@ struct alignas(16) StepRec {
 
 // A density-boundary row in 32 bytes (two 16-byte loads): the receiving voxel, the other
 // voxel of its first pair, the first pair's law with the SERCA scale inline, and the
-// entries of any further pairs.
-enum : unsigned { DROW_APPLY = 1u, DROW_TO = 2u, DROW_SERCA = 4u };
+// entries of any further pairs.  A pair row (DROW_PAIR) stands for the two rows of a pair
+// whose voxels touch no other pair: v is the "to" voxel, vo the "from" voxel, and the one
+// flux goes to both (DROW_APPLY: to v, DROW_APPLY_FROM: to vo).
+enum : unsigned { DROW_APPLY = 1u, DROW_TO = 2u, DROW_SERCA = 4u, DROW_PAIR = 8u, DROW_APPLY_FROM = 16u };
 struct alignas(16) DensityRow {
   int v, vo;                         // receiving voxel, other voxel of the first pair (field indices)
   int r;                             // realisation

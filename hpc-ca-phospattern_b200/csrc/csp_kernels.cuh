@@ -383,7 +383,9 @@ __host__ __device__ inline void write_steprec(const RealDesc& D, const RealCtl& 
 // thread per row: what k_boundaries<false> computes -- the flux of every pair of the row
 // in pair order, summed in FP64, added to the voxel's new value with one rounding -- from
 // a 32-byte row, the realisation's step record and the voxel's new value loaded together
-// with the pair's old values (three dependent loads instead of five).
+// with the pair's old values (three dependent loads instead of five).  A pair row gives
+// both voxels of a pair their flux from one evaluation (each voxel still gets exactly the
+// value its own row would give: 0 + J or 0 - J, then one rounding).
 __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restrict__ descs,
                                                           const StepRec* __restrict__ rec,
                                                           const DensityRow* __restrict__ rows, int nrows,
@@ -402,8 +404,11 @@ __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restr
   const unsigned sel = (R.y >> sp) & 1u;
   const float* __restrict__ uold = D.u[sel][sp];
   float* __restrict__ unew = D.u[sel ^ 1u][sp];
-  const bool write = (meta1 & DROW_APPLY) && (R.z >> sp & 1u);
+  const bool upd = R.z >> sp & 1u;
+  const bool write = (meta1 & DROW_APPLY) && upd;
+  const bool write_from = (meta1 & DROW_APPLY_FROM) && upd;     // pair rows only
   const float nv = write ? unew[a.x] : 0.f;
+  const float nvo = write_from ? unew[a.y] : 0.f;
   double acc = 0.0;
   bool any = false;
   if (R.w >> dsi & 1u) {
@@ -414,6 +419,7 @@ __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restr
                                           : ryr_flux(D.dt, D.h, u0, u1, params[meta0 & 0xffffu].p);
     acc += to ? J : -J;
     any = true;
+    if (write_from) unew[a.y] = (float)((double)nvo + -J);       // the "from" voxel's own row
   }
   const int nmore = (int)((meta1 >> 8) & 0xffu);
   for (int e = a.w; e < a.w + nmore; e++) {

@@ -136,6 +136,7 @@ struct csp_handle {
   int nrows = 0, nch = 0;
   int nrows_density = 0;             // rows [0, nrows_density) have density pairs only
   DensityRow* d_drows = nullptr;     // the density rows in 32 bytes (null: k_boundaries<false>)
+  int ndrows = 0;                    // compact rows (pair rows count once)
   StepRec* d_rec = nullptr;          // per realisation: what its running step does
   int max_plane_vox = 0;
   long long max_vox = 0;
@@ -820,6 +821,34 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
               ((unsigned)(rw.more_end - rw.more_begin) << 8);
     drows.push_back(d);
   }
+  // pairs whose two voxels have single-pair rows: one pair row instead of two rows
+  if (!drows.empty()) {
+    std::vector<int> byv(drows.size());
+    for (size_t i = 0; i < byv.size(); i++) byv[i] = (int)i;
+    std::sort(byv.begin(), byv.end(), [&](int x, int y) {
+      return drows[x].r != drows[y].r ? drows[x].r < drows[y].r : drows[x].v < drows[y].v;
+    });
+    std::vector<char> gone(drows.size(), 0);
+    for (size_t i = 0; i < drows.size(); i++) {
+      DensityRow& t = drows[i];
+      if (!(t.meta1 & DROW_TO) || (t.meta1 >> 8) != 0u) continue;
+      auto it = std::lower_bound(byv.begin(), byv.end(), 0, [&](int x, int) {
+        return drows[x].r != t.r ? drows[x].r < t.r : drows[x].v < t.vo;
+      });
+      if (it == byv.end() || drows[*it].r != t.r || drows[*it].v != t.vo) continue;
+      const DensityRow& f = drows[*it];
+      if ((f.meta1 & (DROW_TO | DROW_PAIR)) || (f.meta1 >> 8) != 0u || f.vo != t.v || f.meta0 != t.meta0 ||
+          gone[*it])
+        continue;
+      t.meta1 |= DROW_PAIR | ((f.meta1 & DROW_APPLY) ? DROW_APPLY_FROM : 0u);
+      gone[*it] = 1;
+    }
+    size_t k = 0;
+    for (size_t i = 0; i < drows.size(); i++)
+      if (!gone[i]) drows[k++] = drows[i];
+    drows.resize(k);
+  }
+  h->ndrows = (int)drows.size();
   auto upload = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (bytes == 0) bytes = 16;
     if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
@@ -884,8 +913,8 @@ static void launch_voxels(csp_handle* h) {
 static void launch_boundaries(csp_handle* h) {
   const int nd = h->nrows_density, nc = h->nrows - h->nrows_density;
   if (nd > 0 && h->d_drows)
-    k_density_rows<<<(nd + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_rec, h->d_drows, nd, h->d_entries,
-                                                            h->d_pairs, h->d_params);
+    k_density_rows<<<(h->ndrows + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_rec, h->d_drows, h->ndrows,
+                                                                   h->d_entries, h->d_pairs, h->d_params);
   else if (nd > 0)
     k_boundaries<false><<<(nd + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, nd, h->d_entries,
                                                                   h->d_pairs, h->d_params, h->d_states,
