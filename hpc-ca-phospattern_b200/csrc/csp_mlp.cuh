@@ -344,9 +344,46 @@ namespace csp {
 // any of its voxels needs it.  counters[0] += voxels, counters[1] += voxels the network
 // ran for, counters[2] += voxels that took the plain integrator.
 constexpr int MLP_DEPLOY_T = 256;
-constexpr int MLP_DEPLOY_VPT = 32;       // voxels per thread (grid-stride within the realisation)
+constexpr int MLP_DEPLOY_VPT = 128;      // voxels per thread (grid-stride within the realisation)
 constexpr size_t MLP_DEPLOY_SMEM = sizeof(MlpTC) + sizeof(float) * (size_t)MLP_TC_STAGE * (MLP_DEPLOY_T / 32);
 
+// One voxel's reaction inputs and the new values they are added to.
+struct RxVoxel {
+  int d;                       // domain
+  bool mine;                   // in the grid and in a domain with buffers
+  float c, b[MLP_SLOTS];       // old Ca and buffers
+  float nc, nb[MLP_SLOTS];     // new Ca and buffers (after diffusion and boundary fluxes)
+};
+
+__device__ __forceinline__ void rx_fetch(const RealDesc& D, const RxConst* sk, unsigned cur, long long v,
+                                         long long nvox, RxVoxel& X) {
+  X.mine = false;
+  X.d = 0;
+  X.c = X.nc = 0.f;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) X.b[q] = X.nb[q] = 0.f;
+  if (v >= nvox || v % D.P >= D.plane) return;
+  X.d = D.dom[v] & DOMAIN_BITS;
+  const RxConst& kc = sk[X.d];
+  bool any = false;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) any = any || kc.tot[q] > 0.f;
+  if (!any) return;
+  X.mine = true;
+  X.c = D.u[cur & 1u][0][v];
+  X.nc = D.u[(cur & 1u) ^ 1u][0][v];
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    const int s = q + 1;
+    if (kc.tot[q] > 0.f) {
+      X.b[q] = D.u[(cur >> s) & 1u][s][v];
+      X.nb[q] = D.u[((cur >> s) & 1u) ^ 1u][s][v];
+    }
+  }
+}
+
+// Each thread walks MLP_DEPLOY_VPT voxels; the next voxel's values are loaded before the
+// current voxel's network pass, so the loads overlap the warp's tensor-core work.
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
                                                                   const RealCtl* __restrict__ ctl,
                                                                   const float* __restrict__ params, float tol,
@@ -371,39 +408,33 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   const unsigned cur = C.cur_mask[k & 1];
   const float dtr = (float)(D.dt * D.reaction_substep);
   unsigned n_vox = 0, n_net = 0, n_fall = 0;
+  const long long v0 = (long long)blockIdx.x * span + threadIdx.x;
+  RxVoxel X;
+  rx_fetch(D, sk, cur, v0, nvox, X);
   for (int it = 0; it < MLP_DEPLOY_VPT; it++) {
-    const long long v = (long long)blockIdx.x * span + (long long)it * MLP_DEPLOY_T + threadIdx.x;
-    const long long p = v % D.P;
-    bool mine = v < nvox && p < D.plane;
-    int d = 0;
-    if (mine) {
-      d = D.dom[v] & DOMAIN_BITS;
-      bool any = false;
-      for (int q = 0; q < MLP_SLOTS; q++) any = any || sk[d].tot[q] > 0.f;
-      mine = any;
-    }
+    const long long v = v0 + (long long)it * MLP_DEPLOY_T;
+    const RxVoxel Y = X;
+    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(D, sk, cur, v + MLP_DEPLOY_T, nvox, X);
+    const int d = Y.d;
     const RxConst& kc = sk[d];
-    float b[MLP_SLOTS], db[MLP_SLOTS], dc = 0.f, c = 0.f, x[MLP_IN], t[MLP_OUT];
-    for (int q = 0; q < MLP_SLOTS; q++) b[q] = 0.f;
+    const float c = Y.c;
+    float b[MLP_SLOTS], db[MLP_SLOTS], dc = 0.f, x[MLP_IN], t[MLP_OUT];
+#pragma unroll
+    for (int q = 0; q < MLP_SLOTS; q++) b[q] = Y.b[q];
     bool elig = false, skip = false;
-    if (mine) {
-      c = D.u[cur & 1u][0][v];
-      for (int q = 0; q < MLP_SLOTS; q++) {
-        const int s = q + 1;
-        b[q] = (kc.tot[q] > 0.f) ? D.u[(cur >> s) & 1u][s][v] : 0.f;
-      }
+    if (Y.mine) {
       elig = (D.mlp_domains >> d) & 1u;
       float S[MLP_SLOTS], smax = 0.f;
       rx_scale<float>(kc, dtr, c, b, S);
       for (int q = 0; q < MLP_SLOTS; q++) smax = fmaxf(smax, S[q]);
       skip = elig && smax <= MLP_SKIP;
     }
-    const bool net = mine && elig && !skip;
+    const bool net = Y.mine && elig && !skip;
     if (net) rx_features(kc, d, dtr, c, b, x);
     else
       for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
     if (__any_sync(0xffffffffu, net)) mlp_forward_tc(T, stage, x, t);   // the whole warp
-    if (!mine) continue;
+    if (!Y.mine) continue;
     bool ok;
     n_vox++;
     if (skip) {
@@ -428,22 +459,20 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
       dc = (float)dcd;
     }
     const unsigned fm = D.fixed_mask[d];
+#pragma unroll
     for (int q = 0; q < MLP_SLOTS; q++) {
       const int s = q + 1;
       if (kc.tot[q] <= 0.f || (fm >> s & 1u)) continue;
-      float* un = D.u[((cur >> s) & 1u) ^ 1u][s];
-      un[v] = __fadd_rn(un[v], db[q]);
+      D.u[((cur >> s) & 1u) ^ 1u][s][v] = __fadd_rn(Y.nb[q], db[q]);
     }
     bool face = false;
     if (D.dirichlet) {
+      const long long p = v % D.P;
       const long long c0 = v / D.P;
       const int c1 = (int)(p / D.nz), c2 = (int)(p % D.nz);
       face = c0 == 0 || c0 == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
     }
-    if (!(fm & 1u) && !face) {
-      float* un = D.u[(cur & 1u) ^ 1u][0];
-      un[v] = __fadd_rn(un[v], dc);
-    }
+    if (!(fm & 1u) && !face) D.u[(cur & 1u) ^ 1u][0][v] = __fadd_rn(Y.nc, dc);
   }
   if (n_vox) atomicAdd(&s_vox, n_vox);
   if (n_net) atomicAdd(&s_net, n_net);
