@@ -355,35 +355,88 @@ struct RxVoxel {
   float nc, nb[MLP_SLOTS];     // new Ca and buffers (after diffusion and boundary fluxes)
 };
 
-__device__ __forceinline__ void rx_fetch(const RealDesc& D, const RxConst* sk, unsigned cur, long long v,
-                                         long long nvox, RxVoxel& X) {
+// p = v mod D.P (the position within the plane), tracked by the caller; uo / un = the
+// old / new buffer of every species, dom = the domain bytes (block-shared copies).
+__device__ __forceinline__ void rx_fetch(const float* const* uo, const float* const* un,
+                                         const unsigned char* __restrict__ dom, int plane, const RxConst* sk,
+                                         long long v, int p, long long nvox, RxVoxel& X) {
   X.mine = false;
   X.d = 0;
   X.c = X.nc = 0.f;
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) X.b[q] = X.nb[q] = 0.f;
-  if (v >= nvox || v % D.P >= D.plane) return;
-  X.d = D.dom[v] & DOMAIN_BITS;
+  if (v >= nvox || p >= plane) return;
+  X.d = dom[v] & DOMAIN_BITS;
   const RxConst& kc = sk[X.d];
   bool any = false;
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) any = any || kc.tot[q] > 0.f;
   if (!any) return;
   X.mine = true;
-  X.c = D.u[cur & 1u][0][v];
-  X.nc = D.u[(cur & 1u) ^ 1u][0][v];
+  X.c = uo[0][v];
+  X.nc = un[0][v];
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
-    const int s = q + 1;
     if (kc.tot[q] > 0.f) {
-      X.b[q] = D.u[(cur >> s) & 1u][s][v];
-      X.nb[q] = D.u[((cur >> s) & 1u) ^ 1u][s][v];
+      X.b[q] = uo[q + 1][v];
+      X.nb[q] = un[q + 1][v];
     }
   }
 }
 
-// Each thread walks MLP_DEPLOY_VPT voxels; the next voxel's values are loaded before the
-// current voxel's network pass, so the loads overlap the warp's tensor-core work.
+// Near equilibrium (every S_s <= MLP_SKIP), with S_s <= MLP_SKIP tested as
+// lam |g| + k_on (tot - b) |G| <= thr_s, thr_s = MLP_SKIP tot_s / (dt_r^2 / 2) (no division).
+__device__ __forceinline__ bool rx_near_equilibrium(const RxConst& k, const float* thr, float c, const float* b) {
+  float G = 0.f;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++)
+    if (k.tot[q] > 0.f) G += rx_g<float>(k, q, c, b[q]);
+  const float aG = fabsf(G);
+  bool near = true;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (k.tot[q] <= 0.f) continue;
+    const float g = rx_g<float>(k, q, c, b[q]);
+    const float lam = k.koff[q] + k.kon[q] * c;
+    near = near && lam * fabsf(g) + k.kon[q] * (k.tot[q] - b[q]) * aG <= thr[q];
+  }
+  return near;
+}
+
+// The plain integrator's increments (the fallback), FP64, rounded to FP32.
+__device__ __forceinline__ void rx_fallback(const RxConst& kc, int n, double dt, float c, const float* b, float& dc,
+                                            float* db) {
+  double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
+  for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
+  rx_plain(kc, n, dt, (double)c, bd, dcd, dbd);
+  for (int q = 0; q < MLP_SLOTS; q++) db[q] = (float)dbd[q];
+  dc = (float)dcd;
+}
+
+// New values of one voxel: its buffers and Ca plus the increments, except fixed species
+// and, with Dirichlet faces (-f), Ca on the outer faces.
+__device__ __forceinline__ void rx_store(const RealDesc& D, const float* const* un, const RxConst& kc, int d, long long v,
+                                         bool face, float nc, const float* nb, float dc, const float* db) {
+  const unsigned fm = D.fixed_mask[d];
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    const int s = q + 1;
+    if (kc.tot[q] <= 0.f || (fm >> s & 1u)) continue;
+    const_cast<float*>(un[s])[v] = __fadd_rn(nb[q], db[q]);
+  }
+  if (!(fm & 1u) && !face) const_cast<float*>(un[0])[v] = __fadd_rn(nc, dc);
+}
+
+__device__ __forceinline__ bool rx_on_face(const RealDesc& D, int x, int p) {
+  const int c1 = p / D.nz, c2 = p - c1 * D.nz;
+  return x == 0 || x == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
+}
+
+// Each thread walks MLP_DEPLOY_VPT voxels, the next voxel's values loaded before the
+// current one is worked on.  Voxels near equilibrium and voxels of stiff domains are
+// finished at once; voxels that need the network are queued per warp (their indices in
+// shared memory) and the network runs on full tiles of 32 queued voxels, which reload
+// their state: the tensor-core passes carry no idle lanes but the last one.
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
                                                                   const RealCtl* __restrict__ ctl,
                                                                   const float* __restrict__ params, float tol,
@@ -392,6 +445,10 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   MlpTC& T = *reinterpret_cast<MlpTC*>(dsm);
   float* stage = dsm + sizeof(MlpTC) / sizeof(float) + (threadIdx.x >> 5) * MLP_TC_STAGE;
   __shared__ RxConst sk[ND];
+  __shared__ float s_thr[ND][MLP_SLOTS];
+  __shared__ const float* s_uo[NS];
+  __shared__ const float* s_un[NS];
+  __shared__ long long s_pend[MLP_DEPLOY_T / 32][64];   // per warp: queued voxels (up to two tiles)
   __shared__ unsigned s_vox, s_net, s_fall;
   const RealDesc& D = descs[blockIdx.y];
   const RealCtl& C = ctl[blockIdx.y];
@@ -401,79 +458,115 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   const long long nvox = (long long)D.nx * D.P;
   const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
   if ((long long)blockIdx.x * span >= nvox) return;  // uniform over the block
-  mlp_tc_load(T, params);
-  if (threadIdx.x < ND) sk[threadIdx.x] = rx_const(D, threadIdx.x < D.nd ? threadIdx.x : 0);
-  if (threadIdx.x == 0) { s_vox = 0; s_net = 0; s_fall = 0; }
-  __syncthreads();
   const unsigned cur = C.cur_mask[k & 1];
   const float dtr = (float)(D.dt * D.reaction_substep);
+  mlp_tc_load(T, params);
+  if (threadIdx.x < ND) {
+    const RxConst kc = rx_const(D, threadIdx.x < D.nd ? threadIdx.x : 0);
+    sk[threadIdx.x] = kc;
+    for (int q = 0; q < MLP_SLOTS; q++) s_thr[threadIdx.x][q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
+  }
+  if (threadIdx.x < NS) {
+    const int t = threadIdx.x;
+    s_uo[t] = D.u[(cur >> t) & 1u][t];
+    s_un[t] = D.u[((cur >> t) & 1u) ^ 1u][t];
+  }
+  if (threadIdx.x == 0) { s_vox = 0; s_net = 0; s_fall = 0; }
+  __syncthreads();
+  const unsigned char* __restrict__ dom = D.dom;
+  const int plane = D.plane;
+  const unsigned elig_mask = D.mlp_domains;
   unsigned n_vox = 0, n_net = 0, n_fall = 0;
   const long long v0 = (long long)blockIdx.x * span + threadIdx.x;
+  // position within the plane and plane index of the voxel being fetched, advanced by
+  // MLP_DEPLOY_T per iteration without divisions (one at the start)
+  const int P = D.P;
+  int pf = (int)(v0 % P), xf = (int)(v0 / P);
+  int pc = pf, xc = xf;
+  long long* pend = s_pend[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  int npend = 0;                                     // warp-uniform
+  // the network on queued voxels pend[0 .. count) (lane i takes pend[i]), whole warp
+  auto flush = [&](int count) {
+    __syncwarp();
+    const bool have = lane < count;
+    const long long v = have ? pend[lane] : 0;
+    RxVoxel Y;
+    int pq = 0, xq = 0;
+    if (have) {
+      xq = (int)(v / P);
+      pq = (int)(v - (long long)xq * P);
+    }
+    rx_fetch(s_uo, s_un, dom, plane, sk, have ? v : nvox, pq, nvox, Y);
+    const RxConst& kc = sk[Y.d];
+    float x[MLP_IN], t[MLP_OUT], db[MLP_SLOTS], dc = 0.f;
+    if (have) rx_features(kc, Y.d, dtr, Y.c, Y.b, x);
+    else
+      for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
+    mlp_forward_tc(T, stage, x, t);
+    if (have) {
+      n_vox++;
+      n_net++;
+      if (!rx_apply_output(kc, dtr, Y.c, Y.b, t, tol, dc, db)) {
+        n_fall++;
+        rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
+      }
+      rx_store(D, s_un, kc, Y.d, v, D.dirichlet && rx_on_face(D, xq, pq), Y.nc, Y.nb, dc, db);
+    }
+    __syncwarp();
+  };
   RxVoxel X;
-  rx_fetch(D, sk, cur, v0, nvox, X);
+  rx_fetch(s_uo, s_un, dom, plane, sk, v0, pf, nvox, X);
   for (int it = 0; it < MLP_DEPLOY_VPT; it++) {
     const long long v = v0 + (long long)it * MLP_DEPLOY_T;
     const RxVoxel Y = X;
-    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(D, sk, cur, v + MLP_DEPLOY_T, nvox, X);
+    pc = pf;
+    xc = xf;
+    pf += MLP_DEPLOY_T;
+    while (pf >= P) { pf -= P; xf++; }
+    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(s_uo, s_un, dom, plane, sk, v + MLP_DEPLOY_T, pf, nvox, X);
     const int d = Y.d;
     const RxConst& kc = sk[d];
-    const float c = Y.c;
-    float b[MLP_SLOTS], db[MLP_SLOTS], dc = 0.f, x[MLP_IN], t[MLP_OUT];
-#pragma unroll
-    for (int q = 0; q < MLP_SLOTS; q++) b[q] = Y.b[q];
     bool elig = false, skip = false;
     if (Y.mine) {
-      elig = (D.mlp_domains >> d) & 1u;
-      float S[MLP_SLOTS], smax = 0.f;
-      rx_scale<float>(kc, dtr, c, b, S);
-      for (int q = 0; q < MLP_SLOTS; q++) smax = fmaxf(smax, S[q]);
-      skip = elig && smax <= MLP_SKIP;
+      elig = (elig_mask >> d) & 1u;
+      skip = elig && rx_near_equilibrium(kc, s_thr[d], Y.c, Y.b);
     }
     const bool net = Y.mine && elig && !skip;
-    if (net) rx_features(kc, d, dtr, c, b, x);
-    else
-      for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
-    if (__any_sync(0xffffffffu, net)) mlp_forward_tc(T, stage, x, t);   // the whole warp
-    if (!Y.mine) continue;
-    bool ok;
-    n_vox++;
-    if (skip) {
-      // near equilibrium: the explicit increment
-      float sdb = 0.f;
-      for (int q = 0; q < MLP_SLOTS; q++) {
-        db[q] = kc.tot[q] > 0.f ? dtr * rx_g<float>(kc, q, c, b[q]) : 0.f;
-        sdb += db[q];
+    if (Y.mine && !net) {
+      float db[MLP_SLOTS], dc;
+      n_vox++;
+      if (skip) {
+        // near equilibrium: the explicit increment
+        float sdb = 0.f;
+        for (int q = 0; q < MLP_SLOTS; q++) {
+          db[q] = kc.tot[q] > 0.f ? dtr * rx_g<float>(kc, q, Y.c, Y.b[q]) : 0.f;
+          sdb += db[q];
+        }
+        dc = -sdb;
+      } else {
+        // a stiff domain: the plain integrator
+        n_fall++;
+        rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
       }
-      dc = -sdb;
-      ok = true;
-    } else {
-      ok = net && rx_apply_output(kc, dtr, c, b, t, tol, dc, db);
-      n_net += net;
+      rx_store(D, s_un, kc, d, v, D.dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db);
     }
-    if (!ok) {
-      n_fall++;
-      double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
-      for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
-      rx_plain(kc, D.reaction_substep, D.dt, (double)c, bd, dcd, dbd);
-      for (int q = 0; q < MLP_SLOTS; q++) db[q] = (float)dbd[q];
-      dc = (float)dcd;
+    const unsigned nm = __ballot_sync(0xffffffffu, net);
+    if (nm) {
+      if (net) pend[npend + __popc(nm & ((1u << lane) - 1u))] = v;
+      npend += __popc(nm);
+      if (npend >= 32) {
+        flush(32);
+        const int rest = npend - 32;
+        const long long mv = lane < rest ? pend[32 + lane] : 0;
+        __syncwarp();
+        if (lane < rest) pend[lane] = mv;
+        __syncwarp();
+        npend = rest;
+      }
     }
-    const unsigned fm = D.fixed_mask[d];
-#pragma unroll
-    for (int q = 0; q < MLP_SLOTS; q++) {
-      const int s = q + 1;
-      if (kc.tot[q] <= 0.f || (fm >> s & 1u)) continue;
-      D.u[((cur >> s) & 1u) ^ 1u][s][v] = __fadd_rn(Y.nb[q], db[q]);
-    }
-    bool face = false;
-    if (D.dirichlet) {
-      const long long p = v % D.P;
-      const long long c0 = v / D.P;
-      const int c1 = (int)(p / D.nz), c2 = (int)(p % D.nz);
-      face = c0 == 0 || c0 == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
-    }
-    if (!(fm & 1u) && !face) D.u[(cur & 1u) ^ 1u][0][v] = __fadd_rn(Y.nc, dc);
   }
+  if (npend) flush(npend);
   if (n_vox) atomicAdd(&s_vox, n_vox);
   if (n_net) atomicAdd(&s_net, n_net);
   if (n_fall) atomicAdd(&s_fall, n_fall);
