@@ -552,21 +552,20 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
       rx_store(D, s_un, kc, d, v, D.dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db);
     }
     const unsigned nm = __ballot_sync(0xffffffffu, net);
-    if (nm) {
-      if (net) pend[npend + __popc(nm & ((1u << lane) - 1u))] = v;
-      npend += __popc(nm);
-      if (npend >= 32) {
-        flush(32);
-        const int rest = npend - 32;
-        const long long mv = lane < rest ? pend[32 + lane] : 0;
-        __syncwarp();
-        if (lane < rest) pend[lane] = mv;
-        __syncwarp();
-        npend = rest;
-      }
+    if (net) pend[npend + __popc(nm & ((1u << lane) - 1u))] = v;
+    npend += __popc(nm);
+    // full tiles, and after the last voxel whatever is queued (one call site)
+    while (npend >= 32 || (npend > 0 && it == MLP_DEPLOY_VPT - 1)) {
+      const int cnt = min(npend, 32);
+      flush(cnt);
+      const int rest = npend - cnt;
+      const long long mv = lane < rest ? pend[32 + lane] : 0;
+      __syncwarp();
+      if (lane < rest) pend[lane] = mv;
+      __syncwarp();
+      npend = rest;
     }
   }
-  if (npend) flush(npend);
   if (n_vox) atomicAdd(&s_vox, n_vox);
   if (n_net) atomicAdd(&s_net, n_net);
   if (n_fall) atomicAdd(&s_fall, n_fall);
