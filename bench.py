@@ -307,6 +307,23 @@ def surrogate_run(pkg, specs, opts, W, K):
             "fallback_fraction": fb / vx if vx else None}
 
 
+def config_leg(pkg, specs, opts, W, K, workload):
+    """One more configuration on the same kernels: autotuned tile, W untimed steps, K steps
+    timed on the device (graph replay); voxel-steps summed over the realisations."""
+    sim = pkg.Simulation(specs, opts)
+    tune = sim.autotune(repeats=3)
+    sim.advance(W)
+    sim.advance(K)
+    ms = sim.last_ms()
+    nvox = sum(int(np.prod(s["voxels"].shape)) for s in specs)
+    tv, tb = sim.profile(8)
+    sim.close()
+    ch = tune["chosen"]
+    return {"value": nvox * K / (ms / 1e3), "unit": "voxel-steps/s", "ms_per_step": ms / K,
+            "voxel_kernel_ms": tv / 8, "boundary_ms": tb / 8, "voxels": nvox, "realisations": len(specs),
+            "tile": {"threads": ch["threads"], "x_planes_per_unit": ch["segment"]}, "workload": workload}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,7 +404,7 @@ def main():
     assert all(np.isfinite(o).all() for o in out)
 
     # ---- plain path: one realisation of the same workload on the same kernels ----
-    plain_single, sur = None, None
+    plain_single, sur, configs = None, None, None
     if args.extras:
         single = pkg.Simulation(specs[:1], opts[:1])
         single.advance(W)
@@ -396,6 +413,16 @@ def main():
         single.close()
         # ---- learned reaction surrogate (dt_update_react = 10 dt): train, deploy, time ----
         sur = surrogate_run(pkg, specs, opts, W, K)
+        # ---- configs 2 and 4 on the same kernels ----
+        s2, o2 = synth.config2()
+        s4, o4 = synth.config4()
+        configs = {
+            "config2": config_leg(pkg, [s2], [o2], W, K,
+                                  "one 200x200x100 grid at 6 nm, 10x10 RyR lattice with vacancies, 20 % pRyR"),
+            "config4": config_leg(pkg, s4, o4, W, K,
+                                  "64 grids from 64^3 to 256x256x128 at h = 6-10 nm (dt per realisation), "
+                                  "dt_update_react = 5 dt"),
+        }
 
     # ---- CPU baseline (rank 0, N=1 only): FP64 port of the reference ----
     cpu = None
@@ -442,6 +469,7 @@ def main():
                 "value": plain_single, "unit": "voxel-steps/s",
                 "workload": "one 100x100x50 realisation of the workload, same kernels"},
             "surrogate": sur,
+            "other_configs": configs,
             "gathered_realisations": gathered,
             "clocks": clk,
         }
