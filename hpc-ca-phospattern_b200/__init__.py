@@ -199,6 +199,30 @@ class Simulation:
         self._check(self.lib.csp_advance(self.h, int(nsteps), flags.ctypes.data_as(C.POINTER(C.c_int32))))
         return flags
 
+    def advance_async(self, nsteps):
+        """Launch nsteps steps and return at once (csp_advance_async)."""
+        self._check(self.lib.csp_advance_async(self.h, int(nsteps)))
+
+    def advance_wait(self):
+        """Wait for advance_async; returns the stop flags (csp_advance_wait)."""
+        flags = np.zeros(self.n, dtype=np.int32)
+        self._check(self.lib.csp_advance_wait(self.h, flags.ctypes.data_as(C.POINTER(C.c_int32))))
+        return flags
+
+    def snapshot_async(self, species_mask=None, r=0):
+        """Start an asynchronous copy of realisation r's fields (csp_snapshot_async)."""
+        if species_mask is None:
+            species_mask = (1 << self.shape(r)[0]) - 1
+        self._check(self.lib.csp_snapshot_async(self.h, r, int(species_mask)))
+        self._snap_shape = self.shape(r)
+
+    def snapshot_wait(self):
+        """Wait for snapshot_async; returns a copy of the fields ([species][x][y][z], FP64)."""
+        p = C.POINTER(C.c_double)()
+        self._check(self.lib.csp_snapshot_wait(self.h, C.byref(p)))
+        n = int(np.prod(self._snap_shape))
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(self._snap_shape).copy()
+
     def profile(self, nsteps):
         """Advance nsteps with per-kernel CUDA events: (voxel_ms, boundary_ms) summed."""
         a, b = C.c_float(), C.c_float()

@@ -245,6 +245,10 @@ def declare(lib):
         "csp_upload_state": (C.c_int, [h, C.c_int32, P(C.c_double)]),
         "csp_download_state": (C.c_int, [h, C.c_int32, P(C.c_double)]),
         "csp_advance": (C.c_int, [h, C.c_int64, P(C.c_int32)]),
+        "csp_advance_async": (C.c_int, [h, C.c_int64]),
+        "csp_advance_wait": (C.c_int, [h, P(C.c_int32)]),
+        "csp_snapshot_async": (C.c_int, [h, C.c_int32, C.c_uint32]),
+        "csp_snapshot_wait": (C.c_int, [h, P(P(C.c_double))]),
         "csp_reduce_outputs": (C.c_int, [h, C.c_int32, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_int32)]),
         "csp_get_channel_states": (C.c_int, [h, C.c_int32, C.c_int32, P(C.c_int32)]),
         "csp_linescan": (C.c_int, [h, C.c_int32, C.c_int32, C.c_int32, P(C.c_double), P(C.c_double), C.c_int32,

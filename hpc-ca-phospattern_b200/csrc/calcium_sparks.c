@@ -105,7 +105,7 @@ typedef struct run {
   int all_sp[CSP_MAX_SPECIES * 4], nall;
   int ls_species, ls_dom_ids[CSP_MAX_DOMAINS];
   double ls_offsets_nm[3];
-  double* state;                                 /* [ns][nx][ny][nz] for sheets / all_data */
+  int fields_pending;                            /* an output waits for its sheets / all_data */
   /* abort rule */
   double last_opened;
 } run;
@@ -334,8 +334,15 @@ static void print_table(run* R, const char* title, const double* v, int divide) 
 }
 
 /* One output (Species_output_data, species.c:2253-2340, with the linescan computed
- * first as calcium_sparks.c:177/208 do). */
-static void write_output(run* R, unsigned output_ind, double t, uint64_t time_ind) {
+ * first as calcium_sparks.c:177/208 do), in two parts.  begin_output: linescan,
+ * reductions, console tables, the group with its scalars, channel states and linescan,
+ * and -- when sheets or all_data are asked for -- an asynchronous copy of those species'
+ * fields (csp_snapshot_async).  finish_output: the sheets and all_data datasets from that
+ * copy and the file write; the main loop runs it while the device takes the next cycle's
+ * steps (csp_advance_async ... csp_advance_wait). */
+static void finish_output(run* R);
+
+static void begin_output(run* R, unsigned output_ind, double t, uint64_t time_ind) {
   cs_arguments* a = R->a;
   const csp_model* m = &R->m;
   const int ns = m->num_species, nd = m->num_domains;
@@ -416,44 +423,60 @@ static void write_output(run* R, unsigned output_ind, double t, uint64_t time_in
     if (cs_output_dataset(R->out, name, 1, &n, ls)) die("*** ERROR: output: %s\n", cs_output_error());
     free(ls);
   }
+  free(open);
   if (R->nsave || R->nall) {
-    const int* n = R->info.n;
-    const size_t nvox = (size_t)n[0] * n[1] * n[2];
-    check(R->h, csp_download_state(R->h, 0, R->state), "csp_download_state");
-    const char axc[3] = {'x', 'y', 'z'};
-    for (int q = 0; q < R->nsave; q++) {
-      const int s = R->save_sp[q];
-      const double* u = R->state + (size_t)s * nvox;
-      for (int ax = 0; ax < 3; ax++) {
-        const int lx = (ax + 1) % 3, ly = (ax + 2) % 3;
-        uint64_t dims[2] = {(uint64_t)n[lx], (uint64_t)n[ly]};
-        double* sheet = malloc(sizeof(double) * (size_t)(n[lx] * n[ly]));
-        for (int k = 0; k < R->sheets[ax]; k++) {
-          const int idx = R->sheet_idx[ax][k];
-          for (int i = 0; i < n[lx]; i++)
-            for (int j = 0; j < n[ly]; j++) {
-              int c[3];
-              c[ax] = idx; c[lx] = i; c[ly] = j;
-              sheet[(size_t)i * n[ly] + j] = u[((size_t)c[0] * n[1] + c[1]) * n[2] + c[2]];
-            }
-          char name[64];
-          snprintf(name, sizeof name, "%s_%c_sheet_%d", m->species_names[s], axc[ax], idx);
-          if (cs_output_dataset(R->out, name, 2, dims, sheet)) die("*** ERROR: output: %s\n", cs_output_error());
-        }
-        free(sheet);
+    uint32_t mask = 0;
+    for (int q = 0; q < R->nsave; q++) mask |= 1u << R->save_sp[q];
+    for (int q = 0; q < R->nall; q++) mask |= 1u << R->all_sp[q];
+    check(R->h, csp_snapshot_async(R->h, 0, mask), "csp_snapshot_async");
+    R->fields_pending = 1;
+  } else {
+    if (cs_output_flush(R->out)) die("*** ERROR: output: %s\n", cs_output_error());
+  }
+  pop_time(T_WRITE);
+}
+
+static void finish_output(run* R) {
+  if (!R->fields_pending) return;
+  R->fields_pending = 0;
+  push_time(T_WRITE);
+  const csp_model* m = &R->m;
+  const int* n = R->info.n;
+  const size_t nvox = (size_t)n[0] * n[1] * n[2];
+  const double* state = NULL;
+  check(R->h, csp_snapshot_wait(R->h, &state), "csp_snapshot_wait");
+  const char axc[3] = {'x', 'y', 'z'};
+  for (int q = 0; q < R->nsave; q++) {
+    const int s = R->save_sp[q];
+    const double* u = state + (size_t)s * nvox;
+    for (int ax = 0; ax < 3; ax++) {
+      const int lx = (ax + 1) % 3, ly = (ax + 2) % 3;
+      uint64_t dims[2] = {(uint64_t)n[lx], (uint64_t)n[ly]};
+      double* sheet = malloc(sizeof(double) * (size_t)(n[lx] * n[ly]));
+      for (int k = 0; k < R->sheets[ax]; k++) {
+        const int idx = R->sheet_idx[ax][k];
+        for (int i = 0; i < n[lx]; i++)
+          for (int j = 0; j < n[ly]; j++) {
+            int c[3];
+            c[ax] = idx; c[lx] = i; c[ly] = j;
+            sheet[(size_t)i * n[ly] + j] = u[((size_t)c[0] * n[1] + c[1]) * n[2] + c[2]];
+          }
+        char name[64];
+        snprintf(name, sizeof name, "%s_%c_sheet_%d", m->species_names[s], axc[ax], idx);
+        if (cs_output_dataset(R->out, name, 2, dims, sheet)) die("*** ERROR: output: %s\n", cs_output_error());
       }
-    }
-    for (int q = 0; q < R->nall; q++) {
-      const int s = R->all_sp[q];
-      char name[64];
-      snprintf(name, sizeof name, "%s_all_data", m->species_names[s]);
-      uint64_t dims[3] = {(uint64_t)n[0], (uint64_t)n[1], (uint64_t)n[2]};
-      if (cs_output_dataset(R->out, name, 3, dims, R->state + (size_t)s * nvox))
-        die("*** ERROR: output: %s\n", cs_output_error());
+      free(sheet);
     }
   }
+  for (int q = 0; q < R->nall; q++) {
+    const int s = R->all_sp[q];
+    char name[64];
+    snprintf(name, sizeof name, "%s_all_data", m->species_names[s]);
+    uint64_t dims[3] = {(uint64_t)n[0], (uint64_t)n[1], (uint64_t)n[2]};
+    if (cs_output_dataset(R->out, name, 3, dims, state + (size_t)s * nvox))
+      die("*** ERROR: output: %s\n", cs_output_error());
+  }
   if (cs_output_flush(R->out)) die("*** ERROR: output: %s\n", cs_output_error());
-  free(open);
   pop_time(T_WRITE);
 }
 
@@ -595,9 +618,6 @@ int main(int argc, char** argv) {
         R.sheet_idx[ax][i] = (int)floor(c / R.h_sim);
       }
     }
-    R.state = malloc(sizeof(double) * (size_t)m->num_species * n[0] * n[1] * n[2]);
-  } else if (a.all_data_num_species) {
-    R.state = malloc(sizeof(double) * (size_t)m->num_species * n[0] * n[1] * n[2]);
   }
   /* linescan (species.c:838-880) */
   if (a.linescan) {
@@ -641,7 +661,8 @@ int main(int argc, char** argv) {
   if (!R.out) die("*** ERROR: cannot create %s: %s\n", path, cs_output_error());
   pop_time(T_SETUP);
 
-  write_output(&R, 0, 0.0, 0);
+  begin_output(&R, 0, 0.0, 0);
+  finish_output(&R);
   unsigned output_ind = 0;
 
   push_time(T_MAINLOOP);
@@ -665,21 +686,23 @@ int main(int argc, char** argv) {
       }
     }
     int32_t flag = 0;
-    check(R.h, csp_advance(R.h, run_to - k, &flag), "csp_advance");
+    check(R.h, csp_advance_async(R.h, run_to - k), "csp_advance_async");
+    finish_output(&R);          /* the previous output's fields and file, while the device steps */
+    check(R.h, csp_advance_wait(R.h, &flag), "csp_advance_wait");
     for (long long j = k; j < run_to; j++) t += dt;
     k = run_to;
     if (stop) break;
     if (k == next_out) {
-      write_output(&R, ++output_ind, t, (uint64_t)k);
+      begin_output(&R, ++output_ind, t, (uint64_t)k);
       if (abort_check(&R, t)) break;
     }
   }
+  finish_output(&R);
   fflush(stdout);
   pop_time(T_MAINLOOP);
 
   if (cs_output_close(R.out)) die("*** ERROR: output: %s\n", cs_output_error());
   csp_destroy(R.h);
-  free(R.state);
   free(R.snapshot);
   cs_model_mem_free(&R.mem);
   pop_time(T_SIM);

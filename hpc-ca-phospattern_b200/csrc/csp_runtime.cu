@@ -133,6 +133,15 @@ struct csp_handle {
   double* d_red_out = nullptr;
   double* d_stage = nullptr;         // FP64 state staging of upload / download (one realisation)
   size_t stage_elems = 0;
+  // asynchronous snapshots: FP64 fields converted on the handle stream into d_snap, copied
+  // on snap_stream into the page-locked h_snap (ev_snap: converted, ev_copy: copied)
+  double* d_snap = nullptr;
+  double* h_snap = nullptr;
+  size_t snap_elems = 0;
+  cudaStream_t snap_stream = nullptr;
+  cudaEvent_t ev_snap = nullptr, ev_copy = nullptr;
+  bool snap_pending = false;
+  bool advance_pending = false;
   int nrows = 0, nch = 0;
   int nrows_density = 0;             // rows [0, nrows_density) have density pairs only
   DensityRow* d_drows = nullptr;     // the density rows in 32 bytes (null: k_boundaries<false>)
@@ -1005,8 +1014,7 @@ extern "C" int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_m
   return rc;
 }
 
-extern "C" int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags) {
-  if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
+static int launch_advance(csp_handle* h, int64_t nsteps) {
   int rc = ensure_graph(h);
   if (rc) return rc;
   CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
@@ -1017,9 +1025,35 @@ extern "C" int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags) {
   }
   while (left-- > 0) CUDA_TRY(h, launch_step(h));
   CUDA_TRY(h, cudaEventRecord(h->ev1, h->stream));
+  return CSP_OK;
+}
+
+extern "C" int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags) {
+  if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
+  if (h->advance_pending) return fail(h, CSP_EINVAL, "an asynchronous advance is pending (csp_advance_wait)");
+  int rc = launch_advance(h, nsteps);
+  if (rc) return rc;
   int rc2 = finish_advance(h, stop_flags);
   cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
   return rc2;
+}
+
+extern "C" int csp_advance_async(csp_handle* h, int64_t nsteps) {
+  if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
+  if (h->advance_pending) return fail(h, CSP_EINVAL, "an asynchronous advance is pending (csp_advance_wait)");
+  int rc = launch_advance(h, nsteps);
+  if (rc) return rc;
+  h->advance_pending = true;
+  return CSP_OK;
+}
+
+extern "C" int csp_advance_wait(csp_handle* h, int32_t* stop_flags) {
+  if (!h) return CSP_EINVAL;
+  if (!h->advance_pending) return fail(h, CSP_EINVAL, "no asynchronous advance is pending");
+  h->advance_pending = false;
+  int rc = finish_advance(h, stop_flags);
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  return rc;
 }
 
 static int read_ctl(csp_handle* h, int r, RealCtl& c) {
@@ -1120,6 +1154,69 @@ extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
   CUDA_TRY(h, cudaGetLastError());
   CUDA_TRY(h, cudaMemcpyAsync(u, h->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+// One species of the physical-order FP64 state (the species slot of k_state_out's output).
+__global__ void k_state_out_species(double* __restrict__ dst, StateMap m, int s) {
+  const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (v >= m.nvox) return;
+  const int z = (int)(v % m.n[2]);
+  const long long xy = v / m.n[2];
+  const int y = (int)(xy % m.n[1]), x = (int)(xy / m.n[1]);
+  dst[v] = (double)m.f[s][x * m.stride[0] + y * m.stride[1] + z * m.stride[2]];
+}
+
+extern "C" int csp_snapshot_async(csp_handle* h, int32_t r, uint32_t species_mask) {
+  if (!h) return CSP_EINVAL;
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  if (h->advance_pending) return fail(h, CSP_EINVAL, "an asynchronous advance is pending (csp_advance_wait)");
+  if (h->snap_pending) return fail(h, CSP_EINVAL, "a snapshot is pending (csp_snapshot_wait)");
+  StateMap m;
+  int rc = state_map(h, r, m);
+  if (rc) return rc;
+  const size_t need = (size_t)m.nvox * m.ns;
+  if (!h->snap_stream) {
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_snap, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_copy, cudaEventDisableTiming));
+  }
+  if (need > h->snap_elems) {
+    cudaFree(h->d_snap);
+    cudaFreeHost(h->h_snap);
+    h->d_snap = nullptr;
+    h->h_snap = nullptr;
+    h->snap_elems = 0;
+    if (cudaMalloc(&h->d_snap, need * sizeof(double)) != cudaSuccess ||
+        cudaHostAlloc(&h->h_snap, need * sizeof(double), cudaHostAllocDefault) != cudaSuccess)
+      return fail(h, CSP_ENOMEM, "snapshot buffers of %.1f MB", need * 8.0 / 1e6);
+    h->snap_elems = need;
+  }
+  // (the previous copy out of d_snap ended in csp_snapshot_wait)
+  for (int sp = 0; sp < m.ns; sp++) {
+    if (!(species_mask >> sp & 1u)) continue;
+    k_state_out_species<<<(unsigned)((m.nvox + 255) / 256), 256, 0, h->stream>>>(h->d_snap + (size_t)sp * m.nvox, m, sp);
+  }
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaEventRecord(h->ev_snap, h->stream));
+  CUDA_TRY(h, cudaStreamWaitEvent(h->snap_stream, h->ev_snap, 0));
+  for (int sp = 0; sp < m.ns; sp++) {
+    if (!(species_mask >> sp & 1u)) continue;
+    const size_t off = (size_t)sp * m.nvox;
+    CUDA_TRY(h, cudaMemcpyAsync(h->h_snap + off, h->d_snap + off, (size_t)m.nvox * sizeof(double),
+                                cudaMemcpyDeviceToHost, h->snap_stream));
+  }
+  CUDA_TRY(h, cudaEventRecord(h->ev_copy, h->snap_stream));
+  h->snap_pending = true;
+  return CSP_OK;
+}
+
+extern "C" int csp_snapshot_wait(csp_handle* h, const double** u) {
+  if (!h || !u) return CSP_EINVAL;
+  if (!h->snap_pending) return fail(h, CSP_EINVAL, "no snapshot is pending");
+  h->snap_pending = false;
+  CUDA_TRY(h, cudaEventSynchronize(h->ev_copy));
+  *u = h->h_snap;
   return CSP_OK;
 }
 
@@ -1640,6 +1737,12 @@ extern "C" void csp_destroy(csp_handle* h) {
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
   cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
   cudaFree(h->d_stage);
+  if (h->snap_stream) cudaStreamSynchronize(h->snap_stream);
+  cudaFree(h->d_snap);
+  cudaFreeHost(h->h_snap);
+  if (h->ev_snap) cudaEventDestroy(h->ev_snap);
+  if (h->ev_copy) cudaEventDestroy(h->ev_copy);
+  if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
   cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);

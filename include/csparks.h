@@ -201,6 +201,25 @@ int csp_download_state(csp_handle* h, int32_t r, double* u);
  * receives 1 for stopped realisations. */
 int csp_advance(csp_handle* h, int64_t nsteps, int32_t* stop_flags);
 
+/* csp_advance in two halves: launch nsteps steps and return at once, then wait for them
+ * and read the stop flags.  Between the two a caller may do host work (write the previous
+ * output) while the device steps; no other call of this handle may come between them but
+ * csp_snapshot_wait.  (The reference's loop body is synchronous, calcium_sparks.c:190-228;
+ * the split lets the output path of species.c:2253-2551 overlap the next cycle.) */
+int csp_advance_async(csp_handle* h, int64_t nsteps);
+int csp_advance_wait(csp_handle* h, int32_t* stop_flags);
+
+/* Start a copy of realisation r's fields to the host without waiting: the species in
+ * species_mask (bit s) are converted to FP64 on the handle stream, in the layout of
+ * csp_download_state ([num_species][nx][ny][nz]; species outside the mask are left
+ * unset), and copied on a second stream into a page-locked buffer owned by the handle, so
+ * the copy overlaps a csp_advance_async launched next.  csp_snapshot_wait waits for the
+ * copy and returns that buffer in *u, valid until the next csp_snapshot_async or
+ * csp_destroy.  Replaces the field reads of Species_output_data (species.c:2263-2298,
+ * 3027-3081: sheets and <sp>_all_data). */
+int csp_snapshot_async(csp_handle* h, int32_t r, uint32_t species_mask);
+int csp_snapshot_wait(csp_handle* h, const double** u);
+
 /* Per (domain, species) min / max / sum(u*dV) in FP64, and the channel openness of
  * every discrete boundary in boundary order (Species_output_scalar_data,
  * species.c:2785-2880).  min/max/total: [num_domains][num_species]; openness: all

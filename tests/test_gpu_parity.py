@@ -316,3 +316,40 @@ def test_uneven_ensemble_matches_oracle(pkg, oracle_mod, synth):
         orc.step(totals[r])
         assert_close(sim.state(r), orc.state(), what=f"uneven r={r}")
         np.testing.assert_array_equal(sim.channels(0, r), orc.channels(0))
+
+
+def test_async_advance_and_snapshot(pkg, synth):
+    """csp_advance_async / _wait give the fields of csp_advance; a snapshot started before
+    an asynchronous advance holds the fields from before it (the conversion is ordered
+    before the steps, the copy overlaps them); the species mask is honoured; misuse is an
+    error code."""
+    spec = synth.tiny((12, 12, 16))
+    opts = dict(h=6.0, tstop=5.0, seed=3, open_states={"ryr": [0, 2]})
+    a = pkg.Simulation(spec, opts)
+    b = pkg.Simulation(spec, opts)
+    a.advance(40)
+    b.advance_async(40)
+    b.advance_wait()
+    np.testing.assert_array_equal(a.state(), b.state())
+    u40 = b.state()
+    b.snapshot_async()
+    b.advance_async(30)
+    snap = b.snapshot_wait()
+    b.advance_wait()
+    np.testing.assert_array_equal(snap, u40)
+    a.advance(30)
+    u70 = a.state()
+    np.testing.assert_array_equal(u70, b.state())
+    b.snapshot_async(species_mask=0b101)
+    part = b.snapshot_wait()
+    np.testing.assert_array_equal(part[[0, 2]], u70[[0, 2]])
+    b.advance_async(1)
+    with pytest.raises(pkg.CspError):
+        b.advance(1)
+    b.advance_wait()
+    with pytest.raises(pkg.CspError):
+        b.advance_wait()
+    with pytest.raises(pkg.CspError):
+        b.snapshot_wait()
+    a.advance(1)
+    np.testing.assert_array_equal(a.state(), b.state())
