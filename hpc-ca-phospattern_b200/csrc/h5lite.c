@@ -8,6 +8,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/types.h>
+#include <unistd.h>
 #include <zlib.h>
 
 #define UNDEF 0xffffffffffffffffULL
@@ -85,6 +87,7 @@ static h5l_obj* obj_new(const char* name, int is_group) {
   h5l_obj* o = (h5l_obj*)calloc(1, sizeof(h5l_obj));
   o->name = strdup(name ? name : "");
   o->is_group = is_group;
+  o->file_addr = UNDEF;
   return o;
 }
 
@@ -600,6 +603,8 @@ h5l_file* h5l_create(const char* path) {
   f->writable = 1;
   f->dirty = 1;
   f->root = obj_new("", 1);
+  f->incremental = 1;
+  f->data_end = 96;                    /* after the superblock */
   return f;
 }
 
@@ -607,15 +612,22 @@ h5l_file* h5l_create(const char* path) {
 #define SYM_LEAF_K 32           /* symbol nodes of 64 entries */
 #define SYM_INT_K 32            /* B-tree nodes of 64 children */
 
+/* A byte buffer holding file addresses [base, n): b[0] is the byte at address base.
+ * place_data: datasets' raw data go into the buffer (whole-file writes), else they are
+ * already in the file at their file_addr (incremental flushes). */
 typedef struct {
   unsigned char* b;
   size_t n, cap;
+  uint64_t base;
+  int place_data;
 } wb_t;
+#define WB(w, at) ((w)->b + ((at) - (w)->base))
 
 static void wb_reserve(wb_t* w, size_t extra) {
-  if (w->n + extra > w->cap) {
+  const size_t used = w->n - w->base;
+  if (used + extra > w->cap) {
     size_t c = w->cap ? w->cap : 4096;
-    while (c < w->n + extra) c *= 2;
+    while (c < used + extra) c *= 2;
     w->b = (unsigned char*)realloc(w->b, c);
     w->cap = c;
   }
@@ -623,14 +635,14 @@ static void wb_reserve(wb_t* w, size_t extra) {
 static uint64_t wb_alloc(wb_t* w, size_t len) {   /* 8-byte aligned, zeroed */
   const size_t pad = (8 - (w->n & 7)) & 7;
   wb_reserve(w, pad + len);
-  memset(w->b + w->n, 0, pad + len);
+  memset(WB(w, w->n), 0, pad + len);
   w->n += pad;
   const uint64_t at = w->n;
   w->n += len;
   return at;
 }
 static void put(wb_t* w, uint64_t at, uint64_t v, int nb) {
-  for (int i = 0; i < nb; i++) w->b[at + i] = (unsigned char)(v >> (8 * i));
+  for (int i = 0; i < nb; i++) WB(w, at)[i] = (unsigned char)(v >> (8 * i));
 }
 
 static size_t dtype_size(const h5l_type* t) { return t->code == H5L_STR ? 8 : (t->code >= H5L_F32 && t->code <= H5L_F64) ? 20 : 12; }
@@ -692,7 +704,7 @@ static uint64_t write_header(wb_t* w, msg_t* m, int nm) {
   for (int i = 0; i < nm; i++) {
     put(w, p, m[i].type, 2);
     put(w, p + 2, A8(m[i].size), 2);
-    memcpy(w->b + p + 8, m[i].data, m[i].size);
+    memcpy(WB(w, p + 8), m[i].data, m[i].size);
     p += 8 + A8(m[i].size);
   }
   if (p < at + 16 + total) {           /* fill the rest with a NIL message */
@@ -700,7 +712,7 @@ static uint64_t write_header(wb_t* w, msg_t* m, int nm) {
     put(w, p + 2, at + 16 + total - p - 8, 2);
     nmsgs++;
   }
-  w->b[at] = 1;
+  WB(w, at)[0] = 1;
   put(w, at + 2, nmsgs, 2);
   put(w, at + 4, 1, 4);
   put(w, at + 8, total, 4);
@@ -714,7 +726,7 @@ static msg_t attr_msg(const h5l_attr* a) {
   m.type = 0x000C;
   m.size = 8 + A8(nl) + A8(ts) + A8(ss) + a->nbytes;
   m.data = (unsigned char*)calloc(1, m.size);
-  wb_t w = {m.data, m.size, m.size};
+  wb_t w = {m.data, m.size, m.size, 0, 0};
   m.data[0] = 1;
   put(&w, 2, nl, 2);
   put(&w, 4, ts, 2);
@@ -750,11 +762,11 @@ static int write_group(wb_t* w, h5l_obj* g, written_t* out) {
   size_t q = 8;
   for (int i = 0; i < n; i++) {
     noff[i] = q;
-    memcpy(w->b + hdata + q, g->children[i]->name, strlen(g->children[i]->name) + 1);
+    memcpy(WB(w, hdata + q), g->children[i]->name, strlen(g->children[i]->name) + 1);
     q += A8(strlen(g->children[i]->name) + 1);
   }
-  memcpy(w->b + heap, "HEAP", 4);
-  w->b[heap + 4] = 0;
+  memcpy(WB(w, heap), "HEAP", 4);
+  WB(w, heap)[4] = 0;
   put(w, heap + 8, hsz, 8);
   put(w, heap + 16, UNDEF, 8);
   put(w, heap + 24, hdata, 8);
@@ -765,8 +777,8 @@ static int write_group(wb_t* w, h5l_obj* g, written_t* out) {
   for (int s = 0; s < nsnod; s++) {
     const size_t sz = 8 + 40 * (size_t)per;
     snod[s] = wb_alloc(w, sz);
-    memcpy(w->b + snod[s], "SNOD", 4);
-    w->b[snod[s] + 4] = 1;
+    memcpy(WB(w, snod[s]), "SNOD", 4);
+    WB(w, snod[s])[4] = 1;
     const int first = s * per, cnt = (n - first) < per ? (n - first) : per;
     put(w, snod[s] + 6, cnt > 0 ? cnt : 0, 2);
     for (int k = 0; k < cnt; k++) {
@@ -784,9 +796,9 @@ static int write_group(wb_t* w, h5l_obj* g, written_t* out) {
   /* one leaf-level B-tree node over the symbol nodes */
   const size_t bsz = 24 + (2 * SYM_INT_K + 1) * 8 + 2 * SYM_INT_K * 8;
   const uint64_t bt = wb_alloc(w, bsz);
-  memcpy(w->b + bt, "TREE", 4);
-  w->b[bt + 4] = 0;
-  w->b[bt + 5] = 0;
+  memcpy(WB(w, bt), "TREE", 4);
+  WB(w, bt)[4] = 0;
+  WB(w, bt)[5] = 0;
   put(w, bt + 6, n ? nsnod : 0, 2);
   put(w, bt + 8, UNDEF, 8);
   put(w, bt + 16, UNDEF, 8);
@@ -802,7 +814,7 @@ static int write_group(wb_t* w, h5l_obj* g, written_t* out) {
   /* group object header: symbol table message + attributes */
   msg_t* m = (msg_t*)calloc(1 + g->nattrs, sizeof(msg_t));
   unsigned char st[16];
-  wb_t sw = {st, 16, 16};
+  wb_t sw = {st, 16, 16, 0, 0};
   put(&sw, 0, bt, 8);
   put(&sw, 8, heap, 8);
   m[0].type = 0x0011; m[0].size = 16; m[0].data = st;
@@ -820,8 +832,12 @@ static int write_group(wb_t* w, h5l_obj* g, written_t* out) {
 static int write_dataset(wb_t* w, h5l_obj* d, written_t* out) {
   uint64_t addr = UNDEF;
   if (d->nbytes) {
-    addr = wb_alloc(w, d->nbytes);
-    memcpy(w->b + addr, d->data, d->nbytes);
+    if (w->place_data) {
+      addr = wb_alloc(w, d->nbytes);
+      memcpy(WB(w, addr), d->data, d->nbytes);
+    } else {
+      addr = d->file_addr;
+    }
   }
   msg_t* m = (msg_t*)calloc(4 + d->nattrs, sizeof(msg_t));
   unsigned char ds[8 + 8 * H5L_MAX_DIMS], dt[20], fill[4] = {2, 1, 0, 0}, lay[18];
@@ -849,28 +865,78 @@ static int write_object(wb_t* w, h5l_obj* o, written_t* out) {
   return o->is_group ? write_group(w, o, out) : write_dataset(w, o, out);
 }
 
+/* The 96-byte version-0 superblock: root group entry and end-of-file address. */
+static void superblock(unsigned char* sb, const written_t* root, uint64_t eof) {
+  static const unsigned char sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
+  wb_t w = {sb, 96, 96, 0, 0};
+  memset(sb, 0, 96);
+  memcpy(sb, sig, 8);
+  sb[13] = 8; sb[14] = 8;
+  put(&w, 16, SYM_LEAF_K, 2);
+  put(&w, 18, SYM_INT_K, 2);
+  put(&w, 20, 0, 4);
+  put(&w, 24, 0, 8);                  /* base address */
+  put(&w, 32, UNDEF, 8);              /* free-space info */
+  put(&w, 40, eof, 8);                /* end of file */
+  put(&w, 48, UNDEF, 8);              /* driver info */
+  put(&w, 56, 0, 8);                  /* root entry: name offset */
+  put(&w, 64, root->header, 8);
+  put(&w, 72, 1, 4);                  /* cache type 1: symbol table scratch */
+  put(&w, 80, root->btree, 8);
+  put(&w, 88, root->heap, 8);
+}
+
+/* Raw data of every dataset not yet in the file, appended at *end. */
+static int place_new_data(FILE* fp, h5l_obj* o, uint64_t* end) {
+  if (o->is_group) {
+    for (int i = 0; i < o->nchildren; i++)
+      if (place_new_data(fp, o->children[i], end)) return -1;
+    return 0;
+  }
+  if (!o->nbytes || o->file_addr != UNDEF) return 0;
+  const uint64_t at = (*end + 7) & ~(uint64_t)7;
+  if (fseeko(fp, (off_t)at, SEEK_SET) || fwrite(o->data, 1, o->nbytes, fp) != o->nbytes) return -1;
+  o->file_addr = at;
+  *end = at + o->nbytes;
+  return 0;
+}
+
+static int flush_incremental(h5l_file* f) {
+  FILE* fp = fopen(f->path, f->flushed ? "r+b" : "w+b");
+  if (!fp) { seterr("cannot write %s: %s", f->path, strerror(errno)); return -1; }
+  uint64_t end = f->data_end;
+  if (place_new_data(fp, f->root, &end)) {
+    fclose(fp);
+    seterr("short write to %s", f->path);
+    return -1;
+  }
+  f->data_end = end;
+  wb_t w = {NULL, 0, 0, 0, 0};
+  w.base = w.n = (end + 7) & ~(uint64_t)7;
+  written_t root;
+  if (write_group(&w, f->root, &root)) { free(w.b); fclose(fp); return -1; }
+  unsigned char sb[96];
+  superblock(sb, &root, w.n);
+  const size_t len = w.n - w.base;
+  int bad = fseeko(fp, (off_t)w.base, SEEK_SET) || fwrite(w.b, 1, len, fp) != len;
+  bad = bad || fseeko(fp, 0, SEEK_SET) || fwrite(sb, 1, 96, fp) != 96;
+  bad = bad || fflush(fp) || ftruncate(fileno(fp), (off_t)w.n);
+  fclose(fp);
+  free(w.b);
+  if (bad) { seterr("short write to %s", f->path); return -1; }
+  f->flushed = 1;
+  f->dirty = 0;
+  return 0;
+}
+
 int h5l_flush(h5l_file* f) {
   if (!f->writable || !f->dirty) return 0;
-  wb_t w = {NULL, 0, 0};
+  if (f->incremental) return flush_incremental(f);
+  wb_t w = {NULL, 0, 0, 0, 1};
   const uint64_t sb = wb_alloc(&w, 96);
   written_t root;
   if (write_group(&w, f->root, &root)) { free(w.b); return -1; }
-  static const unsigned char sig[8] = {0x89, 'H', 'D', 'F', '\r', '\n', 0x1a, '\n'};
-  memcpy(w.b + sb, sig, 8);
-  w.b[sb + 8] = 0; w.b[sb + 9] = 0; w.b[sb + 10] = 0; w.b[sb + 11] = 0; w.b[sb + 12] = 0;
-  w.b[sb + 13] = 8; w.b[sb + 14] = 8;
-  put(&w, sb + 16, SYM_LEAF_K, 2);
-  put(&w, sb + 18, SYM_INT_K, 2);
-  put(&w, sb + 20, 0, 4);
-  put(&w, sb + 24, 0, 8);              /* base address */
-  put(&w, sb + 32, UNDEF, 8);          /* free-space info */
-  put(&w, sb + 40, w.n, 8);            /* end of file */
-  put(&w, sb + 48, UNDEF, 8);          /* driver info */
-  put(&w, sb + 56, 0, 8);              /* root entry: name offset */
-  put(&w, sb + 64, root.header, 8);
-  put(&w, sb + 72, 1, 4);              /* cache type 1: symbol table scratch */
-  put(&w, sb + 80, root.btree, 8);
-  put(&w, sb + 88, root.heap, 8);
+  superblock(WB(&w, sb), &root, w.n);
   FILE* fp = fopen(f->path, "wb");
   if (!fp) { free(w.b); seterr("cannot write %s: %s", f->path, strerror(errno)); return -1; }
   const size_t wr = fwrite(w.b, 1, w.n, fp);

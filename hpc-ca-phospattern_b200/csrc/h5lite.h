@@ -59,6 +59,7 @@ typedef struct h5l_obj {
   uint64_t dims[H5L_MAX_DIMS];
   unsigned char* data;        /* the whole dataset, file byte order (little endian) */
   size_t nbytes;
+  uint64_t file_addr;         /* created files: where the raw data were written (all ones: not yet) */
 } h5l_obj;
 
 typedef struct h5l_file {
@@ -66,6 +67,13 @@ typedef struct h5l_file {
   int writable;
   int dirty;
   h5l_obj* root;
+  /* Files made by h5l_create are flushed incrementally: every dataset's raw data are
+   * written once, at data_end, and only the metadata (after the raw data) and the
+   * superblock are rewritten; a dataset's data must not change after the flush that
+   * wrote them.  Files opened for writing are rewritten whole. */
+  int incremental;
+  int flushed;
+  uint64_t data_end;
 } h5l_file;
 
 /* last error message (thread local) */

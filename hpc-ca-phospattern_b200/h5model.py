@@ -39,6 +39,7 @@ def _load():
         lib.h5l_create.restype = C.c_void_p
         lib.h5l_create.argtypes = [C.c_char_p]
         lib.h5l_close.argtypes = [C.c_void_p]
+        lib.h5l_flush.argtypes = [C.c_void_p]
         lib.h5l_error.restype = C.c_char_p
         lib.h5l_get_attr.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, P(C.c_int), P(C.c_size_t), P(C.c_int),
                                      P(C.c_uint64), P(C.c_void_p), P(C.c_size_t)]
@@ -66,6 +67,11 @@ class H5:
             self.f = self.lib.h5l_open(path.encode(), 1 if mode == "a" else 0)
         if not self.f:
             raise OSError(f"{path}: {self.lib.h5l_error().decode()}")
+
+    def flush(self):
+        """Write the file as it stands (created files: the new datasets' data and the metadata)."""
+        if self.lib.h5l_flush(self.f):
+            raise OSError(f"{self.path}: {self.lib.h5l_error().decode()}")
 
     def close(self):
         if self.f:

@@ -72,3 +72,28 @@ def test_synth_files_read_back(tmp_path):
     for a, b in zip(back["boundaries"], spec["boundaries"]):
         np.testing.assert_array_equal(np.asarray(a["pairs"]), np.asarray(b["pairs"]).reshape(-1, 6))
     assert back["species"] == spec["species"]
+
+
+def test_h5lite_incremental_flushes(tmp_path):
+    """A created file is written incrementally: a later flush appends the new datasets'
+    data and rewrites only the metadata; everything reads back, attributes included."""
+    p = str(tmp_path / "inc.h5")
+    a = np.arange(200_000, dtype=np.float64)
+    b = np.linspace(0.0, 1.0, 5000)
+    with h5m.H5(p, "w") as f:
+        f.put_group("/data_0000000")
+        f.put_attr("/data_0000000", "time", np.array([0.5]))
+        f.put_dset("/data_0000000/Ca_all_data", a)
+        f.flush()
+        s1 = os.path.getsize(p)
+        f.put_group("/data_0000001")
+        f.put_dset("/data_0000001/Ca_all_data", b)
+        f.flush()
+        s2 = os.path.getsize(p)
+    assert s1 > a.nbytes
+    assert 0 < s2 - s1 < b.nbytes + 8192, (s1, s2)
+    with h5m.H5(p) as f:
+        np.testing.assert_array_equal(f.dset("/data_0000000/Ca_all_data"), a)
+        np.testing.assert_array_equal(f.dset("/data_0000001/Ca_all_data"), b)
+        assert float(np.ravel(f.attr("/data_0000000", "time"))[0]) == 0.5
+        assert sorted(n for _, n in f.list("/")) == ["data_0000000", "data_0000001"]
