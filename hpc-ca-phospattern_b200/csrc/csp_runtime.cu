@@ -1440,8 +1440,32 @@ extern "C" int csp_autotune(csp_handle* h, int32_t repeats, csp_tune_report* rep
   if (repeats < 1) repeats = 3;
   std::vector<RealDesc> descs(h->n);
   for (int r = 0; r < h->n; r++) descs[r] = h->real[r].desc;
-  const int cand[][2] = {{256, 0}, {256, 16}, {256, 32}, {256, 1 << 20}, {128, 0}, {128, 32}};
-  const int ncand = (int)(sizeof cand / sizeof cand[0]);
+  int cand[CSP_TUNE_MAX][2] = {{256, 0}, {256, 16}, {256, 32}, {256, 1 << 20}, {128, 0}, {128, 32}};
+  int ncand = 6;
+  // two more segment lengths for 256 threads from a cost model: rounds of work units over
+  // the resident CTAs times the planes a unit stages (its segment and two halo planes)
+  {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long ctas = 2ll * sms, L = 1024;
+    double best[2] = {1e300, 1e300};
+    int bseg[2] = {0, 0};
+    for (int seg = 8; seg <= 64; seg++) {
+      if (seg == 16 || seg == 32) continue;
+      long long units = 0;
+      for (const RealDesc& D : descs) units += (long long)((D.nx + seg - 1) / seg) * ((D.plane + L - 1) / L);
+      const double cost = (double)((units + ctas - 1) / ctas) * (seg + 2);
+      if (cost < best[0]) {
+        best[1] = best[0]; bseg[1] = bseg[0];
+        best[0] = cost; bseg[0] = seg;
+      } else if (cost < best[1]) {
+        best[1] = cost; bseg[1] = seg;
+      }
+    }
+    for (int k = 0; k < 2 && ncand < CSP_TUNE_MAX; k++)
+      if (bseg[k]) { cand[ncand][0] = 256; cand[ncand][1] = bseg[k]; ncand++; }
+  }
   cudaEvent_t e0, e1;
   CUDA_TRY(h, cudaEventCreate(&e0));
   CUDA_TRY(h, cudaEventCreate(&e1));
