@@ -386,19 +386,22 @@ __device__ __forceinline__ void rx_fetch(const float* const* uo, const float* co
 
 // Near equilibrium (every S_s <= MLP_SKIP), with S_s <= MLP_SKIP tested as
 // lam |g| + k_on (tot - b) |G| <= thr_s, thr_s = MLP_SKIP tot_s / (dt_r^2 / 2) (no division).
-__device__ __forceinline__ bool rx_near_equilibrium(const RxConst& k, const float* thr, float c, const float* b) {
+// g[] receives the reaction rates g_s (0 for absent buffers) for the explicit increment.
+__device__ __forceinline__ bool rx_near_equilibrium(const RxConst& k, const float* thr, float c, const float* b,
+                                                    float* g) {
   float G = 0.f;
 #pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++)
-    if (k.tot[q] > 0.f) G += rx_g<float>(k, q, c, b[q]);
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    g[q] = k.tot[q] > 0.f ? rx_g<float>(k, q, c, b[q]) : 0.f;
+    G += g[q];
+  }
   const float aG = fabsf(G);
   bool near = true;
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
     if (k.tot[q] <= 0.f) continue;
-    const float g = rx_g<float>(k, q, c, b[q]);
     const float lam = k.koff[q] + k.kon[q] * c;
-    near = near && lam * fabsf(g) + k.kon[q] * (k.tot[q] - b[q]) * aG <= thr[q];
+    near = near && lam * fabsf(g[q]) + k.kon[q] * (k.tot[q] - b[q]) * aG <= thr[q];
   }
   return near;
 }
@@ -415,9 +418,9 @@ __device__ __forceinline__ void rx_fallback(const RxConst& kc, int n, double dt,
 
 // New values of one voxel: its buffers and Ca plus the increments, except fixed species
 // and, with Dirichlet faces (-f), Ca on the outer faces.
-__device__ __forceinline__ void rx_store(const RealDesc& D, const float* const* un, const RxConst& kc, int d, long long v,
+// fm = the domain's fixed-species mask (RealDesc::fixed_mask).
+__device__ __forceinline__ void rx_store(unsigned fm, const float* const* un, const RxConst& kc, long long v,
                                          bool face, float nc, const float* nb, float dc, const float* db) {
-  const unsigned fm = D.fixed_mask[d];
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
     const int s = q + 1;
@@ -446,6 +449,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   float* stage = dsm + sizeof(MlpTC) / sizeof(float) + (threadIdx.x >> 5) * MLP_TC_STAGE;
   __shared__ RxConst sk[ND];
   __shared__ float s_thr[ND][MLP_SLOTS];
+  __shared__ unsigned s_fm[ND];
   __shared__ const float* s_uo[NS];
   __shared__ const float* s_un[NS];
   __shared__ long long s_pend[MLP_DEPLOY_T / 32][64];   // per warp: queued voxels (up to two tiles)
@@ -465,6 +469,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     const RxConst kc = rx_const(D, threadIdx.x < D.nd ? threadIdx.x : 0);
     sk[threadIdx.x] = kc;
     for (int q = 0; q < MLP_SLOTS; q++) s_thr[threadIdx.x][q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
+    s_fm[threadIdx.x] = D.fixed_mask[threadIdx.x < D.nd ? threadIdx.x : 0];
   }
   if (threadIdx.x < NS) {
     const int t = threadIdx.x;
@@ -476,6 +481,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   const unsigned char* __restrict__ dom = D.dom;
   const int plane = D.plane;
   const unsigned elig_mask = D.mlp_domains;
+  const bool dirichlet = D.dirichlet != 0;
   unsigned n_vox = 0, n_net = 0, n_fall = 0;
   const long long v0 = (long long)blockIdx.x * span + threadIdx.x;
   // position within the plane and plane index of the voxel being fetched, advanced by
@@ -511,7 +517,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
         n_fall++;
         rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
       }
-      rx_store(D, s_un, kc, Y.d, v, D.dirichlet && rx_on_face(D, xq, pq), Y.nc, Y.nb, dc, db);
+      rx_store(s_fm[Y.d], s_un, kc, v, dirichlet && rx_on_face(D, xq, pq), Y.nc, Y.nb, dc, db);
     }
     __syncwarp();
   };
@@ -528,9 +534,10 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     const int d = Y.d;
     const RxConst& kc = sk[d];
     bool elig = false, skip = false;
+    float g[MLP_SLOTS];
     if (Y.mine) {
       elig = (elig_mask >> d) & 1u;
-      skip = elig && rx_near_equilibrium(kc, s_thr[d], Y.c, Y.b);
+      skip = elig && rx_near_equilibrium(kc, s_thr[d], Y.c, Y.b, g);
     }
     const bool net = Y.mine && elig && !skip;
     if (Y.mine && !net) {
@@ -540,7 +547,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
         // near equilibrium: the explicit increment
         float sdb = 0.f;
         for (int q = 0; q < MLP_SLOTS; q++) {
-          db[q] = kc.tot[q] > 0.f ? dtr * rx_g<float>(kc, q, Y.c, Y.b[q]) : 0.f;
+          db[q] = kc.tot[q] > 0.f ? dtr * g[q] : 0.f;
           sdb += db[q];
         }
         dc = -sdb;
@@ -549,7 +556,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
         n_fall++;
         rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
       }
-      rx_store(D, s_un, kc, d, v, D.dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db);
+      rx_store(s_fm[d], s_un, kc, v, dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db);
     }
     const unsigned nm = __ballot_sync(0xffffffffu, net);
     if (net) pend[npend + __popc(nm & ((1u << lane) - 1u))] = v;
