@@ -598,6 +598,12 @@ int main(int argc, char** argv) {
   }
   check(NULL, csp_create(m, &o, 1, &R.h), "csp_create");
   check(R.h, csp_get_info(R.h, 0, &R.info), "csp_get_info");
+  {
+    /* the voxel kernel's tile shape for this grid, timed once (the fields are the same
+       for every shape); without a fitting shape the default stays */
+    csp_tune_report tr;
+    (void)csp_autotune(R.h, 3, &tr);
+  }
   const int* n = R.info.n;
   R.h_sim = R.info.h;
   /* sheets (species.c:790-830): default z = (N_z/2 - subdivisions/2) h */
