@@ -12,8 +12,9 @@ data path); rank 0 prints one JSON line.
 
 value: voxel-steps/s over the K timed steps, device-timed with CUDA events on the
 handle's stream (max over ranks).  e2e: the same metric through the C ABI with host
-buffers: initial fields uploaded from host memory, K calls of csp_advance(1) each
-returning the per-realisation stop flags, final fields downloaded.  The state (5.1 GB
+buffers: initial fields uploaded from host memory (csp_upload_states), K calls of
+csp_advance(1) each returning the per-realisation stop flags, final fields downloaded
+(csp_download_states).  The state (5.1 GB
 per GPU) is larger than L2, so no flush is needed between steps.
 
 cpu_baseline and --impl reference time the reference program itself (oracle/_ref: the
@@ -385,14 +386,12 @@ def main():
     fp = flags.ctypes.data_as(C.POINTER(C.c_int32))
     D.barrier()
     t0 = time.perf_counter()
-    for r in range(nreal):
-        sim2.set_state(host[r], r)
+    sim2.set_states(host)
     for _ in range(K):
         rc = lib.csp_advance(sim2.h, 1, fp)
         if rc:
             raise RuntimeError(f"csp_advance failed: {rc}")
-    for r in range(nreal):
-        sim2.state_into(outb[r], r)
+    sim2.states_into(outb)
     out = outb
     e2e_s = time.perf_counter() - t0
     e2e_s = D.reduce(e2e_s, "max")

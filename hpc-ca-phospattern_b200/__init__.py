@@ -194,6 +194,24 @@ class Simulation:
             raise ValueError(f"state shape {u.shape} != {self.shape(r)}")
         self._check(self.lib.csp_upload_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
 
+    def _state_ptrs(self, arrays):
+        if len(arrays) != self.n:
+            raise ValueError(f"{len(arrays)} states for {self.n} realisations")
+        for r, u in enumerate(arrays):
+            if u.dtype != np.float64 or not u.flags.c_contiguous or u.shape != self.shape(r):
+                raise ValueError(f"state {r} must be a C-contiguous float64 array of shape {self.shape(r)}")
+        ptrs = (C.POINTER(C.c_double) * self.n)(*[u.ctypes.data_as(C.POINTER(C.c_double)) for u in arrays])
+        return ptrs
+
+    def set_states(self, arrays):
+        """Upload every realisation's state in one call (csp_upload_states)."""
+        self._check(self.lib.csp_upload_states(self.h, self._state_ptrs(arrays)))
+
+    def states_into(self, arrays):
+        """Download every realisation's state into caller-owned arrays (csp_download_states)."""
+        self._check(self.lib.csp_download_states(self.h, self._state_ptrs(arrays)))
+        return arrays
+
     def advance(self, nsteps):
         flags = np.zeros(self.n, dtype=np.int32)
         self._check(self.lib.csp_advance(self.h, int(nsteps), flags.ctypes.data_as(C.POINTER(C.c_int32))))

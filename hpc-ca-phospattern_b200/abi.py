@@ -244,6 +244,8 @@ def declare(lib):
         "csp_get_info": (C.c_int, [h, C.c_int32, P(csp_info)]),
         "csp_upload_state": (C.c_int, [h, C.c_int32, P(C.c_double)]),
         "csp_download_state": (C.c_int, [h, C.c_int32, P(C.c_double)]),
+        "csp_upload_states": (C.c_int, [h, P(P(C.c_double))]),
+        "csp_download_states": (C.c_int, [h, P(P(C.c_double))]),
         "csp_advance": (C.c_int, [h, C.c_int64, P(C.c_int32)]),
         "csp_advance_async": (C.c_int, [h, C.c_int64]),
         "csp_advance_wait": (C.c_int, [h, P(C.c_int32)]),

@@ -1157,6 +1157,73 @@ extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
   return CSP_OK;
 }
 
+// Every realisation's state in one call: one read of the progress blocks, the copies and
+// conversions of all realisations queued back to back on the handle stream (the staging
+// buffer is reused in stream order), one wait at the end.
+static int state_maps(csp_handle* h, std::vector<StateMap>& maps) {
+  std::vector<RealCtl> ctl(h->n);
+  CUDA_TRY(h, cudaMemcpyAsync(ctl.data(), h->d_ctl, h->n * sizeof(RealCtl), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  maps.assign(h->n, StateMap{});
+  size_t need = 0;
+  for (int r = 0; r < h->n; r++) {
+    StateMap& m = maps[r];
+    const HostReal& hr = h->real[r];
+    const RealDesc& D = hr.desc;
+    const unsigned cur = ctl[r].cur_mask[ctl[r].step & 1];
+    m.ns = D.ns;
+    for (int s = 0; s < D.ns; s++) m.f[s] = D.u[(cur >> s) & 1u][s];
+    for (int a = 0; a < 3; a++) m.n[a] = hr.nphys[a];
+    const long long dstr[3] = {(long long)D.P, (long long)D.nz, 1};
+    for (int i = 0; i < 3; i++) m.stride[hr.perm[i]] = dstr[i];
+    m.nvox = (long long)m.n[0] * m.n[1] * m.n[2];
+    need = std::max(need, (size_t)m.nvox * m.ns);
+  }
+  if (need > h->stage_elems) {
+    cudaFree(h->d_stage);
+    h->d_stage = nullptr;
+    h->stage_elems = 0;
+    if (cudaMalloc(&h->d_stage, need * sizeof(double)) != cudaSuccess)
+      return fail(h, CSP_ENOMEM, "state staging buffer of %.1f MB", need * 8.0 / 1e6);
+    h->stage_elems = need;
+  }
+  return CSP_OK;
+}
+
+extern "C" int csp_upload_states(csp_handle* h, const double* const* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  for (int r = 0; r < h->n; r++)
+    if (!u[r]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
+  std::vector<StateMap> maps;
+  int rc = state_maps(h, maps);
+  if (rc) return rc;
+  for (int r = 0; r < h->n; r++) {
+    const long long n = maps[r].nvox * maps[r].ns;
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, u[r], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    k_state_in<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, maps[r]);
+    CUDA_TRY(h, cudaGetLastError());
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+extern "C" int csp_download_states(csp_handle* h, double* const* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  for (int r = 0; r < h->n; r++)
+    if (!u[r]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
+  std::vector<StateMap> maps;
+  int rc = state_maps(h, maps);
+  if (rc) return rc;
+  for (int r = 0; r < h->n; r++) {
+    const long long n = maps[r].nvox * maps[r].ns;
+    k_state_out<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, maps[r]);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(u[r], h->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
 // One species of the physical-order FP64 state (the species slot of k_state_out's output).
 __global__ void k_state_out_species(double* __restrict__ dst, StateMap m, int s) {
   const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;

@@ -191,6 +191,11 @@ int csp_get_info(const csp_handle* h, int32_t r, csp_info* info);
  * species.h:52.) */
 int csp_upload_state(csp_handle* h, int32_t r, const double* u);
 int csp_download_state(csp_handle* h, int32_t r, double* u);
+/* The same for every realisation in one call: u[r] is realisation r's state (n pointers).
+ * The copies run back to back with one wait at the end (use page-locked host memory for
+ * full link speed). */
+int csp_upload_states(csp_handle* h, const double* const* u);
+int csp_download_states(csp_handle* h, double* const* u);
 
 /* Advance every still-running realisation by up to nsteps steps: diffusion, channel
  * gating, boundary fluxes, reactions, apply and fixed values, in the order of the

@@ -353,3 +353,20 @@ def test_async_advance_and_snapshot(pkg, synth):
         b.snapshot_wait()
     a.advance(1)
     np.testing.assert_array_equal(a.state(), b.state())
+
+
+def test_batched_state_transfers(pkg, synth):
+    """csp_upload_states / csp_download_states equal the per-realisation calls."""
+    specs = [synth.tiny((12, 12, 16)), synth.tiny((10, 14, 12))]
+    opts = [dict(h=6.0, tstop=5.0, seed=5, open_states={"ryr": [0]})] * 2
+    a = pkg.Simulation(specs, opts)
+    a.advance(20)
+    u = [a.state(r) for r in range(2)]
+    rng = np.random.default_rng(3)
+    new = [np.ascontiguousarray(x * (1.0 + 0.01 * rng.random(x.shape))) for x in u]
+    a.set_states(new)
+    got = [np.empty_like(x) for x in u]
+    a.states_into(got)
+    for r in range(2):
+        np.testing.assert_array_equal(got[r], a.state(r))
+        np.testing.assert_array_equal(got[r], new[r].astype(np.float32).astype(np.float64))
