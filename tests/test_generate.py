@@ -97,3 +97,21 @@ def test_h5lite_incremental_flushes(tmp_path):
         np.testing.assert_array_equal(f.dset("/data_0000001/Ca_all_data"), b)
         assert float(np.ravel(f.attr("/data_0000000", "time"))[0]) == 0.5
         assert sorted(n for _, n in f.list("/")) == ["data_0000000", "data_0000001"]
+
+
+def test_h5lite_incremental_then_append(tmp_path):
+    """A file written by incremental flushes, reopened for appending (whole rewrite),
+    keeps every dataset and attribute."""
+    p = str(tmp_path / "app.h5")
+    a = np.arange(1000, dtype=np.float64)
+    with h5m.H5(p, "w") as f:
+        f.put_group("/g")
+        f.put_dset("/g/a", a)
+        f.flush()
+        f.put_attr("/g", "n", np.array([7], dtype=np.int32))
+    with h5m.H5(p, "a") as f:
+        f.put_dset("/g/b", 2 * a)
+    with h5m.H5(p) as f:
+        np.testing.assert_array_equal(f.dset("/g/a"), a)
+        np.testing.assert_array_equal(f.dset("/g/b"), 2 * a)
+        assert int(np.ravel(f.attr("/g", "n"))[0]) == 7
