@@ -12,10 +12,12 @@ data path); rank 0 prints one JSON line.
 
 value: voxel-steps/s over the K timed steps, device-timed with CUDA events on the
 handle's stream (max over ranks).  e2e: the same metric through the C ABI with host
-buffers: initial fields uploaded from host memory (csp_upload_states), K calls of
-csp_advance(1) each returning the per-realisation stop flags, final fields downloaded
-(csp_download_states).  The state (5.1 GB
-per GPU) is larger than L2, so no flush is needed between steps.
+buffers, one csp_run_states call: every realisation's FP32 state uploaded from
+page-locked host memory, K steps with every realisation's stop flag after every step read
+back, the final fields downloaded, pipelined by realisation groups (the copies of one
+group overlap the steps of another).  The state (5.1 GB per GPU) is larger than L2, so no
+flush is needed between steps.  parity: the FP32 error against the reference program's
+FP64 run on config 2 (tests/golden/configs/config2_short.npz).
 
 cpu_baseline and --impl reference time the reference program itself (oracle/_ref: the
 reference's fvm_mpi sources built with a single-rank MPI stub and the project's HDF5
@@ -23,7 +25,6 @@ subset, FP64, OpenMP on every physical core) on one realisation of the workload,
 own main-loop timer; the FP64 port in oracle/ stands in only when oracle/_ref is absent.
 """
 import argparse
-import ctypes as C
 import importlib
 import json
 import os
@@ -49,51 +50,6 @@ def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", str(rank)))
     return rank, world, local
-
-
-class Dist:
-    """torch.distributed plumbing: barrier and max/sum over ranks (NCCL on GPUs)."""
-
-    def __init__(self, world, local):
-        self.world = world
-        self.dist = None
-        if world > 1:
-            import datetime
-            import torch
-            import torch.distributed as dist
-            backend = "nccl" if torch.cuda.is_available() else "gloo"
-            if backend == "nccl":
-                torch.cuda.set_device(local)
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-            self.dist = dist
-            self.torch = torch
-            self.dev = torch.device("cuda", local) if backend == "nccl" else torch.device("cpu")
-
-    def barrier(self):
-        if self.dist:
-            self.dist.barrier()
-
-    def reduce(self, x, op):
-        if not self.dist:
-            return x
-        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.dev)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX if op == "max" else self.dist.ReduceOp.SUM)
-        return float(t.item())
-
-    def gather_summaries(self, sim, nreal):
-        """Steps taken and stop flag of every realisation of every rank, gathered to rank 0
-        (all_gather over NCCL with N GPUs); returns the number of realisations gathered."""
-        rows = np.array([[sim.info(r).step, sim.info(r).stopped] for r in range(nreal)], dtype=np.float64)
-        if not self.dist:
-            return rows.shape[0]
-        t = self.torch.tensor(rows, device=self.dev)
-        out = [self.torch.empty_like(t) for _ in range(self.world)]
-        self.dist.all_gather(out, t)
-        return int(sum(o.shape[0] for o in out))
-
-    def close(self):
-        if self.dist:
-            self.dist.destroy_process_group()
 
 
 class Clocks:
@@ -141,11 +97,18 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def shard_workload(rank, world, nreal):
-    """The realisations of one rank: its own seed range (weak scaling, nothing shared)."""
+def ensemble_workload(ranks, nreal_per_gpu, simulation=None):
+    """The whole job: nreal_per_gpu x world realisations of config 3 (seed 3), assigned to
+    the ranks by estimated cost (voxels x steps: equal here, so round-robin) with
+    hpc-ca-phospattern_b200.ensemble; every rank builds and advances only its own share
+    (weak scaling, nothing exchanged on the data path)."""
     synth = importlib.import_module("hpc-ca-phospattern_b200.synth")
-    specs, opts = synth.config3(n=nreal, seed=3 + 1000 * rank)
-    return specs, opts
+    ens = importlib.import_module("hpc-ca-phospattern_b200.ensemble")
+    n = nreal_per_gpu * ranks.world
+    draws = synth.config3_draws(n=n, seed=3)
+    costs = [ens.realisation_cost(d["shape"], d["h"], d["opts"], 220000.0) for d in draws]
+    return ens.Ensemble(n, lambda idx: synth.config3(n=n, seed=3, only=idx), costs=costs, ranks=ranks,
+                        simulation=simulation)
 
 
 def pinned_copy(a):
@@ -153,7 +116,8 @@ def pinned_copy(a):
     that the state copies of the e2e leg run at full PCIe speed; a plain copy without torch."""
     try:
         import torch
-        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=torch.cuda.is_available())
+        tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.float32): torch.float32}[a.dtype]
+        t = torch.empty(a.shape, dtype=tdt, pin_memory=torch.cuda.is_available())
         out = t.numpy()
         out[...] = a
         _PINNED.append(t)          # keeps the pinned block alive with the array
@@ -308,6 +272,36 @@ def surrogate_run(pkg, specs, opts, W, K):
             "fallback_fraction": fb / vx if vx else None}
 
 
+def parity_leg(pkg):
+    """FP32 accuracy on one 200x200x100 grid (config 2: 10x10 RyR lattice with vacancies,
+    20 % pRyR), 0.5 ms = 19,296 steps with channels forced, against the reference
+    program's FP64 run stored in tests/golden/configs/config2_short.npz: max over the stored
+    voxels (a lattice of every 5th voxel and the cleft planes around the cluster) of
+    |diff| / max |ref| per species."""
+    golden = os.path.join(ROOT, "tests", "golden")
+    path = os.path.join(golden, "configs", "config2_short.npz")
+    if not os.path.exists(path):
+        return None
+    sys.path.insert(0, golden)
+    mcp = importlib.import_module("make_config_parity")
+    z = np.load(path)
+    spec, opts = mcp.build("config2_short")
+    sim = pkg.Simulation(spec, opts)
+    steps = int(z["time_index"][-1])
+    sim.advance(steps)
+    lat, win = mcp.samples(sim.state(), spec)
+    sim.close()
+    err = []
+    for s in range(lat.shape[0]):
+        e = 0.0
+        for got, ref in ((lat[s], z["lattice"][s].astype(np.float64)), (win[s], z["window"][s].astype(np.float64))):
+            e = max(e, float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))))
+        err.append(e)
+    return {"workload": "config 2: one 200x200x100 grid, 0.5 ms, channels forced (-O/-C)", "steps": steps,
+            "against": "reference program FP64 (oracle/_ref), stored fixture", "max_rel_err": max(err),
+            "per_species": dict(zip(spec["species"], err)), "bar": 1e-4}
+
+
 def config_leg(pkg, specs, opts, W, K, workload):
     """One more configuration on the same kernels: autotuned tile, W untimed steps, K steps
     timed on the device (graph replay); voxel-steps summed over the realisations."""
@@ -343,11 +337,12 @@ def main():
 
     pkg = importlib.import_module("hpc-ca-phospattern_b200")
     synth = importlib.import_module("hpc-ca-phospattern_b200.synth")
-    D = Dist(world, local)
+    ensemble = importlib.import_module("hpc-ca-phospattern_b200.ensemble")
+    D = ensemble.Ranks(world, local)
     pkg.set_device(local)
-    nreal = args.realisations
-    specs, opts = shard_workload(rank, world, nreal)
-    sim = pkg.Simulation(specs, opts)
+    ens = ensemble_workload(D, args.realisations)
+    sim, specs, opts = ens.sim, ens.specs, ens.opts
+    nreal = len(specs)
     nvox = sum(int(np.prod(s["voxels"].shape)) for s in specs)
     W, K = max(3, args.warmup), args.steps
 
@@ -366,8 +361,9 @@ def main():
     ms_max = D.reduce(ms, "max")
     vox_total = D.reduce(nvox, "sum")
     value = vox_total * K / (ms_max / 1e3)
-    # per-realisation summaries (steps taken, stopped) of every rank to rank 0: one gather
-    gathered = D.gather_summaries(sim, nreal)
+    # per-realisation statistics (steps, stop flag, open channels, per-domain min / max /
+    # total of every species) of every rank on every rank: one all_gather
+    gathered = int(len(ens.statistics()["index"]))
 
     # ---- roofline of the dominant kernel: per-launch CUDA events ----
     nprof = min(K, 100)
@@ -377,33 +373,28 @@ def main():
     peak, peak_kind = measured_peaks()
     traffic = profiled_traffic(nvox)
 
-    # ---- e2e through the C ABI with host buffers ----
+    # ---- e2e through the C ABI with host buffers: csp_run_states (upload every
+    # realisation's FP32 state from page-locked host memory, K steps with every
+    # realisation's stop flag read back after every step, download), pipelined by
+    # realisation groups so the copies overlap the steps ----
     sim2 = pkg.Simulation(specs, opts)
-    host = [pinned_copy(sim2.state(r)) for r in range(nreal)]
-    outb = [pinned_copy(h) for h in host]
-    lib = sim2.lib
-    flags = np.zeros(nreal, dtype=np.int32)
-    fp = flags.ctypes.data_as(C.POINTER(C.c_int32))
+    host = [pinned_copy(sim2.state(r).astype(np.float32)) for r in range(nreal)]
+    outb = [pinned_copy(np.zeros_like(h)) for h in host]
+    sim2.run_states(host, W, outb)                  # warm-up: the same call, untimed
     D.barrier()
     t0 = time.perf_counter()
-    sim2.set_states(host)
-    for _ in range(K):
-        rc = lib.csp_advance(sim2.h, 1, fp)
-        if rc:
-            raise RuntimeError(f"csp_advance failed: {rc}")
-    sim2.states_into(outb)
-    out = outb
+    flags, step_flags = sim2.run_states(host, K, outb, step_flags=True)
     e2e_s = time.perf_counter() - t0
     e2e_s = D.reduce(e2e_s, "max")
     e2e = vox_total * K / e2e_s
     ns = len(specs[0]["species"])
-    field_bytes = 8 * ns * nvox                     # FP64 host state copied per direction (rounded on the device)
+    field_bytes = 4 * ns * nvox                     # FP32 host state copied per direction
     h2d = field_bytes / K
-    d2h = (field_bytes + K * nreal * 48) / K        # final fields + per-step progress / stop flags
-    assert all(np.isfinite(o).all() for o in out)
+    d2h = (field_bytes + K * nreal * 4) / K         # final fields + every step's stop flags
+    assert all(np.isfinite(o).all() for o in outb) and step_flags.shape == (K, nreal)
 
     # ---- plain path: one realisation of the same workload on the same kernels ----
-    plain_single, sur, configs = None, None, None
+    plain_single, sur, configs, parity = None, None, None, None
     if args.extras:
         single = pkg.Simulation(specs[:1], opts[:1])
         single.advance(W)
@@ -415,6 +406,7 @@ def main():
         # ---- configs 2 and 4 on the same kernels ----
         s2, o2 = synth.config2()
         s4, o4 = synth.config4()
+        parity = parity_leg(pkg)
         configs = {
             "config2": config_leg(pkg, [s2], [o2], W, K,
                                   "one 200x200x100 grid at 6 nm, 10x10 RyR lattice with vacancies, 20 % pRyR"),
@@ -442,7 +434,7 @@ def main():
                              f"({dt:.1f} s), FP64 port of the reference"}
 
     # per step: voxel kernel, density-row flux kernel, channel-row gating/flux kernel, step
-    # epilogue (the workload has both kinds of flux rows)
+    # epilogue (the workload has both kinds of flux rows), in the device-timed region
     kernels = 4 * K
     if rank == 0:
         line = {
@@ -462,7 +454,9 @@ def main():
                          "bytes_per_voxel": BYTES_PER_VOXEL_STEP, "peak_source": peak_kind,
                          "boundary_kernel_ms": bms / nprof},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": K, "call": "csp_run_states (FP32 host state, pipelined by realisation groups)"},
+            "parity": parity,
             "gpu_launches": kernels,
             "plain_single_realisation": None if plain_single is None else {
                 "value": plain_single, "unit": "voxel-steps/s",
@@ -473,7 +467,7 @@ def main():
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
+    ens.close()
     sim2.close()
     D.close()
     return 0

@@ -194,14 +194,42 @@ class Simulation:
             raise ValueError(f"state shape {u.shape} != {self.shape(r)}")
         self._check(self.lib.csp_upload_state(self.h, r, u.ctypes.data_as(C.POINTER(C.c_double))))
 
-    def _state_ptrs(self, arrays):
+    def _state_ptrs(self, arrays, dtype=np.float64):
         if len(arrays) != self.n:
             raise ValueError(f"{len(arrays)} states for {self.n} realisations")
         for r, u in enumerate(arrays):
-            if u.dtype != np.float64 or not u.flags.c_contiguous or u.shape != self.shape(r):
-                raise ValueError(f"state {r} must be a C-contiguous float64 array of shape {self.shape(r)}")
-        ptrs = (C.POINTER(C.c_double) * self.n)(*[u.ctypes.data_as(C.POINTER(C.c_double)) for u in arrays])
+            if u.dtype != dtype or not u.flags.c_contiguous or u.shape != self.shape(r):
+                raise ValueError(f"state {r} must be a C-contiguous {np.dtype(dtype).name} array of shape "
+                                 f"{self.shape(r)}")
+        ct = C.c_double if dtype == np.float64 else C.c_float
+        ptrs = (C.POINTER(ct) * self.n)(*[u.ctypes.data_as(C.POINTER(ct)) for u in arrays])
         return ptrs
+
+    def set_states_f32(self, arrays):
+        """Upload every realisation's state from FP32 host arrays (csp_upload_states_f32)."""
+        self._check(self.lib.csp_upload_states_f32(self.h, self._state_ptrs(arrays, np.float32)))
+
+    def states_into_f32(self, arrays):
+        """Download every realisation's state into FP32 host arrays (csp_download_states_f32)."""
+        self._check(self.lib.csp_download_states_f32(self.h, self._state_ptrs(arrays, np.float32)))
+        return arrays
+
+    def run_states(self, u_in, nsteps, u_out, step_flags=False):
+        """Upload u_in, advance nsteps, download into u_out, pipelined by realisation groups
+        (csp_run_states); FP32 or FP64 host arrays.  Returns the stop flags, and with
+        step_flags=True also the [nsteps][n] stop flags after every step."""
+        dtype = u_in[0].dtype
+        if dtype not in (np.float32, np.float64):
+            raise ValueError("host states must be float32 or float64")
+        pin = C.cast(self._state_ptrs(u_in, dtype), C.POINTER(C.c_void_p))
+        pout = C.cast(self._state_ptrs(u_out, dtype), C.POINTER(C.c_void_p))
+        flags = np.zeros(self.n, dtype=np.int32)
+        sf = np.zeros((int(nsteps), self.n), dtype=np.int32) if step_flags else None
+        P = C.POINTER(C.c_int32)
+        self._check(self.lib.csp_run_states(self.h, abi.HOST_F32 if dtype == np.float32 else abi.HOST_F64, pin,
+                                            int(nsteps), pout, flags.ctypes.data_as(P),
+                                            sf.ctypes.data_as(P) if sf is not None else None))
+        return (flags, sf) if step_flags else flags
 
     def set_states(self, arrays):
         """Upload every realisation's state in one call (csp_upload_states)."""

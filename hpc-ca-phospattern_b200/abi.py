@@ -13,6 +13,7 @@ MAX_BUFFERS = 8
 MAX_BOUNDARIES = 8
 MAX_FIXED = 8
 NAME_LEN = 20
+HOST_F64, HOST_F32 = 0, 1    # csp_run_states host_dtype (CSP_HOST_F64, CSP_HOST_F32)
 
 OK, EINVAL, ENOMEM, ECUDA, ERANGE, EDEVICE, ENOTSUP = 0, -1, -2, -3, -4, -5, -6
 DENSITY, DISCRETE = 0, 1
@@ -88,7 +89,8 @@ class csp_options(C.Structure):
                 ("force_dirichlet", C.c_int32), ("seed_given", C.c_int32),
                 ("seed", C.c_uint64),
                 ("num_open_lists", C.c_int32), ("open", csp_open_list * MAX_BOUNDARIES),
-                ("num_t_close", C.c_int32), ("t_close", csp_t_close * MAX_BOUNDARIES)]
+                ("num_t_close", C.c_int32), ("t_close", csp_t_close * MAX_BOUNDARIES),
+                ("stream_offset", C.c_int64)]
 
 
 class csp_info(C.Structure):
@@ -207,7 +209,7 @@ def make_model(spec):
 
 def make_options(h=6.0, dt=-1.0, tstop=10.0, dt_save=0.5, dt_update_react=-1.0,
                  dt_update_stoch=-1.0, tabort=0.0, force_dirichlet=False, seed=None,
-                 open_states=None, t_close=None):
+                 open_states=None, t_close=None, stream_offset=0):
     """csp_options with the reference defaults (options.c:502-542) unless overridden.
 
     open_states: {"ryr": [0, 3], ...} as -O; t_close: {"ryr": 2.0} as -C.
@@ -230,6 +232,7 @@ def make_options(h=6.0, dt=-1.0, tstop=10.0, dt_save=0.5, dt_update_react=-1.0,
         o.t_close[i].name = _name(name)
         o.t_close[i].time = float(t)
     o.num_t_close = len(t_close or {})
+    o.stream_offset = int(stream_offset)
     return o, keep
 
 
@@ -246,6 +249,10 @@ def declare(lib):
         "csp_download_state": (C.c_int, [h, C.c_int32, P(C.c_double)]),
         "csp_upload_states": (C.c_int, [h, P(P(C.c_double))]),
         "csp_download_states": (C.c_int, [h, P(P(C.c_double))]),
+        "csp_upload_states_f32": (C.c_int, [h, P(P(C.c_float))]),
+        "csp_download_states_f32": (C.c_int, [h, P(P(C.c_float))]),
+        "csp_run_states": (C.c_int, [h, C.c_int32, P(C.c_void_p), C.c_int64, P(C.c_void_p), P(C.c_int32),
+                                     P(C.c_int32)]),
         "csp_advance": (C.c_int, [h, C.c_int64, P(C.c_int32)]),
         "csp_advance_async": (C.c_int, [h, C.c_int64]),
         "csp_advance_wait": (C.c_int, [h, P(C.c_int32)]),
@@ -260,6 +267,9 @@ def declare(lib):
         "csp_get_stream": (C.c_int, [h, P(C.c_void_p)]),
         "csp_last_advance_ms": (C.c_int, [h, P(C.c_float)]),
         "csp_set_kernel": (C.c_int, [h, C.c_int32]),
+        "csp_test_wait_timeout": (C.c_int, [h, C.c_int32]),
+        "csp_set_phase_timing": (C.c_int, [h, C.c_int32]),
+        "csp_get_phase_times": (C.c_int, [h, P(C.c_double), P(C.c_int64)]),
         "csp_profile_advance": (C.c_int, [h, C.c_int64, P(C.c_float), P(C.c_float)]),
         "csp_reduce_field_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_double,
                                                C.c_void_p, C.c_void_p]),

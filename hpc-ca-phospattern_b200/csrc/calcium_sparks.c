@@ -28,8 +28,14 @@
 #include "csparks.h"
 
 /* ------------------------------------------------------------ timings ---- */
-/* the reference's timing table (utils.c:10-75); buckets this driver does not time
- * (the library's kernels run inside MAINLOOP) stay at zero */
+/* the reference's timing table (utils.c:10-75).  The step's buckets come from the
+ * library's per-phase device times (csp_get_phase_times, estimated from a timed sample of
+ * every advance call): "Diffusion stencil" = the voxel kernel, which also does the buffer
+ * reactions and fixed values ("Reaction stencil" holds only the learned surrogate's
+ * kernel, "Fixed Domains" / "Apply du" stay 0: no separate pass), "Boundary fluxes" =
+ * density-boundary rows + step epilogue, "Stochastic evaluation" = RyR/pRyR gating with
+ * the channel fluxes; "Diffusion Total" = "Diffusion stencil".  Ghost exchange and the
+ * border stencils have no counterpart on one GPU and stay 0. */
 enum {
   T_SETUP = 0, T_INIT, T_GEOM, T_SPECIES, T_GHOST, T_DIFF, T_BORDERS, T_BOUNDARIES, T_STOCH, T_REACT, T_FIXED,
   T_APPLYDU, T_CONV, T_WRITE, T_BORDERSX, T_BORDERSY, T_BORDERSZ, T_MAINLOOP, T_DIFFTOT, T_SIM, T_NUM
@@ -671,6 +677,7 @@ int main(int argc, char** argv) {
   finish_output(&R);
   unsigned output_ind = 0;
 
+  if (a.verbose) check(R.h, csp_set_phase_timing(R.h, 1), "csp_set_phase_timing");
   push_time(T_MAINLOOP);
   const long long total = R.info.total_steps;
   long long k = 0;       /* steps taken */
@@ -708,6 +715,18 @@ int main(int argc, char** argv) {
   pop_time(T_MAINLOOP);
 
   if (cs_output_close(R.out)) die("*** ERROR: output: %s\n", cs_output_error());
+  if (a.verbose) {
+    double ph[CSP_NUM_PHASES];
+    int64_t nst = 0;
+    check(R.h, csp_get_phase_times(R.h, ph, &nst), "csp_get_phase_times");
+    const struct { int bucket; double ms; } map[] = {
+        {T_DIFF, ph[CSP_PHASE_VOXELS]}, {T_BOUNDARIES, ph[CSP_PHASE_DENSITY] + ph[CSP_PHASE_EPILOGUE]},
+        {T_STOCH, ph[CSP_PHASE_CHANNELS]}, {T_REACT, ph[CSP_PHASE_SURROGATE]}, {T_DIFFTOT, ph[CSP_PHASE_VOXELS]}};
+    for (size_t i = 0; i < sizeof map / sizeof map[0]; i++) {
+      tval[map[i].bucket] = map[i].ms / 1e3;
+      tcalls[map[i].bucket] = (unsigned)nst;
+    }
+  }
   csp_destroy(R.h);
   free(R.snapshot);
   cs_model_mem_free(&R.mem);

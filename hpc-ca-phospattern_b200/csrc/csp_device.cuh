@@ -40,7 +40,9 @@ struct RealDesc {
   // the reaction time step dt_r
   float kon_dt[NB * ND], koff_dt[NB * ND], tot[NB * ND];
   float cdiag[ND][NS];               // coef of species s between two voxels of domain d (0: not diffusive)
-  float4 rk[ND][NS];                 // fast reactions: {kon_dt, koff_dt, tot, 1} of the buffer bound to s in d, or 0
+  // fast reactions: {-kon_dt, -koff_dt, a_dt, j0_dt} of the buffer bound to s in d (see
+  // buffer_dj), present where rmask[d] has bit s
+  float4 rk[ND][NS];
   unsigned char bsp0[NB * ND], bsp1[NB * ND];
   unsigned char fixed_mask[ND];      // bit s: species s is fixed in domain d
   signed char dsi_of[NS];            // diffusive index of species s, or -1
@@ -56,7 +58,22 @@ struct RealDesc {
   int fslot_species[4];
   int fslot_kind[4];
   double fslot_p[4][10];
-  float init[ND][NS];
+  float init[ND][NS];                // initial values (Species_init_values, species.c:887-935)
+  // Every field holds a value as its deviation from a base: u = base[d][s] + field, with d
+  // the voxel's domain.  The base of a species that diffuses is one value for each set of
+  // domains that species diffuses between (the initial value of the set's first domain),
+  // so neighbouring deviations differ exactly as the values do and the stencil is the
+  // same on both; other species take their domain's initial value.  In FP32 a value near
+  // 1300 uM (SR Ca) or 20 mM (bound CSQN) keeps increments down to 1e-4 uM only when
+  // stored as a deviation: the per-step SERCA uptake and buffer binding would otherwise
+  // round away.  dinit = init - base (what fixed and Dirichlet values write).
+  double base[ND][NS];
+  float fbase[ND][NS];
+  float dinit[ND][NS];
+  // buffer reactions about the base: for buffer t = bi*nd + d with bound species s0 and
+  // ligand s1, a_dt = dt_r k_on (tot - base_s0), j0_dt = dt_r J(base_s0, base_s1)
+  float a_dt[NB * ND], j0_dt[NB * ND];
+  unsigned char rmask[ND];           // bit s: a buffer binds species s in domain d (fast reactions)
   float* u[2][NS];                   // the two buffers of every species
   const unsigned char* dom;          // [nx][P]
   // Chunk class table [nx][ncls]: for plane x and chunk c (positions c*CLASS_L ...
@@ -67,6 +84,7 @@ struct RealDesc {
   long long total_steps;
   double dt, h, tabort;
   unsigned long long seed;           // Philox key of the realisation's channel draws
+  unsigned stream;                   // Philox stream: batch index + csp_options.stream_offset
   int has_channels;
 };
 
@@ -100,7 +118,7 @@ struct alignas(16) DensityRow {
   int more_begin;                    // further pairs: entries[more_begin .. more_begin + nmore)
   double scale;                      // first pair, kind SERCA: the flux scale (FluxParams::p[9])
   unsigned meta0;                    // first pair's parameter block (bits 0-15), species (16-23), dsi (24-31)
-  unsigned meta1;                    // DROW_* flags (bits 0-7), nmore (8-15)
+  unsigned meta1;                    // DROW_* flags (bits 0-7), nmore (8-15), domain ids of v (16-18), vo (19-21)
 };
 static_assert(sizeof(DensityRow) == 32, "density row");
 
@@ -116,7 +134,7 @@ struct FluxPair {
   int param;              // index into the parameter blocks
   long long v0, v1;       // padded linear indices x*P + p of from / to voxels
   int local_channel;      // channel index within its boundary (RNG counter)
-  int pad;
+  int doms;               // domain ids of v0 (bits 0-2) and v1 (bits 3-5): the fields' bases
 };
 
 // One voxel receiving flux.  Its first pair is stored inline (most voxels touch one
@@ -130,7 +148,9 @@ struct FluxRow {
   int local_channel;      // first pair: channel index within its boundary (RNG counter)
   float sign;             // first pair: +1 receiving side, -1 giving side
   int more_begin, more_end;
-  unsigned char species, dsi, kind, owner, boundary, apply, pad0, pad1;
+  unsigned char species, dsi, kind, owner, boundary, apply;
+  unsigned char doms;     // first pair: domain ids of v0 (bits 0-2) and v1 (bits 3-5)
+  unsigned char pad1;
 };
 static_assert(sizeof(FluxRow) == 64, "a flux row is one 64-byte line");
 

@@ -84,15 +84,18 @@ __device__ __forceinline__ F2 diffuse_uniform2(F2 c, F2 m2, F2 u, F2 zs, F2 ys, 
   return f2_fma(c, f2_add(f2_add(az, ay), ax), u);
 }
 
-// buffer_dj on two voxels, nkoff_dt = -koff_dt.
-__device__ __forceinline__ F2 buffer_dj2(F2 kon_dt, F2 nkoff_dt, F2 tot, F2 b, F2 ca) {
-  return f2_fma(f2_mul(kon_dt, f2_sub(tot, b)), ca, f2_mul(nkoff_dt, b));
+// dt_r * J for one buffer, J = k_on (tot - B) Ca - k_off B (kernel_generic.cpp:495-507), from
+// the deviations dB, dCa of the stored fields (B = base_B + dB, Ca = base_Ca + dCa, ca =
+// the reconstructed Ca): J = J(base) + k_on (tot - base_B) dCa - dB (k_on Ca + k_off), so
+// no term is the difference of two large near-equal products.  nkon = -dt_r k_on,
+// nkoff = -dt_r k_off, a = dt_r k_on (tot - base_B), j0 = dt_r J(base).
+__device__ __forceinline__ float buffer_dj(float nkon, float nkoff, float a, float j0, float db, float dca, float ca) {
+  return __fmaf_rn(db, __fmaf_rn(nkon, ca, nkoff), __fmaf_rn(a, dca, j0));
 }
 
-// dt_r * J for one buffer, J = k_on*(tot-b)*ca - k_off*b (kernel_generic.cpp:495-507), with
-// the rates given premultiplied by dt_r.
-__device__ __forceinline__ float buffer_dj(float kon_dt, float koff_dt, float tot, float b, float ca) {
-  return __fmaf_rn(__fmul_rn(kon_dt, __fsub_rn(tot, b)), ca, -__fmul_rn(koff_dt, b));
+// buffer_dj on two voxels.
+__device__ __forceinline__ F2 buffer_dj2(F2 nkon, F2 nkoff, F2 a, F2 j0, F2 db, F2 dca, F2 ca) {
+  return f2_fma(db, f2_fma(nkon, ca, nkoff), f2_fma(a, dca, j0));
 }
 
 // General buffer reactions: the reference's assign-or-accumulate rule, per buffer in
@@ -104,8 +107,9 @@ __device__ __forceinline__ void react_general(const RealDesc& D, int d, const fl
     if (bi >= D.nbuf) break;
     const int t = bi * D.nd + d;
     const int s0 = D.bsp0[t], s1 = D.bsp1[t];
-    const float b0 = sel(val, s0), b1 = sel(val, s1);
-    const float dJ = buffer_dj(D.kon_dt[t], D.koff_dt[t], D.tot[t], b0, b1);
+    const float b0 = sel(val, s0), b1 = sel(val, s1);     // deviations from the bases
+    const float dJ = buffer_dj(-D.kon_dt[t], -D.koff_dt[t], D.a_dt[t], D.j0_dt[t], b0, b1,
+                               __fadd_rn(D.fbase[d][s1], b1));
     if (pre >> s0 & 1u) put(out, s0, __fadd_rn(sel(out, s0), dJ)); else put(out, s0, __fadd_rn(b0, dJ));
     if (pre >> s1 & 1u) put(out, s1, __fsub_rn(sel(out, s1), dJ)); else put(out, s1, __fsub_rn(b1, dJ));
   }
@@ -191,7 +195,7 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
           if (!code) continue;
           const int slot = (code & 0x7f) - 1;
           if (D.fslot_species[slot] != s) continue;
-          const double self = (double)u, other = (double)un[k];
+          const double self = (double)u + D.base[d][s], other = (double)un[k] + D.base[dn[k]][s];
           if (code & 0x80) acc += pair_flux(D, slot, other, self);
           else acc -= pair_flux(D, slot, self, other);
           any = true;
@@ -202,12 +206,13 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
   }
   if (si.react) {
     if (si.react_fast) {
-      const float ca = val[0];
+      const float dca = val[0], ca = __fadd_rn(D.fbase[d][0], dca);
+      const unsigned rm = D.rmask[d];
 #pragma unroll
       for (int s = 1; s < N; s++) {
+        if (!(rm >> s & 1u)) continue;
         const float4 k = D.rk[d][s];
-        if (k.w == 0.f) continue;
-        const float dJ = buffer_dj(k.x, k.y, k.z, val[s], ca);
+        const float dJ = buffer_dj(k.x, k.y, k.z, k.w, val[s], dca, ca);
         out[s] = __fadd_rn(out[s], dJ);
         out[0] = __fsub_rn(out[0], dJ);
       }
@@ -218,9 +223,9 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
   const unsigned fm = D.fixed_mask[d];
 #pragma unroll
   for (int s = 0; s < N; s++) {
-    if (fm >> s & 1u) out[s] = D.init[d][s];
+    if (fm >> s & 1u) out[s] = D.dinit[d][s];
   }
-  if (D.dirichlet && on_face) out[0] = D.init[d][0];
+  if (D.dirichlet && on_face) out[0] = D.dinit[d][0];
 }
 
 // One thread per voxel; blockIdx.y = realisation.
@@ -293,18 +298,20 @@ __device__ __forceinline__ int gate(const FluxParams& fp, int state, double c0, 
 // stores its new state.  Returns false when the pair carries no flux this step.  CH =
 // false: the caller's rows hold density pairs only (no channel code is compiled).
 template <bool CH>
-__device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int r, int kind, int dsi,
+__device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int species, int kind, int dsi,
                                           int channel, int local_channel, int boundary, int owner, long long v0,
-                                          long long v1, const FluxParams& fp, const float* __restrict__ uold,
-                                          const float* __restrict__ ca, unsigned char* __restrict__ states, int nch,
-                                          long long k, bool stoch, double& J) {
+                                          long long v1, int doms, const FluxParams& fp,
+                                          const float* __restrict__ uold, const float* __restrict__ ca,
+                                          unsigned char* __restrict__ states, int nch, long long k, bool stoch,
+                                          double& J) {
   const long long ti = k + 1;
+  const int d0 = doms & DOMAIN_BITS, d1 = (doms >> 3) & DOMAIN_BITS;
   if (CH && channel >= 0) {
     const int s_old = states[(k & 1) * (long long)nch + channel];
     int s_new = s_old;
     if (stoch && kind != FLUX_SERCA)
-      s_new = gate(fp, s_old, (double)__ldg(ca + v1), (double)ti * D.dt, D.dt * D.stochastic_substep, D.seed,
-                   (unsigned)r, (unsigned)local_channel, (unsigned)boundary, ti);
+      s_new = gate(fp, s_old, (double)__ldg(ca + v1) + D.base[d1][0], (double)ti * D.dt, D.dt * D.stochastic_substep,
+                   D.seed, D.stream, (unsigned)local_channel, (unsigned)boundary, ti);
     if (owner) {
       states[((k + 1) & 1) * (long long)nch + channel] = (unsigned char)s_new;
       if (s_new == 1) atomicAdd(&ctl_r->open_count[(k + 1) & 1], 1);
@@ -312,7 +319,8 @@ __device__ __forceinline__ bool pair_step(const RealDesc& D, RealCtl* ctl_r, int
     if (s_new != 1) return false;
   }
   if (ti % D.substeps[dsi] != 0) return false;
-  const double u0 = (double)__ldg(uold + v0), u1 = (double)__ldg(uold + v1);
+  const double u0 = (double)__ldg(uold + v0) + D.base[d0][species];
+  const double u1 = (double)__ldg(uold + v1) + D.base[d1][species];
   J = kind == FLUX_SERCA ? serca_flux_fast(u0, u1, fp.p[9]) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
   return true;
 }
@@ -349,16 +357,16 @@ __global__ void __launch_bounds__(256, CH ? 4 : 8) k_boundaries(const RealDesc* 
   const float* __restrict__ ca = D.u[cur & 1u][0];
   double acc = 0.0, J;
   bool any = false;
-  if (pair_step<CH>(D, &ctl[row.r], row.r, row.kind, row.dsi, row.channel, row.local_channel, row.boundary,
-                row.owner, row.v0, row.v1, params[row.param], uold, ca, states, nch, k, stoch, J)) {
+  if (pair_step<CH>(D, &ctl[row.r], row.species, row.kind, row.dsi, row.channel, row.local_channel, row.boundary,
+                row.owner, row.v0, row.v1, row.doms, params[row.param], uold, ca, states, nch, k, stoch, J)) {
     acc += (double)row.sign * J;
     any = true;
   }
   for (int e = row.more_begin; e < row.more_end; e++) {
     const FluxEntry en = entries[e];
     const FluxPair pr = pairs[en.pair];
-    if (pair_step<CH>(D, &ctl[row.r], row.r, pr.kind, pr.dsi, pr.channel, pr.local_channel, pr.boundary, en.owner,
-                  pr.v0, pr.v1, params[pr.param], uold, ca, states, nch, k, stoch, J)) {
+    if (pair_step<CH>(D, &ctl[row.r], row.species, pr.kind, pr.dsi, pr.channel, pr.local_channel, pr.boundary,
+                  en.owner, pr.v0, pr.v1, pr.doms, params[pr.param], uold, ca, states, nch, k, stoch, J)) {
       acc += (double)en.sign * J;
       any = true;
     }
@@ -412,7 +420,8 @@ __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restr
   double acc = 0.0;
   bool any = false;
   if (R.w >> dsi & 1u) {
-    const double us = (double)__ldg(uold + a.x), uo = (double)__ldg(uold + a.y);
+    const double us = (double)__ldg(uold + a.x) + D.base[(meta1 >> 16) & DOMAIN_BITS][sp];
+    const double uo = (double)__ldg(uold + a.y) + D.base[(meta1 >> 19) & DOMAIN_BITS][sp];
     const bool to = meta1 & DROW_TO;
     const double u0 = to ? uo : us, u1 = to ? us : uo;
     const double J = (meta1 & DROW_SERCA) ? serca_flux_fast(u0, u1, __hiloint2double(b.y, b.x))
@@ -427,7 +436,8 @@ __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restr
     const FluxPair pr = pairs[en.pair];
     if (!(R.w >> pr.dsi & 1u)) continue;
     const FluxParams& fp = params[pr.param];
-    const double u0 = (double)__ldg(uold + pr.v0), u1 = (double)__ldg(uold + pr.v1);
+    const double u0 = (double)__ldg(uold + pr.v0) + D.base[pr.doms & DOMAIN_BITS][sp];
+    const double u1 = (double)__ldg(uold + pr.v1) + D.base[(pr.doms >> 3) & DOMAIN_BITS][sp];
     const double J = pr.kind == FLUX_SERCA ? serca_flux_fast(u0, u1, fp.p[9]) : ryr_flux(D.dt, D.h, u0, u1, fp.p);
     acc += (double)en.sign * J;
     any = true;
@@ -437,13 +447,17 @@ __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restr
 
 // Step epilogue, one thread per realisation, after the boundary kernel: advance the
 // step counter, apply the abort rule (species.c:3476-3486) on the openness counted by
-// the boundary kernel, stop at the last step.
+// the boundary kernel, stop at the last step.  flags (nullable): the stop flag of every
+// realisation after this step.
 __global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl, StepRec* __restrict__ rec,
-                           int nreal) {
+                           int nreal, int* __restrict__ flags) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nreal) return;
   RealCtl& C = ctl[r];
-  if (C.stopped) return;
+  if (C.stopped) {
+    if (flags) flags[r] = 1;
+    return;
+  }
   const RealDesc& D = descs[r];
   const long long k = C.step;
   const long long ti = k + 1;
@@ -461,6 +475,7 @@ __global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restri
   }
   if (C.step >= D.total_steps) C.stopped = 1;
   write_steprec(D, C, rec[r]);
+  if (flags) flags[r] = C.stopped;
 }
 
 // Output reductions: partial min / max / sum over a block for one species of one
@@ -479,7 +494,7 @@ __global__ void __launch_bounds__(256) k_reduce_partial(const RealDesc* __restri
     const int x = (int)(v / D.plane);
     const long long idx = (long long)x * D.P + (v - (long long)x * D.plane);
     const int d = D.dom[idx] & DOMAIN_BITS;
-    const double val = (double)u[idx];
+    const double val = (double)u[idx] + D.base[d][s];
 #pragma unroll
     for (int dd = 0; dd < ND; dd++) {
       if (dd == d) {

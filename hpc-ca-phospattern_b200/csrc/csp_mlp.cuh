@@ -356,10 +356,13 @@ struct RxVoxel {
 };
 
 // p = v mod D.P (the position within the plane), tracked by the caller; uo / un = the
-// old / new buffer of every species, dom = the domain bytes (block-shared copies).
+// old / new buffer of every species, dom = the domain bytes, base = the fields' bases
+// (RealDesc::fbase; block-shared copies).  The old values are reconstructed (base plus
+// stored deviation) for the network and the integrators; the new values stay deviations,
+// which the increments are added to.
 __device__ __forceinline__ void rx_fetch(const float* const* uo, const float* const* un,
                                          const unsigned char* __restrict__ dom, int plane, const RxConst* sk,
-                                         long long v, int p, long long nvox, RxVoxel& X) {
+                                         const float (*base)[NS], long long v, int p, long long nvox, RxVoxel& X) {
   X.mine = false;
   X.d = 0;
   X.c = X.nc = 0.f;
@@ -373,12 +376,12 @@ __device__ __forceinline__ void rx_fetch(const float* const* uo, const float* co
   for (int q = 0; q < MLP_SLOTS; q++) any = any || kc.tot[q] > 0.f;
   if (!any) return;
   X.mine = true;
-  X.c = uo[0][v];
+  X.c = __fadd_rn(base[X.d][0], uo[0][v]);
   X.nc = un[0][v];
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
     if (kc.tot[q] > 0.f) {
-      X.b[q] = uo[q + 1][v];
+      X.b[q] = __fadd_rn(base[X.d][q + 1], uo[q + 1][v]);
       X.nb[q] = un[q + 1][v];
     }
   }
@@ -450,6 +453,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   __shared__ RxConst sk[ND];
   __shared__ float s_thr[ND][MLP_SLOTS];
   __shared__ unsigned s_fm[ND];
+  __shared__ float s_base[ND][NS];
   __shared__ const float* s_uo[NS];
   __shared__ const float* s_un[NS];
   __shared__ long long s_pend[MLP_DEPLOY_T / 32][64];   // per warp: queued voxels (up to two tiles)
@@ -470,6 +474,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     sk[threadIdx.x] = kc;
     for (int q = 0; q < MLP_SLOTS; q++) s_thr[threadIdx.x][q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
     s_fm[threadIdx.x] = D.fixed_mask[threadIdx.x < D.nd ? threadIdx.x : 0];
+    for (int s = 0; s < NS; s++) s_base[threadIdx.x][s] = D.fbase[threadIdx.x][s];
   }
   if (threadIdx.x < NS) {
     const int t = threadIdx.x;
@@ -503,7 +508,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
       xq = (int)(v / P);
       pq = (int)(v - (long long)xq * P);
     }
-    rx_fetch(s_uo, s_un, dom, plane, sk, have ? v : nvox, pq, nvox, Y);
+    rx_fetch(s_uo, s_un, dom, plane, sk, s_base, have ? v : nvox, pq, nvox, Y);
     const RxConst& kc = sk[Y.d];
     float x[MLP_IN], t[MLP_OUT], db[MLP_SLOTS], dc = 0.f;
     if (have) rx_features(kc, Y.d, dtr, Y.c, Y.b, x);
@@ -522,7 +527,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     __syncwarp();
   };
   RxVoxel X;
-  rx_fetch(s_uo, s_un, dom, plane, sk, v0, pf, nvox, X);
+  rx_fetch(s_uo, s_un, dom, plane, sk, s_base, v0, pf, nvox, X);
   for (int it = 0; it < MLP_DEPLOY_VPT; it++) {
     const long long v = v0 + (long long)it * MLP_DEPLOY_T;
     const RxVoxel Y = X;
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     xc = xf;
     pf += MLP_DEPLOY_T;
     while (pf >= P) { pf -= P; xf++; }
-    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(s_uo, s_un, dom, plane, sk, v + MLP_DEPLOY_T, pf, nvox, X);
+    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(s_uo, s_un, dom, plane, sk, s_base, v + MLP_DEPLOY_T, pf, nvox, X);
     const int d = Y.d;
     const RxConst& kc = sk[d];
     bool elig = false, skip = false;

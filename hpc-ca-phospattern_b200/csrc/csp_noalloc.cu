@@ -14,6 +14,7 @@
 #include <mutex>
 
 #include "../../include/csparks.h"
+#include "csp_device.cuh"   // csp::DOMAIN_BITS: the domain-id bits of a domain byte
 
 namespace {
 
@@ -37,7 +38,7 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_noalloc_partial(const float
 #pragma unroll
   for (int d = 0; d < ND; d++) { mn[d] = FLT_MAX; mx[d] = FLT_MIN; sm[d] = 0.0; }
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int d = dom[i] & 7;
+    const int d = dom[i] & csp::DOMAIN_BITS;
     const double v = (double)u[i];
 #pragma unroll
     for (int dd = 0; dd < ND; dd++)
@@ -90,7 +91,9 @@ __global__ void k_noalloc_final(const double* __restrict__ part, int nblk, int n
 
 }  // namespace
 
-// Address of the partials array on the current device, looked up once per device.
+// Address of the partials array on the current device, looked up once per device and kept
+// for the life of the process.  A cudaDeviceReset reloads the module and may move the
+// array, so this entry point is not supported on a device after cudaDeviceReset.
 static int noalloc_setup(double** ptr) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return CSP_ECUDA;

@@ -31,6 +31,7 @@ using namespace csp;
 namespace {
 
 constexpr int STEPS_PER_GRAPH = 16;
+constexpr int PHASE_SAMPLE = 16;            // steps timed per advance call (csp_set_phase_timing)
 thread_local char g_create_error[512];
 
 struct HostReal {
@@ -131,8 +132,8 @@ struct csp_handle {
   int* d_err = nullptr;
   double* d_red = nullptr;
   double* d_red_out = nullptr;
-  double* d_stage = nullptr;         // FP64 state staging of upload / download (one realisation)
-  size_t stage_elems = 0;
+  void* d_stage = nullptr;           // host-state staging of upload / download (one realisation)
+  size_t stage_bytes = 0;
   // asynchronous snapshots: FP64 fields converted on the handle stream into d_snap, copied
   // on snap_stream into the page-locked h_snap (ev_snap: converted, ev_copy: copied)
   double* d_snap = nullptr;
@@ -146,10 +147,30 @@ struct csp_handle {
   int nrows_density = 0;             // rows [0, nrows_density) have density pairs only
   DensityRow* d_drows = nullptr;     // the density rows in 32 bytes (null: k_boundaries<false>)
   int ndrows = 0;                    // compact rows (pair rows count once)
+  // rows are realisation-major: the rows of realisation r are [first[r], first[r+1]) of the
+  // compact density rows, the density-only FluxRows and the channel FluxRows
+  std::vector<int> drow_first, krow_first, crow_first;
+  // csp_run_states: host-to-device stream, staging (two input and two output slots), per
+  // step stop flags
+  cudaStream_t in_stream = nullptr;
+  void* d_pipe = nullptr;
+  size_t pipe_bytes = 0;
+  int* d_stepflags = nullptr;
+  size_t stepflags_elems = 0;
   StepRec* d_rec = nullptr;          // per realisation: what its running step does
   int max_plane_vox = 0;
   long long max_vox = 0;
   int kernel = 0;                 // 0 staged, 1 direct
+  int inject_wait = 0;            // csp_test_wait_timeout armed (direct launches, no graph)
+  // csp_set_phase_timing: the first steps of every advance call run as direct launches
+  // with events between the step's kernels; the sample's per-phase device time, scaled to
+  // the steps of the call, is added to phase_ms at the call's wait
+  int phase_timing = 0;
+  cudaEvent_t phase_ev[PHASE_SAMPLE * (CSP_NUM_PHASES + 1)] = {};
+  int phase_sampled = 0;
+  int64_t phase_call_steps = 0;
+  double phase_ms[CSP_NUM_PHASES] = {};
+  int64_t phase_steps = 0;
   StagedPlan plan;
   cudaGraphExec_t graph = nullptr;
   int graph_kernel = -1;
@@ -173,6 +194,14 @@ static int fail(csp_handle* h, int code, const char* fmt, ...) {
   if (h) h->msg = buf; else snprintf(g_create_error, sizeof g_create_error, "%s", buf);
   return code;
 }
+
+// Calls that touch the device state of a handle are refused while an asynchronous advance
+// is pending: they would queue behind it and break csp_advance_wait's contract.
+#define CSP_NOT_PENDING(h)                                                                    \
+  do {                                                                                        \
+    if ((h)->advance_pending)                                                                 \
+      return fail(h, CSP_EINVAL, "an asynchronous advance is pending (csp_advance_wait)");    \
+  } while (0)
 
 #define CUDA_TRY(h, call)                                                                     \
   do {                                                                                        \
@@ -459,13 +488,43 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         if (s1 != 0 || s0 == 0 || D.rtab[dd][s0] >= 0) D.react_fast = 0;
         else D.rtab[dd][s0] = (signed char)bi;
       }
+    // field bases (RealDesc::base): for a diffusing species the initial value of the first
+    // domain of each set of domains it diffuses between (coefficient tables, species.c:
+    // 1547-1560), else each domain's own initial value
+    for (int s = 0; s < m.num_species; s++) {
+      int comp[ND];
+      for (int a = 0; a < nd; a++) comp[a] = a;
+      const int k = D.dsi_of[s];
+      for (bool changed = k >= 0; changed;) {
+        changed = false;
+        for (int a = 0; a < nd; a++)
+          for (int b = 0; b < nd; b++)
+            if (a != b && d.coef[k][a][b] != 0.0 && comp[a] < comp[b]) { comp[b] = comp[a]; changed = true; }
+      }
+      for (int a = 0; a < nd; a++) {
+        D.base[a][s] = m.domain[comp[a]].init[s];
+        D.fbase[a][s] = (float)D.base[a][s];
+        D.dinit[a][s] = (float)(m.domain[a].init[s] - D.base[a][s]);
+      }
+    }
+    // buffer reactions about the bases (buffer_dj): a_dt = dt_r k_on (tot - base_s0),
+    // j0_dt = dt_r (k_on (tot - base_s0) base_s1 - k_off base_s0), FP64 before rounding
+    for (int bi = 0; bi < d.nbuf; bi++)
+      for (int dd = 0; dd < nd; dd++) {
+        const int t = bi * nd + dd;
+        const double dtr = d.dt * d.reaction_substep;
+        const double b0 = D.base[dd][d.bsp0[t]], b1 = D.base[dd][d.bsp1[t]];
+        D.a_dt[t] = (float)(dtr * d.kon[t] * (d.tot[t] - b0));
+        D.j0_dt[t] = (float)(dtr * (d.kon[t] * (d.tot[t] - b0) * b1 - d.koff[t] * b0));
+      }
     for (int dd = 0; dd < ND; dd++)
       for (int s = 0; s < NS; s++) {
         D.cdiag[dd][s] = (dd < nd && D.dsi_of[s] >= 0) ? D.coef[D.dsi_of[s]][dd * ND + dd] : 0.f;
         const int bi = D.rtab[dd][s];
         if (bi >= 0) {
           const int t = bi * nd + dd;
-          D.rk[dd][s] = make_float4(D.kon_dt[t], D.koff_dt[t], D.tot[t], 1.f);
+          D.rk[dd][s] = make_float4(-D.kon_dt[t], -D.koff_dt[t], D.a_dt[t], D.j0_dt[t]);
+          D.rmask[dd] |= (unsigned char)(1u << s);
         } else {
           D.rk[dd][s] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -480,6 +539,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     D.total_steps = d.total_steps;
     D.dt = d.dt; D.h = d.h; D.tabort = o.tabort;
     D.seed = o.seed;
+    D.stream = (unsigned)(r + o.stream_offset);
     for (int b = 0; b < 2; b++)
       for (int s = 0; s < m.num_species; s++) {
         D.u[b][s] = h->d_fields + foff;
@@ -503,7 +563,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     for (int dd = 0; dd < ND; dd++) hr.volumes[dd] = dd < nd ? gcount[dd] * m.h_geom * m.h_geom * m.h_geom : 0.0;
     hostf.assign(hr.field_elems, 0.f);
     for (int s = 0; s < m.num_species; s++) {
-      for (size_t i = 0; i < hr.field_elems; i++) hostf[i] = (float)m.domain[hostd[i]].init[s];
+      for (size_t i = 0; i < hr.field_elems; i++) hostf[i] = D.dinit[hostd[i]][s];   // init - base
       cudaMemcpyAsync(D.u[0][s], hostf.data(), hr.field_elems * sizeof(float), cudaMemcpyHostToDevice, h->stream);
       cudaStreamSynchronize(h->stream);
     }
@@ -571,6 +631,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         p.local_channel = i;
         p.v0 = lin(&bv[6 * i]);
         p.v1 = lin(&bv[6 * i + 3]);
+        p.doms = (hostd[p.v0] & DOMAIN_BITS) | (hostd[p.v1] & DOMAIN_BITS) << 3;
         pairs.push_back(p);
         fused.push_back(0);
       }
@@ -710,7 +771,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
           const double c0 = use_ryr_values && i < nr ? c0_at(rv, i) : c0_at(bvox[bi], i);
           const double ko = std::fmax(std::fmin(std::pow(c0 / p[9], p[2]), p[3]), p[4]);
           const double kc = std::fmax(std::fmin(std::pow(c0 / p[0], p[5]), p[1]), p[7]);
-          const double rv_ = channel_uniform(o.seed, (unsigned)r, (unsigned)i, (unsigned)bi, 0);
+          const double rv_ = channel_uniform(o.seed, (unsigned)(r + o.stream_offset), (unsigned)i, (unsigned)bi, 0);
           states0[base + i] = rv_ <= kc / (ko + kc) ? 0 : 1;
         }
         return CSP_OK;
@@ -770,6 +831,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
       row.local_channel = p0.local_channel; row.sign = sides[i].sign;
       row.dsi = (unsigned char)p0.dsi; row.kind = (unsigned char)p0.kind; row.owner = (unsigned char)sides[i].owner;
       row.boundary = (unsigned char)p0.boundary;
+      row.doms = (unsigned char)p0.doms;
     }
     j = i + 1;
     row.more_begin = (int)entries.size();
@@ -826,8 +888,9 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     d.more_begin = rw.more_begin;
     d.scale = rw.kind == FLUX_SERCA ? params[rw.param].p[9] : 0.0;
     d.meta0 = (unsigned)rw.param | ((unsigned)rw.species << 16) | ((unsigned)rw.dsi << 24);
+    const unsigned d0 = rw.doms & DOMAIN_BITS, d1 = (rw.doms >> 3) & DOMAIN_BITS;
     d.meta1 = (rw.apply ? DROW_APPLY : 0u) | (to ? DROW_TO : 0u) | (rw.kind == FLUX_SERCA ? DROW_SERCA : 0u) |
-              ((unsigned)(rw.more_end - rw.more_begin) << 8);
+              ((unsigned)(rw.more_end - rw.more_begin) << 8) | (to ? d1 : d0) << 16 | (to ? d0 : d1) << 19;
     drows.push_back(d);
   }
   // pairs whose two voxels have single-pair rows: one pair row instead of two rows
@@ -840,13 +903,13 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     std::vector<char> gone(drows.size(), 0);
     for (size_t i = 0; i < drows.size(); i++) {
       DensityRow& t = drows[i];
-      if (!(t.meta1 & DROW_TO) || (t.meta1 >> 8) != 0u) continue;
+      if (!(t.meta1 & DROW_TO) || ((t.meta1 >> 8) & 0xffu) != 0u) continue;
       auto it = std::lower_bound(byv.begin(), byv.end(), 0, [&](int x, int) {
         return drows[x].r != t.r ? drows[x].r < t.r : drows[x].v < t.vo;
       });
       if (it == byv.end() || drows[*it].r != t.r || drows[*it].v != t.vo) continue;
       const DensityRow& f = drows[*it];
-      if ((f.meta1 & (DROW_TO | DROW_PAIR)) || (f.meta1 >> 8) != 0u || f.vo != t.v || f.meta0 != t.meta0 ||
+      if ((f.meta1 & (DROW_TO | DROW_PAIR)) || ((f.meta1 >> 8) & 0xffu) != 0u || f.vo != t.v || f.meta0 != t.meta0 ||
           gone[*it])
         continue;
       t.meta1 |= DROW_PAIR | ((f.meta1 & DROW_APPLY) ? DROW_APPLY_FROM : 0u);
@@ -858,6 +921,16 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     drows.resize(k);
   }
   h->ndrows = (int)drows.size();
+  {
+    auto firsts = [&](std::vector<int>& f, int count, auto r_of) {
+      f.assign(n + 1, count);
+      for (int i = count - 1; i >= 0; i--) f[r_of(i)] = i;
+      for (int r = n - 1; r >= 0; r--) f[r] = std::min(f[r], f[r + 1]);
+    };
+    firsts(h->drow_first, h->ndrows, [&](int i) { return drows[i].r; });
+    firsts(h->krow_first, h->nrows_density, [&](int i) { return rows[i].r; });
+    firsts(h->crow_first, h->nrows - h->nrows_density, [&](int i) { return rows[h->nrows_density + i].r; });
+  }
   auto upload = [&](void** dst, const void* src, size_t bytes) -> bool {
     if (bytes == 0) bytes = 16;
     if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
@@ -910,40 +983,87 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
   return CSP_OK;
 }
 
-static void launch_voxels(csp_handle* h) {
+// The kernels of one step, for the realisations [r0, r1) (r1 < 0: all of them, the
+// launches csp_advance captures).  Realisations are independent, so stepping a range
+// gives that range exactly what a step of the whole batch gives it.
+static void launch_voxels(csp_handle* h, int r0 = 0, int r1 = -1) {
+  if (r1 < 0) r1 = h->n;
   if (h->kernel == 1) {
-    dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)h->n);
-    k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_err);
+    dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)(r1 - r0));
+    k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc + r0, h->d_ctl + r0, h->d_err);
   } else {
-    staged_launch(h->plan, h->d_desc, h->d_ctl, h->d_err, h->stream);
+    staged_launch(h->plan, h->d_desc, h->d_ctl, h->d_err, h->stream, h->inject_wait != 0, r0, r1);
   }
 }
 
-static void launch_boundaries(csp_handle* h) {
-  const int nd = h->nrows_density, nc = h->nrows - h->nrows_density;
-  if (nd > 0 && h->d_drows)
-    k_density_rows<<<(h->ndrows + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_rec, h->d_drows, h->ndrows,
-                                                                   h->d_entries, h->d_pairs, h->d_params);
-  else if (nd > 0)
-    k_boundaries<false><<<(nd + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows, nd, h->d_entries,
-                                                                  h->d_pairs, h->d_params, h->d_states,
-                                                                  std::max(h->nch, 1));
-  if (nc > 0)
-    k_boundaries<true><<<(nc + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows + nd, nc, h->d_entries,
-                                                                 h->d_pairs, h->d_params, h->d_states,
-                                                                 std::max(h->nch, 1));
-  if (h->surrogate) {
-    const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
-    dim3 grid((unsigned)((h->max_vox + span - 1) / span), (unsigned)h->n);
-    k_react_surrogate<<<grid, MLP_DEPLOY_T, MLP_DEPLOY_SMEM, h->stream>>>(h->d_desc, h->d_ctl, h->d_mlp,
-                                                                          h->surrogate_tol, h->d_mlp_cnt);
+// The flux-row kernels of one step: density-boundary rows (SERCA), then the channel rows
+// (gating + RyR flux), for the realisations [r0, r1).
+static void launch_density_rows(csp_handle* h, int r0, int r1) {
+  const int nd = h->nrows_density;
+  const int dr0 = h->drow_first[r0], dr1 = h->drow_first[r1];
+  const int kr0 = h->krow_first[r0], kr1 = h->krow_first[r1];
+  if (nd > 0 && h->d_drows) {
+    if (dr1 > dr0)
+      k_density_rows<<<(dr1 - dr0 + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_rec, h->d_drows + dr0,
+                                                                     dr1 - dr0, h->d_entries, h->d_pairs,
+                                                                     h->d_params);
+  } else if (kr1 > kr0) {
+    k_boundaries<false><<<(kr1 - kr0 + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows + kr0,
+                                                                         kr1 - kr0, h->d_entries, h->d_pairs,
+                                                                         h->d_params, h->d_states,
+                                                                         std::max(h->nch, 1));
   }
-  k_epilogue<<<(h->n + 127) / 128, 128, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rec, h->n);
 }
 
-static cudaError_t launch_step(csp_handle* h) {
+static void launch_channel_rows(csp_handle* h, int r0, int r1) {
+  const int nd = h->nrows_density;
+  const int cr0 = h->crow_first[r0], cr1 = h->crow_first[r1];
+  if (cr1 > cr0)
+    k_boundaries<true><<<(cr1 - cr0 + 255) / 256, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_rows + nd + cr0,
+                                                                        cr1 - cr0, h->d_entries, h->d_pairs,
+                                                                        h->d_params, h->d_states,
+                                                                        std::max(h->nch, 1));
+}
+
+static void launch_surrogate(csp_handle* h, int r0, int r1) {
+  if (!h->surrogate) return;
+  const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
+  dim3 grid((unsigned)((h->max_vox + span - 1) / span), (unsigned)(r1 - r0));
+  k_react_surrogate<<<grid, MLP_DEPLOY_T, MLP_DEPLOY_SMEM, h->stream>>>(h->d_desc + r0, h->d_ctl + r0, h->d_mlp,
+                                                                        h->surrogate_tol, h->d_mlp_cnt);
+}
+
+static void launch_epilogue(csp_handle* h, int r0, int r1, int* step_flags) {
+  k_epilogue<<<(r1 - r0 + 127) / 128, 128, 0, h->stream>>>(h->d_desc + r0, h->d_ctl + r0, h->d_rec + r0, r1 - r0,
+                                                           step_flags);
+}
+
+static void launch_boundaries(csp_handle* h, int r0 = 0, int r1 = -1, int* step_flags = nullptr) {
+  if (r1 < 0) r1 = h->n;
+  launch_density_rows(h, r0, r1);
+  launch_channel_rows(h, r0, r1);
+  launch_surrogate(h, r0, r1);
+  launch_epilogue(h, r0, r1, step_flags);
+}
+
+// One step of every realisation with an event before and after each phase (CSP_PHASE_*).
+static void launch_step_timed(csp_handle* h, cudaEvent_t* ev) {
+  cudaEventRecord(ev[0], h->stream);
   launch_voxels(h);
-  launch_boundaries(h);
+  cudaEventRecord(ev[1 + CSP_PHASE_VOXELS], h->stream);
+  launch_density_rows(h, 0, h->n);
+  cudaEventRecord(ev[1 + CSP_PHASE_DENSITY], h->stream);
+  launch_channel_rows(h, 0, h->n);
+  cudaEventRecord(ev[1 + CSP_PHASE_CHANNELS], h->stream);
+  launch_surrogate(h, 0, h->n);
+  cudaEventRecord(ev[1 + CSP_PHASE_SURROGATE], h->stream);
+  launch_epilogue(h, 0, h->n, nullptr);
+  cudaEventRecord(ev[1 + CSP_PHASE_EPILOGUE], h->stream);
+}
+
+static cudaError_t launch_step(csp_handle* h, int r0 = 0, int r1 = -1, int* step_flags = nullptr) {
+  launch_voxels(h, r0, r1);
+  launch_boundaries(h, r0, r1, step_flags);
   return cudaGetLastError();
 }
 
@@ -970,6 +1090,23 @@ static int ensure_graph(csp_handle* h) {
   return CSP_OK;
 }
 
+// The timed sample of the last advance call, scaled to the call's steps, into phase_ms.
+static void add_phase_sample(csp_handle* h) {
+  if (!h->phase_sampled) return;
+  double ms[CSP_NUM_PHASES] = {};
+  for (int i = 0; i < h->phase_sampled; i++) {
+    const cudaEvent_t* ev = &h->phase_ev[i * (CSP_NUM_PHASES + 1)];
+    for (int p = 0; p < CSP_NUM_PHASES; p++) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, ev[p], ev[p + 1]) == cudaSuccess) ms[p] += t;
+    }
+  }
+  const double scale = (double)h->phase_call_steps / h->phase_sampled;
+  for (int p = 0; p < CSP_NUM_PHASES; p++) h->phase_ms[p] += ms[p] * scale;
+  h->phase_steps += h->phase_call_steps;
+  h->phase_sampled = 0;
+}
+
 static int finish_advance(csp_handle* h, int32_t* stop_flags) {
   int err = 0;
   CUDA_TRY(h, cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -981,6 +1118,7 @@ static int finish_advance(csp_handle* h, int32_t* stop_flags) {
     h->real[r].info.stopped = ctl[r].stopped;
     if (stop_flags) stop_flags[r] = ctl[r].stopped;
   }
+  add_phase_sample(h);
   if (err) return fail(h, CSP_EDEVICE, "device error word %d (%s)", err,
                        (err & ERR_TIMEOUT) ? "bounded wait timed out" : "index out of bounds");
   return CSP_OK;
@@ -988,6 +1126,7 @@ static int finish_advance(csp_handle* h, int32_t* stop_flags) {
 
 extern "C" int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_ms, float* boundary_ms) {
   if (!h || nsteps < 0) return fail(h, CSP_EINVAL, "bad handle or nsteps");
+  CSP_NOT_PENDING(h);
   std::vector<cudaEvent_t> ev(3 * (size_t)nsteps);
   for (auto& e : ev) CUDA_TRY(h, cudaEventCreate(&e));
   for (int64_t i = 0; i < nsteps; i++) {
@@ -1015,11 +1154,22 @@ extern "C" int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_m
 }
 
 static int launch_advance(csp_handle* h, int64_t nsteps) {
-  int rc = ensure_graph(h);
-  if (rc) return rc;
+  if (!h->inject_wait) {
+    int rc = ensure_graph(h);
+    if (rc) return rc;
+  }
   CUDA_TRY(h, cudaEventRecord(h->ev0, h->stream));
   int64_t left = nsteps;
-  while (left >= STEPS_PER_GRAPH) {
+  h->phase_sampled = 0;
+  if (h->phase_timing && left > 0) {
+    const int ns = (int)std::min<int64_t>(left, PHASE_SAMPLE);
+    for (int i = 0; i < ns; i++) launch_step_timed(h, &h->phase_ev[i * (CSP_NUM_PHASES + 1)]);
+    CUDA_TRY(h, cudaGetLastError());
+    h->phase_sampled = ns;
+    h->phase_call_steps = nsteps;
+    left -= ns;
+  }
+  while (!h->inject_wait && left >= STEPS_PER_GRAPH) {
     CUDA_TRY(h, cudaGraphLaunch(h->graph, h->stream));
     left -= STEPS_PER_GRAPH;
   }
@@ -1069,169 +1219,305 @@ extern "C" int csp_get_info(const csp_handle* h, int32_t r, csp_info* info) {
   return CSP_OK;
 }
 
-// Physical-order FP64 state <-> device-order FP32 fields of one realisation: one thread
-// per (species, physical voxel); the physical index is linear (coalesced FP64 side), the
-// device index follows the realisation's axis order.
+// Physical-order host state (FP64 or FP32) <-> device-order FP32 fields of one realisation:
+// one thread per (species, physical voxel); the physical index is linear (coalesced
+// host-side layout), the device index follows the realisation's axis order.  Which buffer
+// of a species is current is read from the realisation's progress block when the kernel
+// runs, so a conversion queued behind steps converts what those steps leave current.
 struct StateMap {
-  float* f[NS];                      // current buffer of each species
+  float* f[2][NS];                   // both buffers of each species
+  const RealCtl* ctl;                // the realisation's progress block
+  const unsigned char* dom;          // domain bytes (device order)
+  double base[ND][NS];               // field bases: value = base[domain][s] + field
   int n[3];                          // physical voxels per axis
   long long stride[3];               // device index stride of each physical axis
   long long nvox;
   int ns;
 };
 
-__global__ void k_state_in(const double* __restrict__ src, StateMap m) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= m.nvox * m.ns) return;
-  const int s = (int)(i / m.nvox);
-  const long long v = i - (long long)s * m.nvox;
+__device__ __forceinline__ long long state_index(const StateMap& m, long long v) {
   const int z = (int)(v % m.n[2]);
   const long long xy = v / m.n[2];
   const int y = (int)(xy % m.n[1]), x = (int)(xy / m.n[1]);
-  m.f[s][x * m.stride[0] + y * m.stride[1] + z * m.stride[2]] = __double2float_rn(src[i]);
+  return x * m.stride[0] + y * m.stride[1] + z * m.stride[2];
 }
 
-__global__ void k_state_out(double* __restrict__ dst, StateMap m) {
+__device__ __forceinline__ float* state_field(const StateMap& m, int s) {
+  const unsigned cur = m.ctl->cur_mask[m.ctl->step & 1];
+  return m.f[(cur >> s) & 1u][s];
+}
+
+// host value u -> stored deviation (float)(u - base), one rounding
+template <class T>
+__global__ void k_state_in(const T* __restrict__ src, StateMap m) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= m.nvox * m.ns) return;
   const int s = (int)(i / m.nvox);
-  const long long v = i - (long long)s * m.nvox;
-  const int z = (int)(v % m.n[2]);
-  const long long xy = v / m.n[2];
-  const int y = (int)(xy % m.n[1]), x = (int)(xy / m.n[1]);
-  dst[i] = (double)m.f[s][x * m.stride[0] + y * m.stride[1] + z * m.stride[2]];
+  const long long di = state_index(m, i - (long long)s * m.nvox);
+  const double b = m.base[m.dom[di] & DOMAIN_BITS][s];
+  state_field(m, s)[di] = (float)((double)src[i] - b);
 }
 
-static int state_map(csp_handle* h, int r, StateMap& m) {
-  RealCtl c;
-  int rc = read_ctl(h, r, c);
-  if (rc) return rc;
-  const HostReal& hr = h->real[r];
-  const RealDesc& D = hr.desc;
-  const unsigned cur = c.cur_mask[c.step & 1];
-  memset(&m, 0, sizeof m);
-  m.ns = D.ns;
-  for (int s = 0; s < D.ns; s++) m.f[s] = D.u[(cur >> s) & 1u][s];
-  for (int a = 0; a < 3; a++) m.n[a] = hr.nphys[a];
-  // device axis i holds physical axis perm[i]; device strides P, nz, 1
-  const long long dstr[3] = {(long long)D.P, (long long)D.nz, 1};
-  for (int i = 0; i < 3; i++) m.stride[hr.perm[i]] = dstr[i];
-  m.nvox = (long long)m.n[0] * m.n[1] * m.n[2];
-  const size_t need = (size_t)m.nvox * m.ns;
-  if (need > h->stage_elems) {
-    cudaFree(h->d_stage);
-    h->d_stage = nullptr;
-    h->stage_elems = 0;
-    if (cudaMalloc(&h->d_stage, need * sizeof(double)) != cudaSuccess)
-      return fail(h, CSP_ENOMEM, "state staging buffer of %.1f MB", need * 8.0 / 1e6);
-    h->stage_elems = need;
-  }
-  return CSP_OK;
-}
-
-extern "C" int csp_upload_state(csp_handle* h, int32_t r, const double* u) {
-  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
-  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
-  StateMap m;
-  int rc = state_map(h, r, m);
-  if (rc) return rc;
-  const long long n = m.nvox * m.ns;
-  CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, u, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-  k_state_in<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, m);
-  CUDA_TRY(h, cudaGetLastError());
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  return CSP_OK;
-}
-
-extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
-  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
-  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
-  StateMap m;
-  int rc = state_map(h, r, m);
-  if (rc) return rc;
-  const long long n = m.nvox * m.ns;
-  k_state_out<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, m);
-  CUDA_TRY(h, cudaGetLastError());
-  CUDA_TRY(h, cudaMemcpyAsync(u, h->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  return CSP_OK;
-}
-
-// Every realisation's state in one call: one read of the progress blocks, the copies and
-// conversions of all realisations queued back to back on the handle stream (the staging
-// buffer is reused in stream order), one wait at the end.
-static int state_maps(csp_handle* h, std::vector<StateMap>& maps) {
-  std::vector<RealCtl> ctl(h->n);
-  CUDA_TRY(h, cudaMemcpyAsync(ctl.data(), h->d_ctl, h->n * sizeof(RealCtl), cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  maps.assign(h->n, StateMap{});
-  size_t need = 0;
-  for (int r = 0; r < h->n; r++) {
-    StateMap& m = maps[r];
-    const HostReal& hr = h->real[r];
-    const RealDesc& D = hr.desc;
-    const unsigned cur = ctl[r].cur_mask[ctl[r].step & 1];
-    m.ns = D.ns;
-    for (int s = 0; s < D.ns; s++) m.f[s] = D.u[(cur >> s) & 1u][s];
-    for (int a = 0; a < 3; a++) m.n[a] = hr.nphys[a];
-    const long long dstr[3] = {(long long)D.P, (long long)D.nz, 1};
-    for (int i = 0; i < 3; i++) m.stride[hr.perm[i]] = dstr[i];
-    m.nvox = (long long)m.n[0] * m.n[1] * m.n[2];
-    need = std::max(need, (size_t)m.nvox * m.ns);
-  }
-  if (need > h->stage_elems) {
-    cudaFree(h->d_stage);
-    h->d_stage = nullptr;
-    h->stage_elems = 0;
-    if (cudaMalloc(&h->d_stage, need * sizeof(double)) != cudaSuccess)
-      return fail(h, CSP_ENOMEM, "state staging buffer of %.1f MB", need * 8.0 / 1e6);
-    h->stage_elems = need;
-  }
-  return CSP_OK;
-}
-
-extern "C" int csp_upload_states(csp_handle* h, const double* const* u) {
-  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
-  for (int r = 0; r < h->n; r++)
-    if (!u[r]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
-  std::vector<StateMap> maps;
-  int rc = state_maps(h, maps);
-  if (rc) return rc;
-  for (int r = 0; r < h->n; r++) {
-    const long long n = maps[r].nvox * maps[r].ns;
-    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, u[r], n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    k_state_in<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, maps[r]);
-    CUDA_TRY(h, cudaGetLastError());
-  }
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  return CSP_OK;
-}
-
-extern "C" int csp_download_states(csp_handle* h, double* const* u) {
-  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
-  for (int r = 0; r < h->n; r++)
-    if (!u[r]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
-  std::vector<StateMap> maps;
-  int rc = state_maps(h, maps);
-  if (rc) return rc;
-  for (int r = 0; r < h->n; r++) {
-    const long long n = maps[r].nvox * maps[r].ns;
-    k_state_out<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(h->d_stage, maps[r]);
-    CUDA_TRY(h, cudaGetLastError());
-    CUDA_TRY(h, cudaMemcpyAsync(u[r], h->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  }
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  return CSP_OK;
+// stored deviation -> host value (double)field + base (FP32 hosts: rounded once more)
+template <class T>
+__global__ void k_state_out(T* __restrict__ dst, StateMap m) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m.nvox * m.ns) return;
+  const int s = (int)(i / m.nvox);
+  const long long di = state_index(m, i - (long long)s * m.nvox);
+  dst[i] = static_cast<T>((double)state_field(m, s)[di] + m.base[m.dom[di] & DOMAIN_BITS][s]);
 }
 
 // One species of the physical-order FP64 state (the species slot of k_state_out's output).
 __global__ void k_state_out_species(double* __restrict__ dst, StateMap m, int s) {
   const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (v >= m.nvox) return;
-  const int z = (int)(v % m.n[2]);
-  const long long xy = v / m.n[2];
-  const int y = (int)(xy % m.n[1]), x = (int)(xy / m.n[1]);
-  dst[v] = (double)m.f[s][x * m.stride[0] + y * m.stride[1] + z * m.stride[2]];
+  const long long di = state_index(m, v);
+  dst[v] = (double)state_field(m, s)[di] + m.base[m.dom[di] & DOMAIN_BITS][s];
+}
+
+static StateMap make_state_map(const csp_handle* h, int r) {
+  StateMap m;
+  memset(&m, 0, sizeof m);
+  const HostReal& hr = h->real[r];
+  const RealDesc& D = hr.desc;
+  m.ns = D.ns;
+  for (int s = 0; s < D.ns; s++) { m.f[0][s] = D.u[0][s]; m.f[1][s] = D.u[1][s]; }
+  m.ctl = h->d_ctl + r;
+  m.dom = D.dom;
+  memcpy(m.base, D.base, sizeof m.base);
+  for (int a = 0; a < 3; a++) m.n[a] = hr.nphys[a];
+  // device axis i holds physical axis perm[i]; device strides P, nz, 1
+  const long long dstr[3] = {(long long)D.P, (long long)D.nz, 1};
+  for (int i = 0; i < 3; i++) m.stride[hr.perm[i]] = dstr[i];
+  m.nvox = (long long)m.n[0] * m.n[1] * m.n[2];
+  return m;
+}
+
+static int ensure_stage(csp_handle* h, size_t bytes) {
+  if (bytes <= h->stage_bytes) return CSP_OK;
+  cudaFree(h->d_stage);
+  h->d_stage = nullptr;
+  h->stage_bytes = 0;
+  if (cudaMalloc(&h->d_stage, bytes) != cudaSuccess)
+    return fail(h, CSP_ENOMEM, "state staging buffer of %.1f MB", bytes / 1e6);
+  h->stage_bytes = bytes;
+  return CSP_OK;
+}
+
+static unsigned blocks_of(long long n) { return (unsigned)((n + 255) / 256); }
+
+// Realisations [r0, r1) from host arrays u[r] (a staging buffer reused in stream order),
+// one wait at the end.
+template <class T>
+static int upload_range(csp_handle* h, const T* const* u, int r0, int r1) {
+  size_t need = 0;
+  for (int r = r0; r < r1; r++) {
+    if (!u[r - r0]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
+    const StateMap m = make_state_map(h, r);
+    need = std::max(need, (size_t)(m.nvox * m.ns) * sizeof(T));
+  }
+  int rc = ensure_stage(h, need);
+  if (rc) return rc;
+  for (int r = r0; r < r1; r++) {
+    const StateMap m = make_state_map(h, r);
+    const long long n = m.nvox * m.ns;
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, u[r - r0], n * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+    k_state_in<T><<<blocks_of(n), 256, 0, h->stream>>>(static_cast<const T*>(h->d_stage), m);
+    CUDA_TRY(h, cudaGetLastError());
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+template <class T>
+static int download_range(csp_handle* h, T* const* u, int r0, int r1) {
+  size_t need = 0;
+  for (int r = r0; r < r1; r++) {
+    if (!u[r - r0]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
+    const StateMap m = make_state_map(h, r);
+    need = std::max(need, (size_t)(m.nvox * m.ns) * sizeof(T));
+  }
+  int rc = ensure_stage(h, need);
+  if (rc) return rc;
+  for (int r = r0; r < r1; r++) {
+    const StateMap m = make_state_map(h, r);
+    const long long n = m.nvox * m.ns;
+    k_state_out<T><<<blocks_of(n), 256, 0, h->stream>>>(static_cast<T*>(h->d_stage), m);
+    CUDA_TRY(h, cudaGetLastError());
+    CUDA_TRY(h, cudaMemcpyAsync(u[r - r0], h->d_stage, n * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return CSP_OK;
+}
+
+extern "C" int csp_upload_state(csp_handle* h, int32_t r, const double* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  return upload_range<double>(h, &u, r, r + 1);
+}
+
+extern "C" int csp_download_state(csp_handle* h, int32_t r, double* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
+  if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
+  return download_range<double>(h, &u, r, r + 1);
+}
+
+extern "C" int csp_upload_states(csp_handle* h, const double* const* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
+  return upload_range<double>(h, u, 0, h->n);
+}
+
+extern "C" int csp_download_states(csp_handle* h, double* const* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
+  return download_range<double>(h, u, 0, h->n);
+}
+
+extern "C" int csp_upload_states_f32(csp_handle* h, const float* const* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
+  return upload_range<float>(h, u, 0, h->n);
+}
+
+extern "C" int csp_download_states_f32(csp_handle* h, float* const* u) {
+  if (!h || !u) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
+  return download_range<float>(h, u, 0, h->n);
+}
+
+// csp_run_states: groups of consecutive realisations with about equal voxel counts.
+static std::vector<int> run_groups(const csp_handle* h) {
+  const int G = std::min(h->n, 8);
+  long long total = 0;
+  for (int r = 0; r < h->n; r++) total += h->real[r].desc.nx * (long long)h->real[r].desc.plane;
+  std::vector<int> b{0};
+  long long acc = 0;
+  for (int r = 0; r < h->n; r++) {
+    acc += h->real[r].desc.nx * (long long)h->real[r].desc.plane;
+    const int g = (int)b.size();
+    if (g < G && r + 1 < h->n && acc * G >= total * g) b.push_back(r + 1);
+  }
+  b.push_back(h->n);
+  return b;
+}
+
+// One ensemble job from host memory, pipelined by realisation groups on three streams:
+// the input copies of group g+1 (in_stream) and the output copies of group g-1
+// (snap_stream) overlap the steps of group g (the handle stream).  Each group has two
+// staging slots per direction; events order the reuse of a slot after its previous group.
+template <class T>
+static int run_states(csp_handle* h, const T* const* uin, int64_t nsteps, T* const* uout, int32_t* stop_flags,
+                      int32_t* step_flags) {
+  for (int r = 0; r < h->n; r++)
+    if (!uin[r] || !uout[r]) return fail(h, CSP_EINVAL, "NULL state of realisation %d", r);
+  const std::vector<int> gb = run_groups(h);
+  const int G = (int)gb.size() - 1;
+  std::vector<long long> off(h->n + 1, 0);      // element offset of realisation r in its group's slot
+  size_t slot = 0;
+  for (int g = 0; g < G; g++) {
+    long long o = 0;
+    for (int r = gb[g]; r < gb[g + 1]; r++) {
+      off[r] = o;
+      const StateMap m = make_state_map(h, r);
+      o += (m.nvox * m.ns + 63) / 64 * 64;       // 256-byte aligned starts
+    }
+    slot = std::max(slot, (size_t)o);
+  }
+  const size_t slot_bytes = slot * sizeof(T);
+  if (4 * slot_bytes > h->pipe_bytes) {
+    cudaFree(h->d_pipe);
+    h->d_pipe = nullptr;
+    h->pipe_bytes = 0;
+    if (cudaMalloc(&h->d_pipe, 4 * slot_bytes) != cudaSuccess)
+      return fail(h, CSP_ENOMEM, "pipeline staging of %.1f MB", 4.0 * slot_bytes / 1e6);
+    h->pipe_bytes = 4 * slot_bytes;
+  }
+  if (step_flags && (size_t)nsteps * h->n > h->stepflags_elems) {
+    cudaFree(h->d_stepflags);
+    h->d_stepflags = nullptr;
+    h->stepflags_elems = 0;
+    if (cudaMalloc(&h->d_stepflags, (size_t)nsteps * h->n * sizeof(int)) != cudaSuccess)
+      return fail(h, CSP_ENOMEM, "per-step flags of %lld steps", (long long)nsteps);
+    h->stepflags_elems = (size_t)nsteps * h->n;
+  }
+  if (!h->in_stream) CUDA_TRY(h, cudaStreamCreateWithFlags(&h->in_stream, cudaStreamNonBlocking));
+  if (!h->snap_stream) {
+    CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_snap, cudaEventDisableTiming));
+    CUDA_TRY(h, cudaEventCreateWithFlags(&h->ev_copy, cudaEventDisableTiming));
+  }
+  std::vector<cudaEvent_t> ev(2 * G + 4, nullptr);
+  for (auto& e : ev) CUDA_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t* in_ready = ev.data();
+  cudaEvent_t* out_ready = ev.data() + G;
+  cudaEvent_t* in_free = ev.data() + 2 * G;      // [2]
+  cudaEvent_t* out_free = ev.data() + 2 * G + 2; // [2]
+  T* pipe = static_cast<T*>(h->d_pipe);
+  cudaStream_t cs = h->stream, is = h->in_stream, os = h->snap_stream;
+  cudaError_t e = cudaEventRecord(h->ev0, cs);
+  for (int g = 0; g < G && e == cudaSuccess; g++) {
+    const int r0 = gb[g], r1 = gb[g + 1], k = g & 1;
+    T* in_slot = pipe + (size_t)k * slot;
+    T* out_slot = pipe + (size_t)(2 + k) * slot;
+    if (g >= 2) e = cudaStreamWaitEvent(is, in_free[k], 0);
+    for (int r = r0; r < r1 && e == cudaSuccess; r++) {
+      const StateMap m = make_state_map(h, r);
+      e = cudaMemcpyAsync(in_slot + off[r], uin[r], (size_t)(m.nvox * m.ns) * sizeof(T), cudaMemcpyHostToDevice, is);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(in_ready[g], is);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, in_ready[g], 0);
+    for (int r = r0; r < r1 && e == cudaSuccess; r++) {
+      const StateMap m = make_state_map(h, r);
+      k_state_in<T><<<blocks_of(m.nvox * m.ns), 256, 0, cs>>>(in_slot + off[r], m);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(in_free[k], cs);
+    for (int64_t st = 0; st < nsteps && e == cudaSuccess; st++)
+      e = launch_step(h, r0, r1, step_flags ? h->d_stepflags + st * h->n + r0 : nullptr);
+    if (e == cudaSuccess && g >= 2) e = cudaStreamWaitEvent(cs, out_free[k], 0);
+    for (int r = r0; r < r1 && e == cudaSuccess; r++) {
+      const StateMap m = make_state_map(h, r);
+      k_state_out<T><<<blocks_of(m.nvox * m.ns), 256, 0, cs>>>(out_slot + off[r], m);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(out_ready[g], cs);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(os, out_ready[g], 0);
+    for (int r = r0; r < r1 && e == cudaSuccess; r++) {
+      const StateMap m = make_state_map(h, r);
+      e = cudaMemcpyAsync(uout[r], out_slot + off[r], (size_t)(m.nvox * m.ns) * sizeof(T), cudaMemcpyDeviceToHost, os);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(out_free[k], os);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(h->ev1, cs);
+  // every queued operation ends before the events go and before an error returns
+  const cudaError_t e_in = cudaStreamSynchronize(is), e_out = cudaStreamSynchronize(os);
+  const cudaError_t e_c = cudaStreamSynchronize(cs);
+  for (auto& x : ev) cudaEventDestroy(x);
+  if (e == cudaSuccess) e = e_in != cudaSuccess ? e_in : (e_out != cudaSuccess ? e_out : e_c);
+  if (e != cudaSuccess) return fail(h, CSP_ECUDA, "csp_run_states: %s", cudaGetErrorString(e));
+  if (step_flags && nsteps > 0)
+    CUDA_TRY(h, cudaMemcpy(step_flags, h->d_stepflags, (size_t)nsteps * h->n * sizeof(int), cudaMemcpyDeviceToHost));
+  const int rc = finish_advance(h, stop_flags);
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  return rc;
+}
+
+extern "C" int csp_run_states(csp_handle* h, int32_t host_dtype, const void* const* u_in, int64_t nsteps,
+                              void* const* u_out, int32_t* stop_flags, int32_t* step_flags) {
+  if (!h || !u_in || !u_out || nsteps < 0) return fail(h, CSP_EINVAL, "bad argument");
+  CSP_NOT_PENDING(h);
+  if (h->snap_pending) return fail(h, CSP_EINVAL, "a snapshot is pending (csp_snapshot_wait)");
+  if (h->inject_wait) return fail(h, CSP_EINVAL, "the wait-timeout test hook is armed");
+  if (host_dtype == CSP_HOST_F32)
+    return run_states<float>(h, reinterpret_cast<const float* const*>(u_in), nsteps,
+                             reinterpret_cast<float* const*>(u_out), stop_flags, step_flags);
+  if (host_dtype == CSP_HOST_F64)
+    return run_states<double>(h, reinterpret_cast<const double* const*>(u_in), nsteps,
+                              reinterpret_cast<double* const*>(u_out), stop_flags, step_flags);
+  return fail(h, CSP_EINVAL, "host_dtype %d is neither CSP_HOST_F32 nor CSP_HOST_F64", host_dtype);
 }
 
 extern "C" int csp_snapshot_async(csp_handle* h, int32_t r, uint32_t species_mask) {
@@ -1239,9 +1525,7 @@ extern "C" int csp_snapshot_async(csp_handle* h, int32_t r, uint32_t species_mas
   if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
   if (h->advance_pending) return fail(h, CSP_EINVAL, "an asynchronous advance is pending (csp_advance_wait)");
   if (h->snap_pending) return fail(h, CSP_EINVAL, "a snapshot is pending (csp_snapshot_wait)");
-  StateMap m;
-  int rc = state_map(h, r, m);
-  if (rc) return rc;
+  const StateMap m = make_state_map(h, r);
   const size_t need = (size_t)m.nvox * m.ns;
   if (!h->snap_stream) {
     CUDA_TRY(h, cudaStreamCreateWithFlags(&h->snap_stream, cudaStreamNonBlocking));
@@ -1290,6 +1574,7 @@ extern "C" int csp_snapshot_wait(csp_handle* h, const double** u) {
 extern "C" int csp_get_channel_states(const csp_handle* hc, int32_t r, int32_t boundary, int32_t* states) {
   csp_handle* h = const_cast<csp_handle*>(hc);
   if (!h || !states) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
   const HostReal& hr = h->real[r];
   if (boundary < 0 || boundary >= (int)hr.boundary_channel_base.size() || hr.boundary_channel_base[boundary] < 0)
@@ -1308,6 +1593,7 @@ extern "C" int csp_get_channel_states(const csp_handle* hc, int32_t r, int32_t b
 
 extern "C" int csp_set_channel_states(csp_handle* h, int32_t r, int32_t boundary, const int32_t* states) {
   if (!h || !states) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
   const HostReal& hr = h->real[r];
   if (boundary < 0 || boundary >= (int)hr.boundary_channel_base.size() || hr.boundary_channel_base[boundary] < 0)
@@ -1337,6 +1623,7 @@ extern "C" int csp_set_channel_states(csp_handle* h, int32_t r, int32_t boundary
 struct LinescanMap {
   const float* f;
   const unsigned char* dom;
+  double base[ND];           // the species' field base per domain
   int nd[3];                 // device extents (n0, n1, n2)
   int P;
   int phys_of_dev[3];        // physical axis of each device axis
@@ -1362,7 +1649,7 @@ __global__ void k_linescan_bins(LinescanMap m, double* __restrict__ bins) {
     if (m.num_domains > 0 && dom >= m.num_domains) continue;
     int pc[3];
     pc[m.phys_of_dev[0]] = c0; pc[m.phys_of_dev[1]] = c1; pc[m.phys_of_dev[2]] = c2;
-    double w = (double)m.f[dv];
+    double w = (double)m.f[dv] + m.base[dom];
     for (int a = 0; a < 3; a++)
       if (a != m.axis) w *= m.w[a][pc[a]];
     atomicAdd(&sb[pc[m.axis]], w);
@@ -1379,6 +1666,7 @@ static double gauss_weight(double x, double sigma) {   // utils.c:209-213
 extern "C" int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t axis, const double* offsets_nm,
                             const double* conv, int32_t num_domains, double* out) {
   if (!h || !offsets_nm || !conv || !out) return fail(h, CSP_EINVAL, "NULL argument");
+  CSP_NOT_PENDING(h);
   if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
   const HostReal& hr = h->real[r];
   const RealDesc& D = hr.desc;
@@ -1407,6 +1695,7 @@ extern "C" int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t a
   LinescanMap m;
   m.f = D.u[(cur >> species) & 1u][species];
   m.dom = D.dom;
+  for (int dd = 0; dd < ND; dd++) m.base[dd] = D.base[dd][species];
   m.nd[0] = D.nx; m.nd[1] = D.ny; m.nd[2] = D.nz;
   m.P = D.P;
   for (int i = 0; i < 3; i++) m.phys_of_dev[i] = hr.perm[i];
@@ -1436,6 +1725,7 @@ extern "C" int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t a
 extern "C" int csp_reduce_outputs(csp_handle* h, int32_t r, double* min_values, double* max_values,
                                   double* total_values, int32_t* openness) {
   if (!h) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   if (r < 0 || r >= h->n) return fail(h, CSP_ERANGE, "realisation %d out of range", r);
   const HostReal& hr = h->real[r];
   const RealDesc& D = hr.desc;
@@ -1489,6 +1779,29 @@ extern "C" int csp_set_device(int32_t device) {
   return CSP_OK;
 }
 
+extern "C" int csp_set_phase_timing(csp_handle* h, int32_t on) {
+  if (!h) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
+  if (on && !h->phase_ev[0])
+    for (auto& e : h->phase_ev) CUDA_TRY(h, cudaEventCreate(&e));
+  h->phase_timing = on ? 1 : 0;
+  return CSP_OK;
+}
+
+extern "C" int csp_get_phase_times(const csp_handle* h, double* ms, int64_t* steps) {
+  if (!h || !ms) return CSP_EINVAL;
+  for (int p = 0; p < CSP_NUM_PHASES; p++) ms[p] = h->phase_ms[p];
+  if (steps) *steps = h->phase_steps;
+  return CSP_OK;
+}
+
+extern "C" int csp_test_wait_timeout(csp_handle* h, int32_t on) {
+  if (!h) return CSP_EINVAL;
+  if (on && (h->kernel != 0 || !h->plan.ok)) return fail(h, CSP_EINVAL, "the staged voxel kernel is not in use");
+  h->inject_wait = on ? 1 : 0;
+  return CSP_OK;
+}
+
 extern "C" int csp_set_kernel(csp_handle* h, int32_t which) {
   if (!h || which < 0 || which > 1) return CSP_EINVAL;
   if (which == 0 && !h->plan.ok) return fail(h, CSP_ENOTSUP, "staged kernel unavailable for this batch");
@@ -1504,6 +1817,7 @@ extern "C" int csp_set_kernel(csp_handle* h, int32_t which) {
 // equal fields.  The fastest plan replaces the current one.
 extern "C" int csp_autotune(csp_handle* h, int32_t repeats, csp_tune_report* rep) {
   if (!h) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   if (repeats < 1) repeats = 3;
   std::vector<RealDesc> descs(h->n);
   for (int r = 0; r < h->n; r++) descs[r] = h->real[r].desc;
@@ -1828,6 +2142,8 @@ extern "C" void csp_destroy(csp_handle* h) {
   cudaFree(h->d_rows); cudaFree(h->d_entries); cudaFree(h->d_pairs); cudaFree(h->d_params);
   cudaFree(h->d_states); cudaFree(h->d_err); cudaFree(h->d_red); cudaFree(h->d_red_out);
   cudaFree(h->d_stage);
+  if (h->in_stream) { cudaStreamSynchronize(h->in_stream); cudaStreamDestroy(h->in_stream); }
+  cudaFree(h->d_pipe); cudaFree(h->d_stepflags);
   if (h->snap_stream) cudaStreamSynchronize(h->snap_stream);
   cudaFree(h->d_snap);
   cudaFreeHost(h->h_snap);
@@ -1835,6 +2151,8 @@ extern "C" void csp_destroy(csp_handle* h) {
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
   cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt);
+  for (auto& e : h->phase_ev)
+    if (e) cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -12,8 +12,13 @@
 // stores.  The per-voxel arithmetic is voxel_update (csp_kernels.cuh), shared with the
 // direct kernel, so both kernels give bitwise equal fields.
 //
-// Every mbarrier wait is bounded: after WAIT_LIMIT polls the kernel sets ERR_TIMEOUT in
-// the device error word and leaves the unit.
+// Every mbarrier wait is bounded in time (WAIT_NS).  A thread that gives up sets its own
+// flag; the CTA takes one decision from all flags at the end-of-plane barrier
+// (__syncthreads_or), so every thread leaves the x loop together.  Before the CTA exits,
+// its issuing thread waits (bounded again) for every stage whose bulk copies it has not
+// seen land, so no copy still writes this CTA's shared memory; then ERR_TIMEOUT is set in
+// the device error word and the kernel returns.  The fields of a launch that timed out
+// are undefined (the host reports CSP_EDEVICE).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -25,7 +30,8 @@
 namespace csp {
 
 constexpr int NST = 4;                    // ring stages: planes x-1, x, x+1 resident, 1 in flight
-constexpr long long WAIT_LIMIT = 1ll << 26;
+constexpr unsigned long long WAIT_NS = 1000000000ull;       // 1 s per mbarrier wait
+constexpr unsigned long long INJECT_WAIT_NS = 1000000ull;   // 1 ms for the test hook's wait
 
 struct StagedGeom {
   int L;            // positions per chunk (4*T)
@@ -40,14 +46,19 @@ struct StagedGeom {
   int seg;          // x planes per unit
 };
 
+struct StagedPlan;
+using StagedLaunchFn = cudaError_t (*)(const StagedPlan&, int, int, const RealDesc*, RealCtl*, int*, cudaStream_t);
+
 struct StagedPlan {
   bool ok = false;
   int T = 256;
-  int ctas = 0;
+  int slots = 0;                // resident CTAs of the whole GPU (persistent grid size)
   StagedGeom g{};
-  int4* d_units = nullptr;      // (r, c, x0, x1)
+  int4* d_units = nullptr;      // (r, c, x0, x1), realisation-major
   int nunits = 0;
-  cudaError_t (*launch)(const StagedPlan&, const RealDesc*, RealCtl*, int*, cudaStream_t) = nullptr;
+  std::vector<int> unit_first;  // [n+1]: the units of realisation r are [unit_first[r], unit_first[r+1])
+  StagedLaunchFn launch = nullptr;
+  StagedLaunchFn launch_inject = nullptr;
 };
 
 // ---- PTX helpers (sm_90+ bulk copy / mbarrier) ----
@@ -66,6 +77,19 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
       "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
   return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// true once phase `parity` of the barrier has completed; false after limit_ns
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity, unsigned long long limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
 }
 __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
@@ -118,7 +142,9 @@ __device__ __forceinline__ unsigned ld_u32_any(const unsigned char* p) {
   return __funnelshift_r(w[0], w[1], 8u * (unsigned)(a & 3));
 }
 
-template <int MS, int T>
+// INJ = true builds the test hook's variant (csp_test_wait_timeout); the kernel in use is
+// INJ = false, which has none of that code.
+template <int MS, int T, bool INJ = false>
 __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                         const int4* __restrict__ units, StagedGeom g,
                                                         int* __restrict__ err) {
@@ -131,7 +157,8 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
   unsigned phase = 0;    // bit st = parity of the next completion of stage st (CTA-uniform)
 
   if (tid == 0) {
-    for (int i = 0; i < NST; i++) mbar_init(smem_u32(&bars[i]), 1);
+    // bars[NST] is the test hook's barrier: initialised, never arrived on
+    for (int i = 0; i <= NST; i++) mbar_init(smem_u32(&bars[i]), 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -183,23 +210,30 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
     // class bytes of this chunk (one per plane), when the chunk matches the class table's
     const unsigned char* cls_row = (g.L == CLASS_L && D.cls) ? D.cls + c : nullptr;
 
+    unsigned pending = 0;  // issuing thread: stages whose copies it has not yet seen land
     if (tid == 0) {
       fence_proxy_async();
       for (int q = ql; q <= min(qh, ql + NST - 1); q++) {
         const int st = (q - ql) % NST;
         issue_plane(D, cur, lmask, q, st, ring, g, smem_u32(&bars[st]), lo, hi, lob, hib);
+        pending |= 1u << st;
       }
     }
-    bool timeout = false;
+    bool timeout = false;   // this thread gave up on a wait (the CTA decides at the next barrier)
+    // test hook (INJ only): one thread that issues no copies waits on a barrier that nothing
+    // completes, so the timeout path below runs with the threads of the CTA disagreeing
+    if (INJ && blockIdx.x == 0 && u == (int)blockIdx.x && tid == 37)
+      timeout = !mbar_wait_bounded(smem_u32(&bars[NST]), 0u, INJECT_WAIT_NS);
     auto wait_plane = [&](int q) {
       const int st = (q - ql) % NST;
-      const unsigned par = (phase >> st) & 1u;
-      long long n = 0;
-      while (!mbar_try_wait(smem_u32(&bars[st]), par)) {
-        if (++n > WAIT_LIMIT) { timeout = true; break; }
+      if (mbar_wait_bounded(smem_u32(&bars[st]), (phase >> st) & 1u, WAIT_NS)) {
+        phase ^= 1u << st;
+        pending &= ~(1u << st);
+      } else {
+        timeout = true;     // phase kept: the drain below waits on the same completion
       }
-      phase ^= 1u << st;
     };
+    bool cta_timeout = false;
     auto stage_of = [&](int q) -> const unsigned char* { return ring + (size_t)((q - ql) % NST) * g.stage_bytes; };
     const int so = g.slot;
     const size_t dom_off = (size_t)g.ms * g.slot * 4;
@@ -210,7 +244,6 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
     for (int x = x0; x < x1; x++) {
       const bool has_prev = x > 0, has_next = x + 1 < nx;
       if (has_next) wait_plane(x + 1);
-      if (timeout) break;
       const unsigned char* sc = stage_of(x);
       const unsigned char* sp = has_prev ? stage_of(x - 1) : sc;
       const unsigned char* sn = has_next ? stage_of(x + 1) : sc;
@@ -324,14 +357,18 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
         }
         float out[MS][4];
         if (si.react && si.react_fast) {
-          const F2 ca0 = f2(val[0][0], val[0][1]), ca1 = f2(val[0][2], val[0][3]);
+          // deviations of Ca, and Ca itself (its base plus the deviation)
+          const F2 dca0 = f2(val[0][0], val[0][1]), dca1 = f2(val[0][2], val[0][3]);
+          const float cb = D.fbase[d0][0];
+          const F2 ca0 = f2_add(f2(cb, cb), dca0), ca1 = f2_add(f2(cb, cb), dca1);
+          const unsigned rm = D.rmask[d0];
 #pragma unroll
           for (int s = 1; s < MS; s++) {
+            if (!(rm >> s & 1u)) continue;
             const float4 kk = D.rk[d0][s];
-            if (kk.w == 0.f) continue;
-            const F2 kon = f2(kk.x, kk.x), nkoff = f2(-kk.y, -kk.y), tot = f2(kk.z, kk.z);
-            const F2 dj0 = buffer_dj2(kon, nkoff, tot, f2(val[s][0], val[s][1]), ca0);
-            const F2 dj1 = buffer_dj2(kon, nkoff, tot, f2(val[s][2], val[s][3]), ca1);
+            const F2 nkon = f2(kk.x, kk.x), nkoff = f2(kk.y, kk.y), a = f2(kk.z, kk.z), j0 = f2(kk.w, kk.w);
+            const F2 dj0 = buffer_dj2(nkon, nkoff, a, j0, f2(val[s][0], val[s][1]), dca0, ca0);
+            const F2 dj1 = buffer_dj2(nkon, nkoff, a, j0, f2(val[s][2], val[s][3]), dca1, ca1);
             o2[s][0] = f2_add(o2[s][0], dj0);
             o2[s][1] = f2_add(o2[s][1], dj1);
             o2[0][0] = f2_sub(o2[0][0], dj0);
@@ -360,14 +397,14 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
 #pragma unroll
         for (int s = 0; s < MS; s++)
           if (fm >> s & 1u) {
-            const float iv = D.init[d0][s];
+            const float iv = D.dinit[d0][s];
 #pragma unroll
             for (int j = 0; j < 4; j++) out[s][j] = iv;
           }
         if (D.dirichlet) {
 #pragma unroll
           for (int j = 0; j < 4; j++)
-            if ((vzy[j] | xval) != 63u) out[0][j] = D.init[d0][0];
+            if ((vzy[j] | xval) != 63u) out[0][j] = D.dinit[d0][0];
         }
         // ---- stores (128-bit) ----
 #pragma unroll
@@ -500,7 +537,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
                 if (!code) continue;
                 const int fs = (code & 0x7f) - 1;
                 if (D.fslot_species[fs] != s) continue;
-                const double self = (double)u, other = (double)unb[k];
+                const double self = (double)u + D.base[dj[j]][s], other = (double)unb[k] + D.base[dnb[j][k]][s];
                 if (code & 0x80) acc += pair_flux(D, fs, other, self);
                 else acc -= pair_flux(D, fs, self, other);
                 any = true;
@@ -522,14 +559,17 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             o2[s][0] = f2(out[s][0], out[s][1]);
             o2[s][1] = f2(out[s][2], out[s][3]);
           }
-          const F2 ca0 = f2(val[0][0], val[0][1]), ca1 = f2(val[0][2], val[0][3]);
+          const F2 dca0 = f2(val[0][0], val[0][1]), dca1 = f2(val[0][2], val[0][3]);
+          const float cb = D.fbase[d][0];
+          const F2 ca0 = f2_add(f2(cb, cb), dca0), ca1 = f2_add(f2(cb, cb), dca1);
+          const unsigned rm = D.rmask[d];
 #pragma unroll
           for (int s = 1; s < MS; s++) {
+            if (!(rm >> s & 1u)) continue;
             const float4 kk = D.rk[d][s];
-            if (kk.w == 0.f) continue;
-            const F2 kon = f2(kk.x, kk.x), nkoff = f2(-kk.y, -kk.y), tot = f2(kk.z, kk.z);
-            const F2 dj0 = buffer_dj2(kon, nkoff, tot, f2(val[s][0], val[s][1]), ca0);
-            const F2 dj1 = buffer_dj2(kon, nkoff, tot, f2(val[s][2], val[s][3]), ca1);
+            const F2 nkon = f2(kk.x, kk.x), nkoff = f2(kk.y, kk.y), a = f2(kk.z, kk.z), j0 = f2(kk.w, kk.w);
+            const F2 dj0 = buffer_dj2(nkon, nkoff, a, j0, f2(val[s][0], val[s][1]), dca0, ca0);
+            const F2 dj1 = buffer_dj2(nkon, nkoff, a, j0, f2(val[s][2], val[s][3]), dca1, ca1);
             o2[s][0] = f2_add(o2[s][0], dj0);
             o2[s][1] = f2_add(o2[s][1], dj1);
             o2[0][0] = f2_sub(o2[0][0], dj0);
@@ -546,11 +586,13 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           const int d = dj[j];
           if (si.react && !(si.react_fast && one_dom)) {
             if (si.react_fast) {
+              const float ca = __fadd_rn(D.fbase[d][0], val[0][j]);
+              const unsigned rm = D.rmask[d];
 #pragma unroll
               for (int s = 1; s < MS; s++) {
+                if (!(rm >> s & 1u)) continue;
                 const float4 kk = D.rk[d][s];
-                if (kk.w == 0.f) continue;
-                const float dJ = buffer_dj(kk.x, kk.y, kk.z, val[s][j], val[0][j]);
+                const float dJ = buffer_dj(kk.x, kk.y, kk.z, kk.w, val[s][j], val[0][j], ca);
                 out[s][j] = __fadd_rn(out[s][j], dJ);
                 out[0][j] = __fsub_rn(out[0][j], dJ);
               }
@@ -566,8 +608,8 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           const unsigned fm = D.fixed_mask[d];
 #pragma unroll
           for (int s = 0; s < MS; s++)
-            if (fm >> s & 1u) out[s][j] = D.init[d][s];
-          if (D.dirichlet && (vzy[j] | xval) != 63u) out[0][j] = D.init[d][0];
+            if (fm >> s & 1u) out[s][j] = D.dinit[d][s];
+          if (D.dirichlet && (vzy[j] | xval) != 63u) out[0][j] = D.dinit[d][0];
         }
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -606,35 +648,51 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             if (lmask >> s & 1u) D.u[((cur >> s) & 1u) ^ 1u][s][(long long)x * D.P + pj] = oj[s];
         }
       }
-      // plane x-1 is no longer needed: refill its stage with plane x-1+NST
-      __syncthreads();
+      // plane x-1 is no longer needed: refill its stage with plane x-1+NST.  The barrier
+      // also takes the CTA's one decision on the waits of this plane: if any thread gave
+      // up, every thread leaves the loop here (plane x's outputs are then undefined)
+      if (__syncthreads_or(timeout ? 1 : 0)) { cta_timeout = true; break; }
       if (tid == 0 && has_prev && x - 1 >= ql) {
         const int qn = x - 1 + NST;
         if (qn <= qh) {
           fence_proxy_async();
           const int st = (x - 1 - ql) % NST;
           issue_plane(D, cur, lmask, qn, st, ring, g, smem_u32(&bars[st]), lo, hi, lob, hib);
+          pending |= 1u << st;
         }
       }
     }
-    if (timeout) {
-      if (tid == 0) atomicOr(err, ERR_TIMEOUT);
+    if (cta_timeout) {
+      if (tid == 0) {
+        // no bulk copy may still be writing this CTA's shared memory when it exits
+        for (int st = 0; st < NST; st++)
+          if (pending >> st & 1u) mbar_wait_bounded(smem_u32(&bars[st]), (phase >> st) & 1u, WAIT_NS);
+        atomicOr(err, ERR_TIMEOUT);
+      }
       __syncthreads();
-      return;   // ring state is unknown: leave the kernel
+      return;
     }
     __syncthreads();
   }
 }
 
-template <int MS, int T>
-cudaError_t staged_launch_t(const StagedPlan& pl, const RealDesc* d, RealCtl* c, int* e, cudaStream_t s) {
-  k_voxels_staged<MS, T><<<pl.ctas, T, pl.g.smem, s>>>(d, c, pl.d_units, pl.g, e);
+// Launch over the work units [u0, u1) (all units: one step of every realisation; the units
+// of a range of realisations: one step of those only).
+template <int MS, int T, bool INJ>
+cudaError_t staged_launch_t(const StagedPlan& pl, int u0, int u1, const RealDesc* d, RealCtl* c, int* e,
+                            cudaStream_t s) {
+  if (u1 <= u0) return cudaSuccess;
+  StagedGeom g = pl.g;
+  g.nunits = u1 - u0;
+  k_voxels_staged<MS, T, INJ><<<std::min(g.nunits, pl.slots), T, g.smem, s>>>(d, c, pl.d_units + u0, g, e);
   return cudaGetLastError();
 }
 
 template <int MS, int T>
 cudaError_t staged_configure(StagedPlan& pl) {
   cudaError_t e = cudaFuncSetAttribute(k_voxels_staged<MS, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.g.smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_voxels_staged<MS, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.g.smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_voxels_staged<MS, T>, T, pl.g.smem);
@@ -643,8 +701,9 @@ cudaError_t staged_configure(StagedPlan& pl) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  pl.ctas = std::min(pl.nunits, per_sm * sms);
-  pl.launch = &staged_launch_t<MS, T>;
+  pl.slots = per_sm * sms;
+  pl.launch = &staged_launch_t<MS, T, false>;
+  pl.launch_inject = &staged_launch_t<MS, T, true>;
   return cudaSuccess;
 }
 
@@ -674,12 +733,15 @@ inline StagedPlan staged_plan(const std::vector<RealDesc>& descs, int T = 256, i
   }
   g.seg = seg;
   std::vector<int4> units;
+  pl.unit_first.assign(descs.size() + 1, 0);
   for (int r = 0; r < (int)descs.size(); r++) {
     const RealDesc& D = descs[r];
     const int nch = (D.plane + g.L - 1) / g.L;
+    pl.unit_first[r] = (int)units.size();
     for (int x0 = 0; x0 < D.nx; x0 += seg)
       for (int c = 0; c < nch; c++) units.push_back(make_int4(r, c, x0, std::min(D.nx, x0 + seg)));
   }
+  pl.unit_first[descs.size()] = (int)units.size();
   pl.nunits = (int)units.size();
   g.nunits = pl.nunits;
   if (cudaMalloc(&pl.d_units, units.size() * sizeof(int4)) != cudaSuccess) return pl;
@@ -697,8 +759,11 @@ inline cudaError_t staged_prepare(StagedPlan& pl) {
   return e;
 }
 
-inline void staged_launch(const StagedPlan& pl, const RealDesc* d, RealCtl* c, int* e, cudaStream_t s) {
-  pl.launch(pl, d, c, e, s);
+// One step of the realisations [r0, r1) (default: all).
+inline void staged_launch(const StagedPlan& pl, const RealDesc* d, RealCtl* c, int* e, cudaStream_t s,
+                          bool inject = false, int r0 = 0, int r1 = -1) {
+  if (r1 < 0) r1 = (int)pl.unit_first.size() - 1;
+  (inject ? pl.launch_inject : pl.launch)(pl, pl.unit_first[r0], pl.unit_first[r1], d, c, e, s);
 }
 
 inline void staged_release(StagedPlan& pl) {

@@ -194,12 +194,11 @@ def config2(seed=2):
     return spec, opts
 
 
-def config3(n=256, seed=3, shape=(100, 100, 50)):
-    """Batched ensemble: n realisations of 100x100x50, 16-100 RyRs, pRyR 0-50 %,
-    compact / elongated / fragmented clusters drawn from the seed, abort 1.5 ms after
-    all channels close."""
+def config3_draws(n=256, seed=3, shape=(100, 100, 50)):
+    """The random draws of config3 for every realisation (cheap: no geometry is built):
+    cluster channel positions, pRyR mask and options, in the order config3 draws them."""
     rng = np.random.default_rng(seed)
-    specs, opts = [], []
+    out = []
     for r in range(n):
         nch = int(rng.integers(16, 101))
         kind = ["compact", "elongated", "fragmented"][int(rng.integers(0, 3))]
@@ -210,28 +209,45 @@ def config3(n=256, seed=3, shape=(100, 100, 50)):
         pfrac = rng.uniform(0.0, 0.5)
         pmask = rng.random(len(pts)) < pfrac
         pmask[0] = False                  # channel 0 of "ryr" is the forced-open trigger
-        spec = spark_model(shape, channels=pts, pryr_mask=pmask, serca=True)
-        specs.append(spec)
-        opts.append(dict(h=6.0, tstop=10.0, seed=seed * 1000003 + r, tabort=1.5,
-                         open_states={"ryr": [0]}))
-    return specs, opts
+        out.append(dict(shape=shape, h=6.0, channels=pts, pryr_mask=pmask,
+                        opts=dict(h=6.0, tstop=10.0, seed=seed * 1000003 + r, tabort=1.5, open_states={"ryr": [0]})))
+    return out
 
 
-def config4(n=64, seed=4):
-    """Uneven ensemble: grids from 64^3 to 256x256x128 at h = 6-10 nm, -T 5*dt."""
+def config3(n=256, seed=3, shape=(100, 100, 50), only=None):
+    """Batched ensemble: n realisations of 100x100x50, 16-100 RyRs, pRyR 0-50 %,
+    compact / elongated / fragmented clusters drawn from the seed, abort 1.5 ms after
+    all channels close.  only: build just these realisation indices (the draws of all n
+    are still taken, so realisation i is the same whichever others are built)."""
+    draws = config3_draws(n, seed, shape)
+    idx = range(n) if only is None else only
+    specs = [spark_model(shape, channels=draws[i]["channels"], pryr_mask=draws[i]["pryr_mask"], serca=True)
+             for i in idx]
+    return specs, [dict(draws[i]["opts"]) for i in idx]
+
+
+def config4_draws(n=64, seed=4):
+    """The random draws of config4 for every realisation (no geometry built): grid shape,
+    resolution h and options."""
     rng = np.random.default_rng(seed)
-    specs, opts = [], []
+    out = []
     for r in range(n):
         nx = int(rng.integers(64, 257)) // 2 * 2
         ny = int(rng.integers(64, 257)) // 2 * 2
         nz = int(rng.integers(64, 129)) // 2 * 2
         h = float(rng.uniform(6.0, 10.0))
-        spec = spark_model((nx, ny, nz), h=h, serca=True)
         dt = 0.95 * h * h / (6 * 220000.0)
-        specs.append(spec)
-        opts.append(dict(h=h, tstop=10.0, seed=seed * 1000003 + r, dt_update_react=5 * dt,
-                         open_states={"ryr": [0]}))
-    return specs, opts
+        out.append(dict(shape=(nx, ny, nz), h=h, opts=dict(h=h, tstop=10.0, seed=seed * 1000003 + r,
+                                                              dt_update_react=5 * dt, open_states={"ryr": [0]})))
+    return out
+
+
+def config4(n=64, seed=4, only=None):
+    """Uneven ensemble: grids from 64^3 to 256x256x128 at h = 6-10 nm, -T 5*dt."""
+    draws = config4_draws(n, seed)
+    idx = range(n) if only is None else only
+    specs = [spark_model(draws[i]["shape"], h=draws[i]["h"], serca=True) for i in idx]
+    return specs, [dict(draws[i]["opts"]) for i in idx]
 
 
 def tiny(shape=(12, 12, 16), serca=True, pryr=True, **kw):

@@ -142,6 +142,12 @@ typedef struct csp_options {
   csp_open_list open[CSP_MAX_BOUNDARIES];
   int32_t num_t_close;
   csp_t_close t_close[CSP_MAX_BOUNDARIES];
+  /* Philox stream of the realisation's channel draws = its index in the csp_create batch +
+   * stream_offset (0: the batch index).  A realisation run in another batch (a shard of an
+   * ensemble on another GPU) draws the same channel trajectory when the offsets make the
+   * stream its index in the whole ensemble.  No counterpart in the reference: one MT19937
+   * stream per run, seeded by -S (calcium_sparks.c:113-116). */
+  int64_t stream_offset;
 } csp_options;
 
 /* Fills `o` with the reference defaults (options.c:502-542). */
@@ -197,6 +203,27 @@ int csp_download_state(csp_handle* h, int32_t r, double* u);
 int csp_upload_states(csp_handle* h, const double* const* u);
 int csp_download_states(csp_handle* h, double* const* u);
 
+/* The same transfers with FP32 host fields (the device precision: the values are those of
+ * the FP64 calls, with half the bytes over PCIe).  u[r]: float [num_species][nx][ny][nz]. */
+int csp_upload_states_f32(csp_handle* h, const float* const* u);
+int csp_download_states_f32(csp_handle* h, float* const* u);
+
+/* One ensemble job from host memory: every realisation's state uploaded from u_in[r],
+ * advanced by nsteps steps, downloaded into u_out[r] (u_out may alias u_in), in the layout
+ * of csp_upload_states with host_dtype CSP_HOST_F64 or of csp_upload_states_f32 with
+ * CSP_HOST_F32.  The fields equal those of upload + csp_advance(nsteps) + download: the
+ * realisations are independent, so the call advances them in groups of consecutive
+ * realisations (about equal voxels, at most 8 groups) and pipelines the groups on three
+ * streams -- the input copies of group g+1 and the output copies of group g-1 overlap the
+ * steps of group g.  Use page-locked host memory for the copies to overlap.  stop_flags
+ * (nullable, n entries) as csp_advance; step_flags (nullable, [nsteps][n]) receives every
+ * realisation's stop flag after every step.  (The reference has no ensemble: its host
+ * loop, calcium_sparks.c:190-228, advances one domain held in Species_t::u1,
+ * species.h:52.) */
+enum { CSP_HOST_F64 = 0, CSP_HOST_F32 = 1 };
+int csp_run_states(csp_handle* h, int32_t host_dtype, const void* const* u_in, int64_t nsteps, void* const* u_out,
+                   int32_t* stop_flags, int32_t* step_flags);
+
 /* Advance every still-running realisation by up to nsteps steps: diffusion, channel
  * gating, boundary fluxes, reactions, apply and fixed values, in the order of the
  * reference loop body calcium_sparks.c:190-228 (Species_step_diffusion species.c:1501,
@@ -250,6 +277,34 @@ int csp_last_advance_ms(const csp_handle* h, float* ms);
  * events around each launch (no graph); voxel_ms / boundary_ms receive the summed device
  * times of the voxel kernel and of the boundary / gating kernel. */
 int csp_profile_advance(csp_handle* h, int64_t nsteps, float* voxel_ms, float* boundary_ms);
+
+/* Per-phase device times of the step (the counterpart of the reference's -v timing buckets
+ * Diffusion stencil / Boundary fluxes / Stochastic evaluation / Reaction stencil,
+ * utils.c:11-75).  The step's kernels fuse several of the reference's phases, so a phase
+ * here is one kernel family: CSP_PHASE_VOXELS = diffusion of every species with the buffer
+ * reactions and fixed values (species.c:1501-1702), CSP_PHASE_DENSITY = density-boundary
+ * (SERCA) fluxes, CSP_PHASE_CHANNELS = RyR/pRyR gating with the channel fluxes
+ * (species.c:1704-1957), CSP_PHASE_SURROGATE = the learned reaction increments,
+ * CSP_PHASE_EPILOGUE = step counter and abort rule.  While enabled, the first 16 steps of
+ * every csp_advance / csp_advance_async call run as direct launches with CUDA events
+ * between the kernels; their per-phase time, scaled to the call's steps, is accumulated
+ * (an estimate: the other steps replay the captured graph untimed).  ms[CSP_NUM_PHASES]
+ * receives the accumulated milliseconds, steps the steps they stand for. */
+enum { CSP_PHASE_VOXELS = 0, CSP_PHASE_DENSITY, CSP_PHASE_CHANNELS, CSP_PHASE_SURROGATE, CSP_PHASE_EPILOGUE,
+       CSP_NUM_PHASES };
+int csp_set_phase_timing(csp_handle* h, int32_t on);
+int csp_get_phase_times(const csp_handle* h, double* ms, int64_t* steps);
+
+/* Test hook for the failure path of the staged voxel kernel's bounded waits.  While armed
+ * (on != 0), every launch of the staged kernel makes one thread of its first CTA wait on an
+ * mbarrier that nothing completes, with a 1 ms limit; that CTA then leaves its x loop as
+ * one (the decision is taken at the end-of-plane barrier), waits for its own bulk copies
+ * in flight, sets the timeout bit of the device error word and returns, and csp_advance
+ * returns CSP_EDEVICE with csp_status naming the timeout.  The handle's fields are
+ * undefined afterwards and the error stays set; the device and other handles stay usable.
+ * No counterpart in the reference: it has no device and aborts on any error
+ * (fvm_mpi/src/utils.h:21-27). */
+int csp_test_wait_timeout(csp_handle* h, int32_t on);
 
 /* Select the voxel kernel: 0 = staged (TMA bulk copies into shared memory, default),
  * 1 = direct (one thread per voxel, global loads).  Both give bitwise equal results. */
@@ -342,8 +397,10 @@ void csp_destroy(csp_handle* h);
  * array out[3][num_domains] (min, max, total), on `stream` (NULL = default stream).
  * It allocates nothing: block partials live in a file-scope device array of
  * CSP_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.
- *  - the first call on a device looks the array's address up (cudaGetSymbolAddress);
- *    make that first call before any stream capture;
+ *  - the first call on a device looks the array's address up (cudaGetSymbolAddress) and
+ *    keeps it for the life of the process; make that first call before any stream
+ *    capture; after a cudaDeviceReset of that device the call is not supported (the
+ *    array may move when the module is loaded again);
  *  - all calls share the array: calls that overlap on the GPU race; each call overwrites
  *    every partial it reads, so no clearing is needed;
  *  - num_domains above CSP_NOALLOC_MAX_DOMAINS or n above CSP_NOALLOC_MAX_VOXELS return

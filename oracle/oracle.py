@@ -56,7 +56,9 @@ class Oracle:
         self.m, k1 = abi.make_model(spec)
         self.o, k2 = abi.make_options(**options)
         self._keep = (k1, k2)
-        self.h = self.lib.oracle_create(C.byref(self.m), C.byref(self.o), realisation)
+        # the Philox stream of the GPU path: batch index + stream_offset
+        self.h = self.lib.oracle_create(C.byref(self.m), C.byref(self.o),
+                                        realisation + int(options.get("stream_offset", 0)))
         if not self.h:
             raise RuntimeError("oracle_create failed")
         self.spec = spec

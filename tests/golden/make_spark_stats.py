@@ -6,7 +6,7 @@ and every other channel gated stochastically, and stores per realisation:
   amplitude -- max over the outputs (t > 0) of the cleft's average Ca (uM);
   duration  -- time (ms) of the last output with a channel open;
   open      -- open channels at every output t > 0 (pooled by the test).
-Writes tests/golden/spark_stats_ref.npz.  Needs /root/reference (oracle/_ref built from it);
+Writes tests/golden/spark_stats_ref.npz.  Needs oracle/_ref (built from the reference checkout);
 takes a few minutes on 8 cores:  python tests/golden/make_spark_stats.py [N]
 """
 import multiprocessing as mp

@@ -149,3 +149,26 @@ def test_cli_abort_rule_matches_reference(synth, tmp_path):
     ours, ref = compare_outputs(str(ours_dir / "case.h5"), str(ref_dir / "case.h5"), spec)
     total = round(0.05 / (0.95 * 36 / (6 * 220000.0)))
     assert ref[-1]["time_index"] < total * 0.5, "the reference run did not abort"
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="CLI not built")
+@pytest.mark.gpu
+def test_cli_verbose_timing_buckets(synth, tmp_path):
+    """-v: the reference's timing table (utils.c:11-75) with the step's buckets filled from
+    the library's per-phase device times: every step counted in Diffusion stencil,
+    Boundary fluxes and Stochastic evaluation, their times within the main loop's."""
+    spec, g, s = model_files(synth, tmp_path)
+    args = ["-g", g, "-m", s, "-c", "case", "-h", "6", "-t", "0.004", "-o", "0.002", "-S", "3",
+            "-O", "ryr", "0", "-v"]
+    r = run(CLI, args, str(tmp_path))
+    assert r.returncode == 0, r.stderr[-2000:]
+    rows = {}
+    for ln in r.stdout.splitlines():
+        parts = ln.split("|")
+        if len(parts) == 5:
+            rows[parts[0].strip()] = (float(parts[1]), int(parts[4]))
+    steps = round(0.004 / (0.95 * 36 / (6 * 220000.0)))
+    for name in ("Diffusion stencil", "Boundary fluxes", "Stochastic evaluation", "Diffusion Total"):
+        assert abs(rows[name][1] - steps) <= 1, (name, rows[name], steps)
+    main = rows["Main Loop time"][0]
+    assert rows["Diffusion stencil"][0] + rows["Boundary fluxes"][0] + rows["Stochastic evaluation"][0] <= main + 0.1

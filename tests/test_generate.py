@@ -13,13 +13,14 @@ import numpy as np
 import pytest
 
 from oracle import refrun
+from oracle.refsrc import reference_file
 
 gen = importlib.import_module("hpc-ca-phospattern_b200.generate")
 h5m = importlib.import_module("hpc-ca-phospattern_b200.h5model")
-G1 = "/root/reference/createdgeometries/G1/G1_nonP_0.h5"
-MAP = "/root/reference/createdgeometries/G1/G1_inner_10.npy"
-PHOS = "/root/reference/parameters/phosphorylation/parameters_sr1100_ryr55_pryr25.h5"
-have_ref = os.path.exists(G1) and os.path.exists(MAP) and os.path.exists(PHOS)
+G1 = reference_file("createdgeometries", "G1", "G1_nonP_0.h5")
+MAP = reference_file("createdgeometries", "G1", "G1_inner_10.npy")
+PHOS = reference_file("parameters", "phosphorylation", "parameters_sr1100_ryr55_pryr25.h5")
+have_ref = bool(G1 and MAP and PHOS)
 
 
 @pytest.mark.skipif(not have_ref, reason="reference input files absent")

@@ -171,7 +171,9 @@ def test_state_roundtrip_and_channels(pkg, synth):
     rng = np.random.default_rng(0)
     v = u * (1 + 0.01 * rng.standard_normal(u.shape))
     sim.set_state(v)
-    np.testing.assert_array_equal(sim.state(), v.astype(np.float32).astype(np.float64))
+    # the device keeps each value as an FP32 deviation from its domain's base: one FP32
+    # rounding of the deviation, so within FP32 precision of the value
+    np.testing.assert_allclose(sim.state(), v, rtol=2.0 ** -22, atol=0)
     st = np.array([1, 0, 1, 1, 0, 0, 1], dtype=np.int32)
     sim.set_channels(0, st)
     np.testing.assert_array_equal(sim.channels(0), st)
@@ -369,4 +371,55 @@ def test_batched_state_transfers(pkg, synth):
     a.states_into(got)
     for r in range(2):
         np.testing.assert_array_equal(got[r], a.state(r))
-        np.testing.assert_array_equal(got[r], new[r].astype(np.float32).astype(np.float64))
+        np.testing.assert_allclose(got[r], new[r], rtol=2.0 ** -22, atol=0)
+
+
+def test_fp32_transfers_and_pipelined_run(pkg, synth):
+    """csp_upload_states_f32 / csp_download_states_f32 move the FP64 calls' values;
+    csp_run_states (upload, nsteps steps, download, pipelined by realisation groups) gives
+    bitwise the fields, channel states and step counts of upload + csp_advance + download,
+    with FP32 and FP64 host arrays, for more realisations than groups and uneven sizes; its
+    per-step stop flags show each realisation stopping at its own last step."""
+    shapes = [(12, 12, 16), (10, 14, 12), (14, 10, 12), (12, 12, 20), (10, 10, 16), (16, 12, 12), (12, 14, 14),
+              (10, 12, 18), (12, 10, 16), (14, 12, 10), (10, 16, 12)]
+    specs = [synth.tiny(s, pryr=(k % 3 != 1)) for k, s in enumerate(shapes)]
+    dt = 0.95 * 36 / (6 * 220000.0)
+    opts = [dict(h=6.0, tstop=(20 + 2 * k) * dt, seed=17, open_states={"ryr": [k % 7]}) for k in range(len(shapes))]
+    a = pkg.Simulation(specs, opts)
+    b = pkg.Simulation(specs, opts)
+    a.advance(5)
+    b.advance(5)
+    u64 = [a.state(r) for r in range(a.n)]
+    u32 = [np.ascontiguousarray(x.astype(np.float32)) for x in u64]
+    got = [np.empty_like(x) for x in u32]
+    a.set_states_f32(u32)
+    a.states_into_f32(got)
+    for r in range(a.n):
+        # an FP32 download is the FP64 download rounded; both within FP32 precision of the input
+        np.testing.assert_array_equal(got[r], a.state(r).astype(np.float32))
+        np.testing.assert_allclose(got[r], u32[r], rtol=2.0 ** -22, atol=0)
+    # reference sequence on a: FP64 upload, 40 steps, download
+    a.set_states(u64)
+    fa = a.advance(40)
+    ref = [a.state(r) for r in range(a.n)]
+    out = [np.zeros_like(x) for x in u64]
+    fb, sf = b.run_states(u64, 40, out, step_flags=True)
+    np.testing.assert_array_equal(fa, fb)
+    for r in range(a.n):
+        np.testing.assert_array_equal(out[r], ref[r])
+        assert b.info(r).step == a.info(r).step
+        np.testing.assert_array_equal(b.channels(0, r), a.channels(0, r))
+        last = b.info(r).total_steps
+        col = sf[:, r]
+        assert col[-1] == 1 and np.all(col[: last - 5 - 1] == 0) and np.all(col[last - 5 - 1:] == 1)
+    # FP32 host arrays, output aliasing input, against FP32 upload + csp_advance
+    c = pkg.Simulation(specs, opts)
+    d = pkg.Simulation(specs, opts)
+    c.advance(5)
+    d.advance(5)
+    d.set_states_f32(u32)
+    d.advance(40)
+    buf = [x.copy() for x in u32]
+    c.run_states(buf, 40, buf)
+    for r in range(c.n):
+        np.testing.assert_array_equal(buf[r], d.state(r).astype(np.float32))

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 from oracle import refrun
+from oracle.refsrc import reference_file
 
 BIN = refrun.ref_binary()
 pytestmark = pytest.mark.skipif(BIN is None, reason="oracle/_ref not built")
@@ -79,11 +80,11 @@ def test_pin_forced_dt_odd_sizes(synth, tmp_path):
     compare(spec, opts, tmp_path)
 
 
-G1 = "/root/reference/createdgeometries/G1/G1_nonP_0.h5"
-P55 = "/root/reference/parameters/nonP_blanket/parameters_sr1100_ryr55.h5"
+G1 = reference_file("createdgeometries", "G1", "G1_nonP_0.h5")
+P55 = reference_file("parameters", "nonP_blanket", "parameters_sr1100_ryr55.h5")
 
 
-@pytest.mark.skipif(not (os.path.exists(G1) and os.path.exists(P55)), reason="reference input files absent")
+@pytest.mark.skipif(not (G1 and P55), reason="reference input files absent")
 def test_pin_reference_g1_geometry(tmp_path):
     """The reference's own G1 geometry (84^3 at 12 nm) and parameter file."""
     import importlib
