@@ -157,15 +157,34 @@ class Simulation:
 
     # ---- learned reaction surrogate ----
     def mlp_train(self, params=None, r=0, samples=1_000_000, val_samples=65536, epochs=10, batch=16384, lr=1e-3,
-                  tol=1e-4, seed=1):
-        """Train the reaction surrogate on device (csp_mlp_train); returns (params, report dict)."""
+                  tol=1e-4, seed=1, harvested=False):
+        """Train the reaction surrogate on device (csp_mlp_train); returns (params, report dict).
+        harvested=True: on the pairs taken by mlp_harvest instead of sampled states."""
         p = mlp_init(seed) if params is None else np.array(params, dtype=np.float32)
         cfg = abi.csp_mlp_config(samples=samples, val_samples=val_samples, epochs=epochs, batch=batch, lr=lr,
-                                 tol=tol, seed=seed)
+                                 tol=tol, seed=seed, source=1 if harvested else 0)
         rep = abi.csp_mlp_report()
         self._check(self.lib.csp_mlp_train(self.h, r, C.byref(cfg), p.ctypes.data_as(C.POINTER(C.c_float)),
                                            C.byref(rep)))
         return p, {f: getattr(rep, f) for f, _ in abi.csp_mlp_report._fields_}
+
+    def mlp_harvest(self, n, seed=1, capacity=None):
+        """Take about n training pairs from the current fields (csp_mlp_harvest); returns
+        (taken, held)."""
+        taken, held = C.c_int64(), C.c_int64()
+        self._check(self.lib.csp_mlp_harvest(self.h, int(n), int(seed), int(capacity or n), C.byref(taken),
+                                             C.byref(held)))
+        return taken.value, held.value
+
+    def mlp_harvested(self, first=0, n=None):
+        """The held training pairs [first, first + n) as (x[n][8], t[n][5]) (csp_mlp_harvested)."""
+        if n is None:
+            n = self.mlp_harvest(0)[1] - first
+        x = np.zeros((n, abi.MLP_IN), dtype=np.float32)
+        t = np.zeros((n, abi.MLP_OUT), dtype=np.float32)
+        P = C.POINTER(C.c_float)
+        self._check(self.lib.csp_mlp_harvested(self.h, int(first), int(n), x.ctypes.data_as(P), t.ctypes.data_as(P)))
+        return x, t
 
     def set_surrogate(self, params, tol=1e-4):
         """Use the surrogate with these parameters on reaction steps (None: switch off)."""

@@ -14,6 +14,7 @@ MAX_BOUNDARIES = 8
 MAX_FIXED = 8
 NAME_LEN = 20
 HOST_F64, HOST_F32 = 0, 1    # csp_run_states host_dtype (CSP_HOST_F64, CSP_HOST_F32)
+TUNE_MAX = 10                # CSP_TUNE_MAX
 
 OK, EINVAL, ENOMEM, ECUDA, ERANGE, EDEVICE, ENOTSUP = 0, -1, -2, -3, -4, -5, -6
 DENSITY, DISCRETE = 0, 1
@@ -105,11 +106,12 @@ class csp_info(C.Structure):
 
 
 MLP_NPARAM = 5061
+MLP_IN, MLP_OUT = 8, 5
 
 
 class csp_mlp_config(C.Structure):
     _fields_ = [("samples", C.c_int64), ("val_samples", C.c_int64), ("epochs", C.c_int32), ("batch", C.c_int32),
-                ("lr", C.c_float), ("tol", C.c_double), ("seed", C.c_uint64)]
+                ("lr", C.c_float), ("tol", C.c_double), ("seed", C.c_uint64), ("source", C.c_int32)]
 
 
 class csp_mlp_report(C.Structure):
@@ -118,8 +120,8 @@ class csp_mlp_report(C.Structure):
 
 
 class csp_tune_report(C.Structure):
-    _fields_ = [("n", C.c_int32), ("threads", C.c_int32 * 8), ("segment", C.c_int32 * 8), ("ms", C.c_float * 8),
-                ("chosen", C.c_int32)]
+    _fields_ = [("n", C.c_int32), ("threads", C.c_int32 * TUNE_MAX), ("segment", C.c_int32 * TUNE_MAX),
+                ("ms", C.c_float * TUNE_MAX), ("chosen", C.c_int32)]
 
 
 def _name(s):
@@ -275,6 +277,8 @@ def declare(lib):
                                                C.c_void_p, C.c_void_p]),
         "csp_mlp_init": (None, [C.c_uint64, P(C.c_float)]),
         "csp_mlp_train": (C.c_int, [h, C.c_int32, P(csp_mlp_config), P(C.c_float), P(csp_mlp_report)]),
+        "csp_mlp_harvest": (C.c_int, [h, C.c_int64, C.c_uint64, C.c_int64, P(C.c_int64), P(C.c_int64)]),
+        "csp_mlp_harvested": (C.c_int, [h, C.c_int64, C.c_int64, P(C.c_float), P(C.c_float)]),
         "csp_mlp_gradient": (C.c_int, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64, P(C.c_float),
                                        P(C.c_float)]),
         "csp_mlp_forward": (C.c_int, [P(C.c_float), P(C.c_float), C.c_int64, C.c_int32, P(C.c_float)]),

@@ -10,6 +10,7 @@
 // species.c:1513).
 #pragma once
 #include <cstdint>
+#include <cstring>
 
 #include "../../include/csparks.h"
 
@@ -74,6 +75,14 @@ struct RealDesc {
   // ligand s1, a_dt = dt_r k_on (tot - base_s0), j0_dt = dt_r J(base_s0, base_s1)
   float a_dt[NB * ND], j0_dt[NB * ND];
   unsigned char rmask[ND];           // bit s: a buffer binds species s in domain d (fast reactions)
+  // Species that diffuse in no domain and only ever are the bound form of a buffer (TRPN
+  // in the reference model) hold a 32-bit integer q instead: value = base + q qunit[d][s],
+  // qunit a power of two with |q| < 2^30 over [0, 2 tot].  Such a buffer relaxes slowly;
+  // in FP32 its per-step increments would round away once below half an ulp of the
+  // deviation, stalling it short of equilibrium by about ulp / (2 rate dt) (0.02 uM for
+  // TRPN at the channel mouth); the integer adds every increment at 2^-30 of the total.
+  unsigned fixq;                     // bit s: species s is stored as q
+  float qunit[ND][NS], qinv[ND][NS];
   float* u[2][NS];                   // the two buffers of every species
   const unsigned char* dom;          // [nx][P]
   // Chunk class table [nx][ncls]: for plane x and chunk c (positions c*CLASS_L ...
@@ -181,6 +190,26 @@ __host__ __device__ inline void step_masks(const RealDesc& D, long long time_ind
   }
   updated = pre;
   if (D.nbuf > 0 && time_ind % D.reaction_substep == 0) updated |= D.reaction_flag_mask;
+}
+
+// Fixed-point fields (RealDesc::fixq): the stored bits are the integer q.
+__host__ __device__ inline int q_bits(float stored) {
+#ifdef __CUDA_ARCH__
+  return __float_as_int(stored);
+#else
+  int q;
+  memcpy(&q, &stored, sizeof q);
+  return q;
+#endif
+}
+__device__ __forceinline__ float q_value(float stored, float unit) {       // deviation q * unit
+  return __fmul_rn(__int2float_rn(__float_as_int(stored)), unit);
+}
+__device__ __forceinline__ float q_add(float stored, float inc, float inv) {   // q + round(inc / unit)
+  return __int_as_float(__float_as_int(stored) + __float2int_rn(__fmul_rn(inc, inv)));
+}
+__device__ __forceinline__ float q_set(float dev, float inv) {             // round(dev / unit)
+  return __int_as_float(__float2int_rn(__fmul_rn(dev, inv)));
 }
 
 // Register-array access with a run-time index, as a chain of selects (no local memory).

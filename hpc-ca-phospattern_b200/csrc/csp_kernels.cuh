@@ -100,9 +100,11 @@ __device__ __forceinline__ F2 buffer_dj2(F2 nkon, F2 nkoff, F2 a, F2 j0, F2 db, 
 
 // General buffer reactions: the reference's assign-or-accumulate rule, per buffer in
 // buffer order (species.c:1653-1702, kernel_generic.cpp:397-509).
+// fq: fixed-point species (RealDesc::fixq), whose out[] holds the increment (so the
+// assign form writes dJ, not b0 + dJ).
 template <int N>
 __device__ __forceinline__ void react_general(const RealDesc& D, int d, const float (&val)[N], float (&out)[N],
-                                              unsigned pre) {
+                                              unsigned pre, unsigned fq) {
   for (int bi = 0; bi < NB; bi++) {
     if (bi >= D.nbuf) break;
     const int t = bi * D.nd + d;
@@ -110,7 +112,8 @@ __device__ __forceinline__ void react_general(const RealDesc& D, int d, const fl
     const float b0 = sel(val, s0), b1 = sel(val, s1);     // deviations from the bases
     const float dJ = buffer_dj(-D.kon_dt[t], -D.koff_dt[t], D.a_dt[t], D.j0_dt[t], b0, b1,
                                __fadd_rn(D.fbase[d][s1], b1));
-    if (pre >> s0 & 1u) put(out, s0, __fadd_rn(sel(out, s0), dJ)); else put(out, s0, __fadd_rn(b0, dJ));
+    if (pre >> s0 & 1u) put(out, s0, __fadd_rn(sel(out, s0), dJ));
+    else put(out, s0, (fq >> s0 & 1u) ? dJ : __fadd_rn(b0, dJ));
     if (pre >> s1 & 1u) put(out, s1, __fsub_rn(sel(out, s1), dJ)); else put(out, s1, __fsub_rn(b1, dJ));
   }
 }
@@ -157,11 +160,13 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
   const int braw = ldd(6);
   const int d = braw & DOMAIN_BITS;
   const int pat = braw >> 3;
+  const unsigned fq = D.fixq & si.updated;        // fixed-point species: out[] holds the increment
   float val[N];
 #pragma unroll
   for (int s = 0; s < N; s++) {
-    val[s] = (si.updated >> s & 1u) ? ld(s, 6) : 0.f;
-    out[s] = val[s];
+    const float v = (si.updated >> s & 1u) ? ld(s, 6) : 0.f;
+    val[s] = (fq >> s & 1u) ? q_value(v, D.qunit[d][s]) : v;
+    out[s] = (fq >> s & 1u) ? 0.f : v;
   }
   if (si.pre) {
     int dn[6];
@@ -217,13 +222,15 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
         out[0] = __fsub_rn(out[0], dJ);
       }
     } else {
-      react_general<N>(D, d, val, out, si.pre);
+      react_general<N>(D, d, val, out, si.pre, fq);
     }
   }
   const unsigned fm = D.fixed_mask[d];
 #pragma unroll
   for (int s = 0; s < N; s++) {
     if (fm >> s & 1u) out[s] = D.dinit[d][s];
+    if (fq >> s & 1u)
+      out[s] = (fm >> s & 1u) ? q_set(out[s], D.qinv[d][s]) : q_add(ld(s, 6), out[s], D.qinv[d][s]);
   }
   if (D.dirichlet && on_face) out[0] = D.dinit[d][0];
 }
@@ -494,7 +501,7 @@ __global__ void __launch_bounds__(256) k_reduce_partial(const RealDesc* __restri
     const int x = (int)(v / D.plane);
     const long long idx = (long long)x * D.P + (v - (long long)x * D.plane);
     const int d = D.dom[idx] & DOMAIN_BITS;
-    const double val = (double)u[idx] + D.base[d][s];
+    const double val = ((D.fixq >> s & 1u) ? (double)q_bits(u[idx]) * D.qunit[d][s] : (double)u[idx]) + D.base[d][s];
 #pragma unroll
     for (int dd = 0; dd < ND; dd++) {
       if (dd == d) {

@@ -362,7 +362,8 @@ struct RxVoxel {
 // which the increments are added to.
 __device__ __forceinline__ void rx_fetch(const float* const* uo, const float* const* un,
                                          const unsigned char* __restrict__ dom, int plane, const RxConst* sk,
-                                         const float (*base)[NS], long long v, int p, long long nvox, RxVoxel& X) {
+                                         const float (*base)[NS], unsigned fixq, const float (*qunit)[NS], long long v,
+                                         int p, long long nvox, RxVoxel& X) {
   X.mine = false;
   X.d = 0;
   X.c = X.nc = 0.f;
@@ -381,8 +382,9 @@ __device__ __forceinline__ void rx_fetch(const float* const* uo, const float* co
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
     if (kc.tot[q] > 0.f) {
-      X.b[q] = __fadd_rn(base[X.d][q + 1], uo[q + 1][v]);
-      X.nb[q] = un[q + 1][v];
+      const float o = uo[q + 1][v];
+      X.b[q] = __fadd_rn(base[X.d][q + 1], (fixq >> (q + 1) & 1u) ? q_value(o, qunit[X.d][q + 1]) : o);
+      X.nb[q] = un[q + 1][v];     // stored form (an integer for fixed-point species)
     }
   }
 }
@@ -423,12 +425,13 @@ __device__ __forceinline__ void rx_fallback(const RxConst& kc, int n, double dt,
 // and, with Dirichlet faces (-f), Ca on the outer faces.
 // fm = the domain's fixed-species mask (RealDesc::fixed_mask).
 __device__ __forceinline__ void rx_store(unsigned fm, const float* const* un, const RxConst& kc, long long v,
-                                         bool face, float nc, const float* nb, float dc, const float* db) {
+                                         bool face, float nc, const float* nb, float dc, const float* db,
+                                         unsigned fixq, const float* qinv) {
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
     const int s = q + 1;
     if (kc.tot[q] <= 0.f || (fm >> s & 1u)) continue;
-    const_cast<float*>(un[s])[v] = __fadd_rn(nb[q], db[q]);
+    const_cast<float*>(un[s])[v] = (fixq >> s & 1u) ? q_add(nb[q], db[q], qinv[s]) : __fadd_rn(nb[q], db[q]);
   }
   if (!(fm & 1u) && !face) const_cast<float*>(un[0])[v] = __fadd_rn(nc, dc);
 }
@@ -454,6 +457,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   __shared__ float s_thr[ND][MLP_SLOTS];
   __shared__ unsigned s_fm[ND];
   __shared__ float s_base[ND][NS];
+  __shared__ float s_qunit[ND][NS], s_qinv[ND][NS];
   __shared__ const float* s_uo[NS];
   __shared__ const float* s_un[NS];
   __shared__ long long s_pend[MLP_DEPLOY_T / 32][64];   // per warp: queued voxels (up to two tiles)
@@ -474,7 +478,11 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     sk[threadIdx.x] = kc;
     for (int q = 0; q < MLP_SLOTS; q++) s_thr[threadIdx.x][q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
     s_fm[threadIdx.x] = D.fixed_mask[threadIdx.x < D.nd ? threadIdx.x : 0];
-    for (int s = 0; s < NS; s++) s_base[threadIdx.x][s] = D.fbase[threadIdx.x][s];
+    for (int s = 0; s < NS; s++) {
+      s_base[threadIdx.x][s] = D.fbase[threadIdx.x][s];
+      s_qunit[threadIdx.x][s] = D.qunit[threadIdx.x][s];
+      s_qinv[threadIdx.x][s] = D.qinv[threadIdx.x][s];
+    }
   }
   if (threadIdx.x < NS) {
     const int t = threadIdx.x;
@@ -487,6 +495,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
   const int plane = D.plane;
   const unsigned elig_mask = D.mlp_domains;
   const bool dirichlet = D.dirichlet != 0;
+  const unsigned fixq = D.fixq;
   unsigned n_vox = 0, n_net = 0, n_fall = 0;
   const long long v0 = (long long)blockIdx.x * span + threadIdx.x;
   // position within the plane and plane index of the voxel being fetched, advanced by
@@ -508,7 +517,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
       xq = (int)(v / P);
       pq = (int)(v - (long long)xq * P);
     }
-    rx_fetch(s_uo, s_un, dom, plane, sk, s_base, have ? v : nvox, pq, nvox, Y);
+    rx_fetch(s_uo, s_un, dom, plane, sk, s_base, fixq, s_qunit, have ? v : nvox, pq, nvox, Y);
     const RxConst& kc = sk[Y.d];
     float x[MLP_IN], t[MLP_OUT], db[MLP_SLOTS], dc = 0.f;
     if (have) rx_features(kc, Y.d, dtr, Y.c, Y.b, x);
@@ -522,12 +531,12 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
         n_fall++;
         rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
       }
-      rx_store(s_fm[Y.d], s_un, kc, v, dirichlet && rx_on_face(D, xq, pq), Y.nc, Y.nb, dc, db);
+      rx_store(s_fm[Y.d], s_un, kc, v, dirichlet && rx_on_face(D, xq, pq), Y.nc, Y.nb, dc, db, fixq, s_qinv[Y.d]);
     }
     __syncwarp();
   };
   RxVoxel X;
-  rx_fetch(s_uo, s_un, dom, plane, sk, s_base, v0, pf, nvox, X);
+  rx_fetch(s_uo, s_un, dom, plane, sk, s_base, fixq, s_qunit, v0, pf, nvox, X);
   for (int it = 0; it < MLP_DEPLOY_VPT; it++) {
     const long long v = v0 + (long long)it * MLP_DEPLOY_T;
     const RxVoxel Y = X;
@@ -535,7 +544,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     xc = xf;
     pf += MLP_DEPLOY_T;
     while (pf >= P) { pf -= P; xf++; }
-    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(s_uo, s_un, dom, plane, sk, s_base, v + MLP_DEPLOY_T, pf, nvox, X);
+    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(s_uo, s_un, dom, plane, sk, s_base, fixq, s_qunit, v + MLP_DEPLOY_T, pf, nvox, X);
     const int d = Y.d;
     const RxConst& kc = sk[d];
     bool elig = false, skip = false;
@@ -561,7 +570,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
         n_fall++;
         rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
       }
-      rx_store(s_fm[d], s_un, kc, v, dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db);
+      rx_store(s_fm[d], s_un, kc, v, dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db, fixq, s_qinv[d]);
     }
     const unsigned nm = __ballot_sync(0xffffffffu, net);
     if (net) pend[npend + __popc(nm & ((1u << lane) - 1u))] = v;
@@ -650,6 +659,82 @@ __global__ void k_mlp_pairs(const RealDesc* __restrict__ desc, unsigned long lon
   rx_target(kc, dtr, (float)c, b, dbd, tf);
   for (int j = 0; j < MLP_IN; j++) x[i * MLP_IN + j] = xf[j];
   for (int j = 0; j < MLP_OUT; j++) t[i * MLP_OUT + j] = tf[j];
+}
+
+// ---- training pairs harvested from simulation states (csp_mlp_harvest) ----
+// Candidates are the voxels of the surrogate's domains with Ca in [0.1, 500] uM; their
+// log10 Ca falls in one of MLP_HARVEST_BINS bins.  Pass 0 counts the candidates per bin;
+// pass 1 takes each with its bin's probability (prob[], chosen on the host so the taken
+// pairs are as near log-uniform in Ca as the states allow) and writes its features and
+// its target from the plain integrator, exactly as k_mlp_pairs does for drawn states.
+constexpr int MLP_HARVEST_BINS = 32;
+constexpr float MLP_HARVEST_LO = -1.f, MLP_HARVEST_HI = 2.69897f;   // log10(0.1), log10(500)
+
+__global__ void k_mlp_harvest(const RealDesc* __restrict__ descs, const RealCtl* __restrict__ ctl,
+                              const unsigned* __restrict__ elig, int pass, const float* __restrict__ prob,
+                              unsigned long long seed,
+                              unsigned long long* __restrict__ hist, unsigned long long* __restrict__ cursor,
+                              long long cap, float* __restrict__ x, float* __restrict__ t) {
+  __shared__ unsigned s_hist[MLP_HARVEST_BINS];
+  if (threadIdx.x < MLP_HARVEST_BINS) s_hist[threadIdx.x] = 0;
+  __syncthreads();
+  const int r = blockIdx.y;
+  const RealDesc& D = descs[r];
+  const RealCtl& C = ctl[r];
+  const unsigned cur = C.cur_mask[C.step & 1];
+  const long long nvox = (long long)D.nx * D.P;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvox;
+       v += (long long)gridDim.x * blockDim.x) {
+    if ((int)(v % D.P) >= D.plane) continue;
+    const int d = D.dom[v] & DOMAIN_BITS;
+    if (!((elig[r] >> d) & 1u)) continue;
+    const float c = __fadd_rn(D.fbase[d][0], D.u[cur & 1u][0][v]);
+    if (!(c >= 0.1f && c <= 500.f)) continue;
+    const int bin = min(MLP_HARVEST_BINS - 1,
+                        (int)((log10f(c) - MLP_HARVEST_LO) * (MLP_HARVEST_BINS / (MLP_HARVEST_HI - MLP_HARVEST_LO))));
+    if (pass == 0) {
+      atomicAdd(&s_hist[max(bin, 0)], 1u);
+      continue;
+    }
+    unsigned ctr[4] = {(unsigned)v, (unsigned)(v >> 32), (unsigned)r, 0x68727374u}, rr[4];
+    philox4x32(ctr, (unsigned)seed, (unsigned)(seed >> 32), rr);
+    if (((double)rr[0] + 0.5) * (1.0 / 4294967296.0) >= prob[max(bin, 0)]) continue;
+    const unsigned long long slot = atomicAdd(cursor, 1ull);
+    if ((long long)slot >= cap) continue;
+    const RxConst kc = rx_const(D, d);
+    float b[MLP_SLOTS];
+    double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      const float o = D.u[(cur >> (q + 1)) & 1u][q + 1][v];
+      b[q] = kc.tot[q] > 0.f
+                 ? __fadd_rn(D.fbase[d][q + 1], (D.fixq >> (q + 1) & 1u) ? q_value(o, D.qunit[d][q + 1]) : o)
+                 : 0.f;
+      bd[q] = b[q];
+    }
+    const float dtr = (float)(D.dt * D.reaction_substep);
+    rx_plain(kc, D.reaction_substep, D.dt, (double)c, bd, dcd, dbd);
+    float xf[MLP_IN], tf[MLP_OUT];
+    rx_features(kc, d, dtr, c, b, xf);
+    rx_target(kc, dtr, c, b, dbd, tf);
+    for (int j = 0; j < MLP_IN; j++) x[slot * MLP_IN + j] = xf[j];
+    for (int j = 0; j < MLP_OUT; j++) t[slot * MLP_OUT + j] = tf[j];
+  }
+  if (pass == 0) {
+    __syncthreads();
+    if (threadIdx.x < MLP_HARVEST_BINS && s_hist[threadIdx.x])
+      atomicAdd(&hist[threadIdx.x], (unsigned long long)s_hist[threadIdx.x]);
+  }
+}
+
+// Pairs [0, n) gathered in the order of the affine bijection j -> (a j + b) mod n (a odd
+// and coprime with n), so training batches mix states from every part of the harvest.
+__global__ void k_mlp_permute(const float* __restrict__ x, const float* __restrict__ t, long long n,
+                              unsigned long long a, unsigned long long b, float* __restrict__ xo, float* __restrict__ to) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const long long i = (long long)((a * (unsigned long long)j + b) % (unsigned long long)n);
+  for (int q = 0; q < MLP_IN; q++) xo[j * MLP_IN + q] = x[i * MLP_IN + q];
+  for (int q = 0; q < MLP_OUT; q++) to[j * MLP_OUT + q] = t[i * MLP_OUT + q];
 }
 
 constexpr int MLP_TB = 128;           // samples (threads) per CTA of the gradient kernel

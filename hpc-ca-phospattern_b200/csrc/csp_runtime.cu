@@ -182,6 +182,10 @@ struct csp_handle {
   float surrogate_tol = 1e-4f;
   float* d_mlp = nullptr;                   // MLP_NPARAM parameters
   unsigned long long* d_mlp_cnt = nullptr;  // voxels, network evaluations, fallbacks
+  // training pairs harvested from the fields (csp_mlp_harvest): features [cap][8], targets [cap][5]
+  float* d_hx = nullptr;
+  float* d_ht = nullptr;
+  long long harvest_cap = 0, harvest_n = 0;
   std::string msg;
 };
 
@@ -507,6 +511,30 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
         D.dinit[a][s] = (float)(m.domain[a].init[s] - D.base[a][s]);
       }
     }
+    // fixed-point species (RealDesc::fixq): never diffusive, the bound form of some buffer
+    // and the ligand of none; unit a power of two with 2 tot below 2^31 units
+    {
+      unsigned bound = 0, ligand = 0;
+      for (int dd = 0; dd < nd; dd++)
+        for (int bi = 0; bi < m.domain[dd].num_buffers; bi++) {
+          bound |= 1u << m.domain[dd].bsp0[bi];
+          ligand |= 1u << m.domain[dd].bsp1[bi];
+        }
+      for (int s = 1; s < m.num_species; s++)
+        if (D.dsi_of[s] < 0 && (bound >> s & 1u) && !(ligand >> s & 1u)) D.fixq |= 1u << s;
+      for (int dd = 0; dd < ND; dd++)
+        for (int s = 0; s < NS; s++) {
+          double range = 0.0;
+          if (dd < nd && s < m.num_species) {
+            range = std::fabs(m.domain[dd].init[s]) + std::fabs(D.base[dd][s]);
+            for (int bi = 0; bi < m.domain[dd].num_buffers; bi++)
+              if (m.domain[dd].bsp0[bi] == s) range = std::max(range, m.domain[dd].tot[bi]);
+          }
+          const int e = range > 0.0 ? (int)std::ceil(std::log2(range)) : 0;
+          D.qunit[dd][s] = std::ldexp(1.0f, e - 30);
+          D.qinv[dd][s] = std::ldexp(1.0f, 30 - e);
+        }
+    }
     // buffer reactions about the bases (buffer_dj): a_dt = dt_r k_on (tot - base_s0),
     // j0_dt = dt_r (k_on (tot - base_s0) base_s1 - k_off base_s0), FP64 before rounding
     for (int bi = 0; bi < d.nbuf; bi++)
@@ -563,7 +591,14 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     for (int dd = 0; dd < ND; dd++) hr.volumes[dd] = dd < nd ? gcount[dd] * m.h_geom * m.h_geom * m.h_geom : 0.0;
     hostf.assign(hr.field_elems, 0.f);
     for (int s = 0; s < m.num_species; s++) {
-      for (size_t i = 0; i < hr.field_elems; i++) hostf[i] = D.dinit[hostd[i]][s];   // init - base
+      for (size_t i = 0; i < hr.field_elems; i++) {
+        const int dd = hostd[i];
+        hostf[i] = D.dinit[dd][s];                                                   // init - base
+        if (D.fixq >> s & 1u) {
+          const int32_t q = (int32_t)std::lrint((double)D.dinit[dd][s] * D.qinv[dd][s]);
+          memcpy(&hostf[i], &q, sizeof q);
+        }
+      }
       cudaMemcpyAsync(D.u[0][s], hostf.data(), hr.field_elems * sizeof(float), cudaMemcpyHostToDevice, h->stream);
       cudaStreamSynchronize(h->stream);
     }
@@ -1229,6 +1264,8 @@ struct StateMap {
   const RealCtl* ctl;                // the realisation's progress block
   const unsigned char* dom;          // domain bytes (device order)
   double base[ND][NS];               // field bases: value = base[domain][s] + field
+  unsigned fixq;                     // fixed-point species: value = base + q * qunit
+  float qunit[ND][NS];
   int n[3];                          // physical voxels per axis
   long long stride[3];               // device index stride of each physical axis
   long long nvox;
@@ -1254,8 +1291,21 @@ __global__ void k_state_in(const T* __restrict__ src, StateMap m) {
   if (i >= m.nvox * m.ns) return;
   const int s = (int)(i / m.nvox);
   const long long di = state_index(m, i - (long long)s * m.nvox);
-  const double b = m.base[m.dom[di] & DOMAIN_BITS][s];
-  state_field(m, s)[di] = (float)((double)src[i] - b);
+  const int d = m.dom[di] & DOMAIN_BITS;
+  const double dev = (double)src[i] - m.base[d][s];
+  if (m.fixq >> s & 1u) {   // round to the unit, saturated to the integer range
+    const double q = fmin(fmax(rint(dev / m.qunit[d][s]), -2147483647.0), 2147483647.0);
+    state_field(m, s)[di] = __int_as_float((int)q);
+  } else {
+    state_field(m, s)[di] = (float)dev;
+  }
+}
+
+__device__ __forceinline__ double state_value(const StateMap& m, int s, long long di) {
+  const int d = m.dom[di] & DOMAIN_BITS;
+  const float f = state_field(m, s)[di];
+  const double dev = (m.fixq >> s & 1u) ? (double)__float_as_int(f) * m.qunit[d][s] : (double)f;
+  return dev + m.base[d][s];
 }
 
 // stored deviation -> host value (double)field + base (FP32 hosts: rounded once more)
@@ -1264,16 +1314,14 @@ __global__ void k_state_out(T* __restrict__ dst, StateMap m) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= m.nvox * m.ns) return;
   const int s = (int)(i / m.nvox);
-  const long long di = state_index(m, i - (long long)s * m.nvox);
-  dst[i] = static_cast<T>((double)state_field(m, s)[di] + m.base[m.dom[di] & DOMAIN_BITS][s]);
+  dst[i] = static_cast<T>(state_value(m, s, state_index(m, i - (long long)s * m.nvox)));
 }
 
 // One species of the physical-order FP64 state (the species slot of k_state_out's output).
 __global__ void k_state_out_species(double* __restrict__ dst, StateMap m, int s) {
   const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (v >= m.nvox) return;
-  const long long di = state_index(m, v);
-  dst[v] = (double)state_field(m, s)[di] + m.base[m.dom[di] & DOMAIN_BITS][s];
+  dst[v] = state_value(m, s, state_index(m, v));
 }
 
 static StateMap make_state_map(const csp_handle* h, int r) {
@@ -1286,6 +1334,8 @@ static StateMap make_state_map(const csp_handle* h, int r) {
   m.ctl = h->d_ctl + r;
   m.dom = D.dom;
   memcpy(m.base, D.base, sizeof m.base);
+  m.fixq = D.fixq;
+  memcpy(m.qunit, D.qunit, sizeof m.qunit);
   for (int a = 0; a < 3; a++) m.n[a] = hr.nphys[a];
   // device axis i holds physical axis perm[i]; device strides P, nz, 1
   const long long dstr[3] = {(long long)D.P, (long long)D.nz, 1};
@@ -1624,6 +1674,8 @@ struct LinescanMap {
   const float* f;
   const unsigned char* dom;
   double base[ND];           // the species' field base per domain
+  int fixq;                  // the species is stored in fixed point: value = base + q * qunit
+  double qunit[ND];
   int nd[3];                 // device extents (n0, n1, n2)
   int P;
   int phys_of_dev[3];        // physical axis of each device axis
@@ -1649,7 +1701,7 @@ __global__ void k_linescan_bins(LinescanMap m, double* __restrict__ bins) {
     if (m.num_domains > 0 && dom >= m.num_domains) continue;
     int pc[3];
     pc[m.phys_of_dev[0]] = c0; pc[m.phys_of_dev[1]] = c1; pc[m.phys_of_dev[2]] = c2;
-    double w = (double)m.f[dv] + m.base[dom];
+    double w = (m.fixq ? (double)__float_as_int(m.f[dv]) * m.qunit[dom] : (double)m.f[dv]) + m.base[dom];
     for (int a = 0; a < 3; a++)
       if (a != m.axis) w *= m.w[a][pc[a]];
     atomicAdd(&sb[pc[m.axis]], w);
@@ -1695,7 +1747,11 @@ extern "C" int csp_linescan(csp_handle* h, int32_t r, int32_t species, int32_t a
   LinescanMap m;
   m.f = D.u[(cur >> species) & 1u][species];
   m.dom = D.dom;
-  for (int dd = 0; dd < ND; dd++) m.base[dd] = D.base[dd][species];
+  for (int dd = 0; dd < ND; dd++) {
+    m.base[dd] = D.base[dd][species];
+    m.qunit[dd] = D.qunit[dd][species];
+  }
+  m.fixq = (D.fixq >> species) & 1u;
   m.nd[0] = D.nx; m.nd[1] = D.ny; m.nd[2] = D.nz;
   m.P = D.P;
   for (int i = 0; i < 3; i++) m.phys_of_dev[i] = hr.perm[i];
@@ -1855,7 +1911,7 @@ extern "C" int csp_autotune(csp_handle* h, int32_t repeats, csp_tune_report* rep
   StagedPlan best_plan;
   csp_tune_report local;
   memset(&local, 0, sizeof local);
-  for (int i = 0; i < ncand && i < CSP_TUNE_MAX; i++) {
+  for (int i = 0; i < ncand && i < CSP_TUNE_MAX - 1; i++) {
     StagedPlan pl = staged_plan(descs, cand[i][0], cand[i][1]);
     local.threads[local.n] = cand[i][0];
     local.segment[local.n] = pl.g.seg;
@@ -1892,15 +1948,41 @@ extern "C" int csp_autotune(csp_handle* h, int32_t repeats, csp_tune_report* rep
     }
     local.n++;
   }
+  // the direct kernel (recomputes the same step, like the staged candidates)
+  bool direct = false;
+  {
+    const int i = local.n;
+    local.threads[i] = 256;
+    local.segment[i] = -1;
+    dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)h->n);
+    k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_err);
+    cudaEventRecord(e0, h->stream);
+    for (int k = 0; k < repeats; k++) k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc, h->d_ctl, h->d_err);
+    cudaEventRecord(e1, h->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      if (best >= 0) staged_release(best_plan);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(h, CSP_ECUDA, "autotune: %s", cudaGetErrorString(e));
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    local.ms[i] = ms / repeats;
+    if (best < 0 || local.ms[i] < best_ms) direct = true;
+    local.n++;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (best < 0) return fail(h, CSP_ENOTSUP, "autotune: no staged plan fits this batch");
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  staged_release(h->plan);
-  h->plan = best_plan;
+  if (best >= 0) {
+    staged_release(h->plan);
+    h->plan = best_plan;
+  }
   h->plan_epoch++;
-  h->kernel = 0;
-  local.chosen = best;
+  h->kernel = direct ? 1 : 0;
+  local.chosen = direct ? local.n - 1 : best;
   if (rep) *rep = local;
   return CSP_OK;
 }
@@ -2031,6 +2113,90 @@ extern "C" int csp_mlp_forward(const float* params, const float* x, int64_t n, i
   return CSP_OK;
 }
 
+extern "C" int csp_mlp_harvest(csp_handle* h, int64_t n, uint64_t seed, int64_t capacity, int64_t* taken,
+                               int64_t* held) {
+  if (!h || n < 0 || capacity < 1) return fail(h, CSP_EINVAL, "bad argument");
+  CSP_NOT_PENDING(h);
+  int rc = surrogate_supported(h);
+  if (rc) return rc;
+  if (!h->d_hx) {
+    if (cudaMalloc(&h->d_hx, (size_t)capacity * MLP_IN * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&h->d_ht, (size_t)capacity * MLP_OUT * sizeof(float)) != cudaSuccess) {
+      cudaFree(h->d_hx); cudaFree(h->d_ht);
+      h->d_hx = h->d_ht = nullptr;
+      return fail(h, CSP_ENOMEM, "harvest buffer of %lld pairs", (long long)capacity);
+    }
+    h->harvest_cap = capacity;
+    h->harvest_n = 0;
+  } else if (capacity > h->harvest_cap) {
+    return fail(h, CSP_EINVAL, "capacity %lld above the first call's %lld", (long long)capacity, h->harvest_cap);
+  }
+  unsigned long long* dcnt = nullptr;      // [BINS] histogram, then the cursor
+  float* dprob = nullptr;
+  unsigned* delig = nullptr;               // per realisation: the domains the surrogate serves
+  std::vector<unsigned> elig(h->n);
+  for (int r = 0; r < h->n; r++) elig[r] = mlp_eligible_domains(h->real[r].desc);
+  cudaError_t e = cudaMalloc(&dcnt, (MLP_HARVEST_BINS + 1) * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&dprob, MLP_HARVEST_BINS * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&delig, h->n * sizeof(unsigned));
+  cudaStream_t st = h->stream;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(delig, elig.data(), h->n * sizeof(unsigned), cudaMemcpyHostToDevice, st);
+  unsigned long long hist[MLP_HARVEST_BINS + 1] = {};
+  dim3 grid((unsigned)std::min<long long>(1184, (h->max_vox + 255) / 256), (unsigned)h->n);
+  if (e == cudaSuccess) e = cudaMemsetAsync(dcnt, 0, (MLP_HARVEST_BINS + 1) * sizeof(unsigned long long), st);
+  if (e == cudaSuccess) {
+    k_mlp_harvest<<<grid, 256, 0, st>>>(h->d_desc, h->d_ctl, delig, 0, dprob, seed, dcnt, nullptr, 0, nullptr, nullptr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hist, dcnt, MLP_HARVEST_BINS * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  // water filling: every bin gives min(count, level) pairs, the level set so the bins give n
+  const long long want = std::min<long long>(n, h->harvest_cap - h->harvest_n);
+  double total = 0.0;
+  for (int b = 0; b < MLP_HARVEST_BINS; b++) total += (double)hist[b];
+  double lo = 0.0, hi = 0.0;
+  for (int b = 0; b < MLP_HARVEST_BINS; b++) hi = std::max(hi, (double)hist[b]);
+  for (int it = 0; it < 100 && total > want; it++) {
+    const double mid = 0.5 * (lo + hi);
+    double s = 0.0;
+    for (int b = 0; b < MLP_HARVEST_BINS; b++) s += std::min((double)hist[b], mid);
+    (s > want ? hi : lo) = mid;
+  }
+  float prob[MLP_HARVEST_BINS];
+  for (int b = 0; b < MLP_HARVEST_BINS; b++)
+    prob[b] = hist[b] == 0 ? 0.f : (total <= want ? 1.f : (float)(std::min((double)hist[b], lo) / (double)hist[b]));
+  const unsigned long long start = (unsigned long long)h->harvest_n;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dprob, prob, sizeof prob, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dcnt + MLP_HARVEST_BINS, &start, sizeof start, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && want > 0) {
+    k_mlp_harvest<<<grid, 256, 0, st>>>(h->d_desc, h->d_ctl, delig, 1, dprob, seed, nullptr, dcnt + MLP_HARVEST_BINS,
+                                        h->harvest_cap, h->d_hx, h->d_ht);
+    e = cudaGetLastError();
+  }
+  unsigned long long end = start;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&end, dcnt + MLP_HARVEST_BINS, sizeof end, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(dcnt);
+  cudaFree(dprob);
+  cudaFree(delig);
+  if (e != cudaSuccess) return fail(h, CSP_ECUDA, "harvest: %s", cudaGetErrorString(e));
+  const long long now = std::min<long long>((long long)end, h->harvest_cap);
+  if (taken) *taken = now - h->harvest_n;
+  h->harvest_n = now;
+  if (held) *held = now;
+  return CSP_OK;
+}
+
+extern "C" int csp_mlp_harvested(const csp_handle* hc, int64_t first, int64_t n, float* x, float* t) {
+  csp_handle* h = const_cast<csp_handle*>(hc);
+  if (!h || !x || !t || first < 0 || n < 0) return CSP_EINVAL;
+  if (first + n > h->harvest_n) return fail(h, CSP_ERANGE, "pairs [%lld, %lld) beyond the %lld held", (long long)first,
+                                            (long long)(first + n), h->harvest_n);
+  CUDA_TRY(h, cudaMemcpy(x, h->d_hx + first * MLP_IN, (size_t)n * MLP_IN * sizeof(float), cudaMemcpyDeviceToHost));
+  CUDA_TRY(h, cudaMemcpy(t, h->d_ht + first * MLP_OUT, (size_t)n * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost));
+  return CSP_OK;
+}
+
 extern "C" int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg, float* params,
                              csp_mlp_report* rep) {
   if (!h || !cfg || !params) return CSP_EINVAL;
@@ -2043,7 +2209,13 @@ extern "C" int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg
   for (int d = 0; d < D.nd; d++)
     if ((elig >> d) & 1u) doms.push_back(d);
   if (doms.empty()) return fail(h, CSP_EINVAL, "realisation %d has no domain the surrogate can serve", r);
-  const long long nt = cfg->samples > 0 ? cfg->samples : 1000000, nv = cfg->val_samples > 0 ? cfg->val_samples : 65536;
+  const bool harvested = cfg->source == CSP_MLP_SOURCE_HARVEST;
+  if (harvested && h->harvest_n < 2) return fail(h, CSP_EINVAL, "no harvested pairs (csp_mlp_harvest)");
+  long long nt = cfg->samples > 0 ? cfg->samples : 1000000, nv = cfg->val_samples > 0 ? cfg->val_samples : 65536;
+  if (harvested) {   // every harvested pair; the held-out share at most a tenth
+    nv = std::max<long long>(1, std::min<long long>(nv, h->harvest_n / 10));
+    nt = h->harvest_n - nv;
+  }
   const int batch = cfg->batch > 0 ? cfg->batch : 16384, epochs = cfg->epochs > 0 ? cfg->epochs : 10;
   const long long ntot = nt + nv;
   float *dx = nullptr, *dtg = nullptr, *dp = nullptr, *dg = nullptr, *dm = nullptr, *dv = nullptr;
@@ -2067,8 +2239,22 @@ extern "C" int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg
   if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, pb, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(dm, 0, pb, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(dv, 0, pb, st);
-  if (e == cudaSuccess) {
+  if (e == cudaSuccess && !harvested) {
     k_mlp_pairs<<<(unsigned)((ntot + 255) / 256), 256, 0, st>>>(ddesc, cfg->seed, ntot, dd, (int)doms.size(), dx, dtg);
+    e = cudaGetLastError();
+  } else if (e == cudaSuccess) {
+    // harvested pairs, shuffled by an affine bijection (a coprime with ntot)
+    auto gcd = [](unsigned long long p, unsigned long long q) {
+      while (q) { const unsigned long long t = p % q; p = q; q = t; }
+      return p;
+    };
+    const unsigned long long nn = (unsigned long long)ntot;
+    unsigned long long a = 1;
+    if (nn > 2) {
+      a = 2654435761ull % nn;
+      while (a < 2 || gcd(a, nn) != 1) a = a + 1 < nn ? a + 1 : 2;
+    }
+    k_mlp_permute<<<(unsigned)((ntot + 255) / 256), 256, 0, st>>>(h->d_hx, h->d_ht, ntot, a, cfg->seed % ntot, dx, dtg);
     e = cudaGetLastError();
   }
   float val_first = 0.f, val_last = 0.f;
@@ -2151,6 +2337,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
   cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt);
+  cudaFree(h->d_hx); cudaFree(h->d_ht);
   for (auto& e : h->phase_ev)
     if (e) cudaEventDestroy(e);
   if (h->ev0) cudaEventDestroy(h->ev0);

@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
         // pairs (0,1) and (2,3) in two-lane FP32 ----
         float val[MS][4];
         F2 o2[MS][2];
+        const unsigned fq = D.fixq & lmask;   // fixed-point species: o2 holds the increment
         int slot = 0;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -306,8 +307,15 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           } else {
             val[s][0] = val[s][1] = val[s][2] = val[s][3] = 0.f;
           }
-          o2[s][0] = f2(val[s][0], val[s][1]);
-          o2[s][1] = f2(val[s][2], val[s][3]);
+          if (fq >> s & 1u) {
+            const float qu = D.qunit[d0][s];
+#pragma unroll
+            for (int j = 0; j < 4; j++) val[s][j] = q_value(val[s][j], qu);
+            o2[s][0] = o2[s][1] = f2(0.f, 0.f);
+          } else {
+            o2[s][0] = f2(val[s][0], val[s][1]);
+            o2[s][1] = f2(val[s][2], val[s][3]);
+          }
         }
         const F2 m2 = f2(-2.f, -2.f);
         slot = 0;
@@ -387,7 +395,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
               float vj[MS], oj[MS];
 #pragma unroll
               for (int s = 0; s < MS; s++) { vj[s] = val[s][j]; oj[s] = out[s][j]; }
-              react_general<MS>(D, d0, vj, oj, si.pre);
+              react_general<MS>(D, d0, vj, oj, si.pre, fq);
 #pragma unroll
               for (int s = 0; s < MS; s++) out[s][j] = oj[s];
             }
@@ -395,12 +403,21 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
         }
         const unsigned fm = D.fixed_mask[d0];
 #pragma unroll
-        for (int s = 0; s < MS; s++)
+        for (int s = 0; s < MS; s++) {
           if (fm >> s & 1u) {
             const float iv = D.dinit[d0][s];
 #pragma unroll
             for (int j = 0; j < 4; j++) out[s][j] = iv;
           }
+          if (fq >> s & 1u) {
+            // the stored integers plus the increments (or the fixed value)
+            const float4 raw = *reinterpret_cast<const float4*>(fc + __popc(lmask & ((1u << s) - 1u)) * so + p0);
+            const float qi = D.qinv[d0][s];
+            const float rw[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++) out[s][j] = (fm >> s & 1u) ? q_set(out[s][j], qi) : q_add(rw[j], out[s][j], qi);
+          }
+        }
         if (D.dirichlet) {
 #pragma unroll
           for (int j = 0; j < 4; j++)
@@ -438,6 +455,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           }
           unij[j] = u;
         }
+        const unsigned fq = D.fixq & lmask;   // fixed-point species: out holds the increment
         int slot = 0;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -449,7 +467,10 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             val[s][0] = val[s][1] = val[s][2] = val[s][3] = 0.f;
           }
 #pragma unroll
-          for (int j = 0; j < 4; j++) out[s][j] = val[s][j];
+          for (int j = 0; j < 4; j++) {
+            if (fq >> s & 1u) val[s][j] = q_value(val[s][j], D.qunit[dj[j]][s]);
+            out[s][j] = (fq >> s & 1u) ? 0.f : val[s][j];
+          }
         }
         slot = 0;
 #pragma unroll
@@ -600,15 +621,20 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
               float vj[MS], oj[MS];
 #pragma unroll
               for (int s = 0; s < MS; s++) { vj[s] = val[s][j]; oj[s] = out[s][j]; }
-              react_general<MS>(D, d, vj, oj, si.pre);
+              react_general<MS>(D, d, vj, oj, si.pre, fq);
 #pragma unroll
               for (int s = 0; s < MS; s++) out[s][j] = oj[s];
             }
           }
           const unsigned fm = D.fixed_mask[d];
 #pragma unroll
-          for (int s = 0; s < MS; s++)
+          for (int s = 0; s < MS; s++) {
             if (fm >> s & 1u) out[s][j] = D.dinit[d][s];
+            if (fq >> s & 1u) {
+              const float rw = fc[__popc(lmask & ((1u << s) - 1u)) * so + p0 + j];
+              out[s][j] = (fm >> s & 1u) ? q_set(out[s][j], D.qinv[d][s]) : q_add(rw, out[s][j], D.qinv[d][s]);
+            }
+          }
           if (D.dirichlet && (vzy[j] | xval) != 63u) out[0][j] = D.dinit[d][0];
         }
 #pragma unroll

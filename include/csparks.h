@@ -341,7 +341,9 @@ typedef struct csp_mlp_config {
   float lr;                 /* Adam learning rate, cosine decay (default 1e-3) */
   double tol;               /* acceptance tolerance reported on the held-out pairs (default 1e-4) */
   uint64_t seed;            /* Philox key of the pair sampler */
+  int32_t source;           /* CSP_MLP_SOURCE_SAMPLED (default) or CSP_MLP_SOURCE_HARVEST */
 } csp_mlp_config;
+enum { CSP_MLP_SOURCE_SAMPLED = 0, CSP_MLP_SOURCE_HARVEST = 1 };
 
 typedef struct csp_mlp_report {
   float val_loss_first, val_loss_last;   /* held-out mean squared error before / after */
@@ -358,6 +360,20 @@ void csp_mlp_init(uint64_t seed, float* params);
  * 0.1-500 uM in the cytosol, 10-2000 uM in SR domains; targets from the plain integrator),
  * Adam on the mean squared error; params in (start) / out (trained). */
 int csp_mlp_train(csp_handle* h, int32_t r, const csp_mlp_config* cfg, float* params, csp_mlp_report* rep);
+/* Training pairs from the simulation's own states.  Every voxel of the surrogate's domains
+ * with Ca in 0.1-500 uM, in every realisation, at the current step, is a candidate; each
+ * is taken with a probability for its log10-Ca bin (32 bins) chosen so that about n pairs
+ * are taken, as near log-uniform in Ca as the states allow (bins with fewer candidates
+ * give all they have).  A pair is the features of the voxel's state and the target from
+ * the plain integrator, as for sampled states.  Pairs accumulate in the handle (device
+ * memory for `capacity` pairs, allocated by the first call) across calls at different
+ * steps; *taken / *held receive the pairs of this call / all held.  csp_mlp_train with
+ * cfg->source = CSP_MLP_SOURCE_HARVEST trains on every held pair (a tenth at most, up to
+ * val_samples, held out), shuffled.  The reaction these pairs stand for is the
+ * reference's Species_step_reaction (species.c:1653-1702). */
+int csp_mlp_harvest(csp_handle* h, int64_t n, uint64_t seed, int64_t capacity, int64_t* taken, int64_t* held);
+/* Copy held pairs [first, first + n) to the host: x[n][8] features, t[n][5] targets. */
+int csp_mlp_harvested(const csp_handle* h, int64_t first, int64_t n, float* x, float* t);
 /* Loss and gradient of the mean squared error of params on n host pairs x[n][8], t[n][5]
  * with the device kernels used in training (for checks against a CPU implementation). */
 int csp_mlp_gradient(const float* params, const float* x, const float* t, int64_t n, float* grad, float* loss);
@@ -373,9 +389,11 @@ int csp_surrogate_counts(const csp_handle* h, int64_t* voxels, int64_t* network,
 
 /* ---- autotuner ----
  * Times candidate tile shapes of the staged voxel kernel (threads per CTA, x planes per
- * work unit) at the current step and keeps the fastest; fields are the same for every
- * shape.  No counterpart in the reference (its OpenMP loops have no tile parameters). */
-#define CSP_TUNE_MAX 8
+ * work unit) and the direct kernel (segment = -1: one thread per voxel, every plane at
+ * once, which wins on batches too small to give the staged kernel's work units to every
+ * CTA slot) at the current step and keeps the fastest; fields are the same for every
+ * candidate.  No counterpart in the reference (its OpenMP loops have no tile parameters). */
+#define CSP_TUNE_MAX 10
 typedef struct csp_tune_report {
   int32_t n;                       /* candidates tried */
   int32_t threads[CSP_TUNE_MAX];

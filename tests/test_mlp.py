@@ -184,9 +184,16 @@ def test_surrogate_deployed_in_simulation(pkg, synth):
     scale = np.max(np.abs(uf), axis=(1, 2, 3))
     err_plain = np.max(np.abs(up - uf), axis=(1, 2, 3)) / scale
     err_sur = np.max(np.abs(us - uf), axis=(1, 2, 3)) / scale
+    rms_plain = np.sqrt(np.mean((up - uf) ** 2, axis=(1, 2, 3))) / scale
+    rms_sur = np.sqrt(np.mean((us - uf) ** 2, axis=(1, 2, 3))) / scale
     print(f"voxels {vx}, network {ev}, fallbacks {fb} ({fb / vx:.3f}); max error vs reacting every step: plain -T 10dt "
-          f"{err_plain.max():.2e}, surrogate {err_sur.max():.2e}")
-    assert err_sur.max() <= 1.05 * err_plain.max() + 1e-6
+          f"{err_plain.max():.2e}, surrogate {err_sur.max():.2e}; per species plain {np.array2string(err_plain, precision=2)}"
+          f" surrogate {np.array2string(err_sur, precision=2)}; rms plain {np.array2string(rms_plain, precision=2)}"
+          f" surrogate {np.array2string(rms_sur, precision=2)}")
+    # a strict gain over the method without the network (most of what remains is the
+    # operator splitting of reacting every 10 steps, which the network does not see)
+    assert err_sur.max() < 0.95 * err_plain.max()
+    assert np.sqrt(np.mean(rms_sur ** 2)) < np.sqrt(np.mean(rms_plain ** 2))
 
 
 @pytest.mark.gpu
@@ -203,3 +210,49 @@ def test_forward_passes_match_oracle(pkg):
     print(f"forward max error / scale: FP32 {e32:.2e}, TF32 tensor cores {etc:.2e}")
     assert e32 <= 1e-5
     assert etc <= 2e-3
+
+
+@pytest.mark.gpu
+def test_harvest_pairs_from_simulation(pkg, synth):
+    """Training pairs taken from a running batched ensemble (csp_mlp_harvest): about the
+    requested count, Ca within 0.1-500 uM, flatter in log Ca than the states themselves,
+    targets those of the numpy oracle's plain integrator for the pair's state; a network
+    trained on them is accepted on most held-out pairs."""
+    specs, opts = synth.config3(n=4, shape=(40, 40, 30))
+    dtr10 = 10 * DT
+    opts = [dict(o, dt_update_react=dtr10, tstop=1.0) for o in opts]
+    sim = pkg.Simulation(specs, opts)
+    held = 0
+    for k in range(4):
+        sim.advance(500)
+        taken, held = sim.mlp_harvest(60000, seed=10 + k, capacity=400000)
+        assert 0 < taken <= 70000
+    assert held > 100000
+    x, t = sim.mlp_harvested(0, held)
+    logc = 3.0 * x[:, 0].astype(np.float64)
+    assert logc.min() >= -1.0 - 1e-5 and logc.max() <= np.log10(500.0) + 1e-5
+    # flatter than the states: the rest Ca (0.14 uM) bin holds far less than it would
+    hist, _ = np.histogram(logc, bins=32, range=(-1.0, np.log10(500.0)))
+    assert hist.max() < 0.25 * held, hist
+    # targets: the oracle's plain integrator for the state the features describe
+    spec, d_rng = specs[0], np.random.default_rng(4)
+    n = sim.info().reaction_substep
+    checked = 0
+    for i in d_rng.choice(held, 300, replace=False):
+        d = int(round(4.0 * x[i, 7]))
+        k = om.constants(spec, d)
+        c = 10.0 ** logc[i]
+        b = x[i, 1:6].astype(np.float64) * k[2]
+        dc, db = om.plain(k, n, DT, c, b)
+        S = om.scale(k, dtr10, c, b)
+        gg = om.g(k, c, b)
+        on = (k[2] > 0) & (S > 1e-30)
+        tref = np.clip((db[on] / k[2][on] - dtr10 * gg[on] / k[2][on]) / S[on], -20, 20)
+        np.testing.assert_allclose(t[i][on], tref, rtol=0.05, atol=0.05)
+        checked += 1
+    assert checked == 300
+    p, rep = sim.mlp_train(samples=0, val_samples=20000, epochs=30, batch=4096, lr=2e-3, seed=3, harvested=True)
+    print("harvested", held, rep)
+    assert rep["val_loss_last"] < 0.5 * rep["val_loss_first"], rep
+    assert rep["val_accept_rate"] > 0.9, rep
+    sim.close()
