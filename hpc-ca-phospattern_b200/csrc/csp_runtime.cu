@@ -1853,7 +1853,8 @@ extern "C" int csp_get_phase_times(const csp_handle* h, double* ms, int64_t* ste
 
 extern "C" int csp_test_wait_timeout(csp_handle* h, int32_t on) {
   if (!h) return CSP_EINVAL;
-  if (on && (h->kernel != 0 || !h->plan.ok)) return fail(h, CSP_EINVAL, "the staged voxel kernel is not in use");
+  if (on && (h->kernel != 0 || !h->plan.ok || !h->plan.launch_inject))
+    return fail(h, CSP_EINVAL, "the staged voxel kernel with the test hook is not in use");
   h->inject_wait = on ? 1 : 0;
   return CSP_OK;
 }

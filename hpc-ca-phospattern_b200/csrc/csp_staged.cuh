@@ -58,7 +58,8 @@ struct StagedPlan {
   int nunits = 0;
   std::vector<int> unit_first;  // [n+1]: the units of realisation r are [unit_first[r], unit_first[r+1])
   StagedLaunchFn launch = nullptr;
-  StagedLaunchFn launch_inject = nullptr;
+  StagedLaunchFn launch_inject = nullptr;   // null: no test-hook variant for this plan
+  unsigned fixq = 0;                        // union of the realisations' fixed-point species
 };
 
 // ---- PTX helpers (sm_90+ bulk copy / mbarrier) ----
@@ -143,8 +144,10 @@ __device__ __forceinline__ unsigned ld_u32_any(const unsigned char* p) {
 }
 
 // INJ = true builds the test hook's variant (csp_test_wait_timeout); the kernel in use is
-// INJ = false, which has none of that code.
-template <int MS, int T, bool INJ = false>
+// INJ = false, which has none of that code.  FQ: the species that may be stored in fixed
+// point (RealDesc::fixq is a subset), known at compile time so that the code for every
+// other species has no fixed-point branch (a run-time mask over all species cost 18 %).
+template <int MS, int T, bool INJ, unsigned FQ>
 __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                         const int4* __restrict__ units, StagedGeom g,
                                                         int* __restrict__ err) {
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
         // pairs (0,1) and (2,3) in two-lane FP32 ----
         float val[MS][4];
         F2 o2[MS][2];
-        const unsigned fq = D.fixq & lmask;   // fixed-point species: o2 holds the increment
+        const unsigned fq = FQ & D.fixq & lmask;   // fixed-point species: o2 holds the increment
         int slot = 0;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -455,7 +458,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           }
           unij[j] = u;
         }
-        const unsigned fq = D.fixq & lmask;   // fixed-point species: out holds the increment
+        const unsigned fq = FQ & D.fixq & lmask;   // fixed-point species: out holds the increment
         int slot = 0;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -704,32 +707,36 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
 
 // Launch over the work units [u0, u1) (all units: one step of every realisation; the units
 // of a range of realisations: one step of those only).
-template <int MS, int T, bool INJ>
+template <int MS, int T, bool INJ, unsigned FQ>
 cudaError_t staged_launch_t(const StagedPlan& pl, int u0, int u1, const RealDesc* d, RealCtl* c, int* e,
                             cudaStream_t s) {
   if (u1 <= u0) return cudaSuccess;
   StagedGeom g = pl.g;
   g.nunits = u1 - u0;
-  k_voxels_staged<MS, T, INJ><<<std::min(g.nunits, pl.slots), T, g.smem, s>>>(d, c, pl.d_units + u0, g, e);
+  k_voxels_staged<MS, T, INJ, FQ><<<std::min(g.nunits, pl.slots), T, g.smem, s>>>(d, c, pl.d_units + u0, g, e);
   return cudaGetLastError();
 }
 
-template <int MS, int T>
+template <int MS, int T, unsigned FQ, bool WITH_INJ>
 cudaError_t staged_configure(StagedPlan& pl) {
-  cudaError_t e = cudaFuncSetAttribute(k_voxels_staged<MS, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.g.smem);
+  cudaError_t e = cudaFuncSetAttribute(k_voxels_staged<MS, T, false, FQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       pl.g.smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_voxels_staged<MS, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.g.smem);
-  if (e != cudaSuccess) return e;
+  if (WITH_INJ) {
+    e = cudaFuncSetAttribute(k_voxels_staged<MS, T, WITH_INJ, FQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             pl.g.smem);
+    if (e != cudaSuccess) return e;
+  }
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_voxels_staged<MS, T>, T, pl.g.smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_voxels_staged<MS, T, false, FQ>, T, pl.g.smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   pl.slots = per_sm * sms;
-  pl.launch = &staged_launch_t<MS, T, false>;
-  pl.launch_inject = &staged_launch_t<MS, T, true>;
+  pl.launch = &staged_launch_t<MS, T, false, FQ>;
+  pl.launch_inject = WITH_INJ ? &staged_launch_t<MS, T, WITH_INJ, FQ> : nullptr;
   return cudaSuccess;
 }
 
@@ -738,7 +745,11 @@ inline StagedPlan staged_plan(const std::vector<RealDesc>& descs, int T = 256, i
   StagedPlan pl;
   pl.T = T;
   int nz_max = 0, ns_max = 0;
-  for (const RealDesc& D : descs) { nz_max = std::max(nz_max, D.nz); ns_max = std::max(ns_max, D.ns); }
+  for (const RealDesc& D : descs) {
+    nz_max = std::max(nz_max, D.nz);
+    ns_max = std::max(ns_max, D.ns);
+    pl.fixq |= D.fixq;
+  }
   StagedGeom& g = pl.g;
   g.L = 4 * T;
   g.slot = (g.L + 2 * nz_max + 8 + 3) & ~3;
@@ -776,11 +787,19 @@ inline StagedPlan staged_plan(const std::vector<RealDesc>& descs, int T = 256, i
   return pl;
 }
 
+// The kernel variants built: five species with fixed point only for species 4 (the
+// reference model: TRPN), at 256 and 128 threads (the first with the test hook); five
+// species with any of species 1-4 fixed; eight species with any of 1-7 fixed.
 inline cudaError_t staged_prepare(StagedPlan& pl) {
   if (!pl.ok) return cudaErrorNotSupported;
-  cudaError_t e;
-  if (pl.g.ms == 5) e = pl.T == 128 ? staged_configure<5, 128>(pl) : staged_configure<5, 256>(pl);
-  else e = pl.T == 128 ? staged_configure<8, 128>(pl) : staged_configure<8, 256>(pl);
+  cudaError_t e = cudaErrorNotSupported;
+  const bool only4 = (pl.fixq & ~(1u << 4)) == 0;
+  if (pl.g.ms == 5 && only4)
+    e = pl.T == 128 ? staged_configure<5, 128, 1u << 4, false>(pl) : staged_configure<5, 256, 1u << 4, true>(pl);
+  else if (pl.g.ms == 5 && pl.T == 256)
+    e = staged_configure<5, 256, 0x1Eu, false>(pl);
+  else if (pl.T == 256)
+    e = staged_configure<8, 256, 0xFEu, false>(pl);
   if (e != cudaSuccess) pl.ok = false;
   return e;
 }
@@ -789,7 +808,7 @@ inline cudaError_t staged_prepare(StagedPlan& pl) {
 inline void staged_launch(const StagedPlan& pl, const RealDesc* d, RealCtl* c, int* e, cudaStream_t s,
                           bool inject = false, int r0 = 0, int r1 = -1) {
   if (r1 < 0) r1 = (int)pl.unit_first.size() - 1;
-  (inject ? pl.launch_inject : pl.launch)(pl, pl.unit_first[r0], pl.unit_first[r1], d, c, e, s);
+  (inject && pl.launch_inject ? pl.launch_inject : pl.launch)(pl, pl.unit_first[r0], pl.unit_first[r1], d, c, e, s);
 }
 
 inline void staged_release(StagedPlan& pl) {
