@@ -199,37 +199,60 @@ __device__ __forceinline__ void mlp_forward(const MlpW& W, const float* x, float
 //   A (16x8, row): a0 (g, q), a1 (g+8, q), a2 (g, q+4), a3 (g+8, q+4)
 //   B (8x8, col):  b0 (q, g), b1 (q+4, g)
 //   C (16x8):      c0 (g, 2q), c1 (g, 2q+1), c2 (g+8, 2q), c3 (g+8, 2q+1)
-// Weights sit in shared memory with padded rows (MLP_TC_LD) so that the fragment loads
-// hit 32 different banks; activations are staged per warp in a [32][MLP_TC_LD] tile.
+// Weights sit in shared memory as TF32 bit patterns (converted once per CTA) in fragment
+// order: for k-block kb and n-tile pair np, lane l's four words (b0, b1 of n-tile 2np, then
+// of 2np + 1) are contiguous, so a lane fetches two B fragments with one 16-byte load
+// (the output layer, a single n-tile: two words).  Activations are staged per warp in a
+// [32][MLP_TC_LD] tile whose padded rows put the A-fragment loads in 32 different banks.
 constexpr int MLP_TC_LD = MLP_H + 4;     // padded row length (floats)
 constexpr int MLP_TC_N3 = 8;             // output layer padded to one n-tile
+constexpr int MLP_F1 = (MLP_IN / 8) * (MLP_H / 16) * 32 * 4;
+constexpr int MLP_F2 = (MLP_H / 8) * (MLP_H / 16) * 32 * 4;
+constexpr int MLP_F3 = (MLP_H / 8) * 32 * 2;
 struct MlpTC {
-  float w1[MLP_IN * MLP_TC_LD];
-  float w2[MLP_H * MLP_TC_LD];
-  float w3[MLP_H * MLP_TC_LD];           // [64][8 used of LD], columns 5..7 zero
+  unsigned f1[MLP_F1], f2[MLP_F2], f3[MLP_F3];
   float b1[MLP_H], b2[MLP_H], b3[MLP_TC_N3];
 };
+static_assert(sizeof(MlpTC) % 16 == 0, "activation tiles follow the weights");
 constexpr int MLP_TC_STAGE = 32 * MLP_TC_LD;   // floats of one warp's activation tile
-
-__device__ __forceinline__ void mlp_tc_load(MlpTC& T, const float* __restrict__ p) {
-  const MlpW& W = *reinterpret_cast<const MlpW*>(p);
-  for (int i = threadIdx.x; i < MLP_IN * MLP_H; i += blockDim.x) T.w1[(i / MLP_H) * MLP_TC_LD + i % MLP_H] = W.w1[i];
-  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) T.w2[(i / MLP_H) * MLP_TC_LD + i % MLP_H] = W.w2[i];
-  for (int i = threadIdx.x; i < MLP_H * MLP_TC_N3; i += blockDim.x) {
-    const int k = i / MLP_TC_N3, n = i % MLP_TC_N3;
-    T.w3[k * MLP_TC_LD + n] = n < MLP_OUT ? W.w3[k * MLP_OUT + n] : 0.f;
-  }
-  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
-    T.b1[i] = W.b1[i];
-    T.b2[i] = W.b2[i];
-  }
-  for (int i = threadIdx.x; i < MLP_TC_N3; i += blockDim.x) T.b3[i] = i < MLP_OUT ? W.b3[i] : 0.f;
-}
 
 __device__ __forceinline__ unsigned tf32_bits(float f) {
   unsigned r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
   return r;
+}
+
+// Fragment-order word i of a layer with K inputs, NT n-tiles and W = [K][NV] (columns
+// beyond NV read as 0).
+template <int K, int NT, int NV>
+__device__ __forceinline__ unsigned mlp_frag_word(const float* W, int i) {
+  int kb, nt, lane, h;
+  if constexpr (NT >= 2) {
+    const int w = i & 3, rest = i >> 7;
+    lane = (i >> 2) & 31;
+    kb = rest / (NT / 2);
+    nt = 2 * (rest % (NT / 2)) + (w >> 1);
+    h = w & 1;
+  } else {
+    h = i & 1;
+    lane = (i >> 1) & 31;
+    kb = i >> 6;
+    nt = 0;
+  }
+  const int k = kb * 8 + (lane & 3) + 4 * h, n = nt * 8 + (lane >> 2);
+  return n < NV ? tf32_bits(W[k * NV + n]) : 0u;
+}
+
+__device__ __forceinline__ void mlp_tc_load(MlpTC& T, const float* __restrict__ p) {
+  const MlpW& W = *reinterpret_cast<const MlpW*>(p);
+  for (int i = threadIdx.x; i < MLP_F1; i += blockDim.x) T.f1[i] = mlp_frag_word<MLP_IN, MLP_H / 8, MLP_H>(W.w1, i);
+  for (int i = threadIdx.x; i < MLP_F2; i += blockDim.x) T.f2[i] = mlp_frag_word<MLP_H, MLP_H / 8, MLP_H>(W.w2, i);
+  for (int i = threadIdx.x; i < MLP_F3; i += blockDim.x) T.f3[i] = mlp_frag_word<MLP_H, 1, MLP_OUT>(W.w3, i);
+  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+    T.b1[i] = W.b1[i];
+    T.b2[i] = W.b2[i];
+  }
+  for (int i = threadIdx.x; i < MLP_TC_N3; i += blockDim.x) T.b3[i] = i < MLP_OUT ? W.b3[i] : 0.f;
 }
 
 __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
@@ -243,7 +266,7 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const unsigned (&a)[4], 
 // out[32][NT*8] = act(in[32][K] W[K][NT*8] + bias), in / out: [32][MLP_TC_LD] warp tiles
 // (out may be in: every read of a tile precedes its writes, and mma.sync converges the warp)
 template <int K, int NT, bool RELU>
-__device__ __forceinline__ void mlp_tc_layer(const float* in, const float* W, const float* bias, float* out,
+__device__ __forceinline__ void mlp_tc_layer(const float* in, const unsigned* F, const float* bias, float* out,
                                              int lane) {
   const int g = lane >> 2, q = lane & 3;
 #pragma unroll
@@ -251,20 +274,29 @@ __device__ __forceinline__ void mlp_tc_layer(const float* in, const float* W, co
     float acc[NT][4];
 #pragma unroll
     for (int nt = 0; nt < NT; nt++) {
-      acc[nt][0] = acc[nt][2] = bias[nt * 8 + 2 * q];
-      acc[nt][1] = acc[nt][3] = bias[nt * 8 + 2 * q + 1];
+      const float2 bb = *reinterpret_cast<const float2*>(bias + nt * 8 + 2 * q);
+      acc[nt][0] = acc[nt][2] = bb.x;
+      acc[nt][1] = acc[nt][3] = bb.y;
     }
     const float* r0 = in + (mt * 16 + g) * MLP_TC_LD;
     const float* r1 = r0 + 8 * MLP_TC_LD;
 #pragma unroll
-    for (int k0 = 0; k0 < K; k0 += 8) {
+    for (int kb = 0; kb < K / 8; kb++) {
+      const int k0 = kb * 8;
       const unsigned a[4] = {tf32_bits(r0[k0 + q]), tf32_bits(r1[k0 + q]), tf32_bits(r0[k0 + q + 4]),
                              tf32_bits(r1[k0 + q + 4])};
+      if constexpr (NT >= 2) {
 #pragma unroll
-      for (int nt = 0; nt < NT; nt++) {
-        const unsigned b[2] = {tf32_bits(W[(k0 + q) * MLP_TC_LD + nt * 8 + g]),
-                               tf32_bits(W[(k0 + q + 4) * MLP_TC_LD + nt * 8 + g])};
-        mma_tf32(acc[nt], a, b);
+        for (int np = 0; np < NT / 2; np++) {
+          const uint4 bb = *reinterpret_cast<const uint4*>(F + ((kb * (NT / 2) + np) * 32 + lane) * 4);
+          const unsigned b0[2] = {bb.x, bb.y}, b1[2] = {bb.z, bb.w};
+          mma_tf32(acc[2 * np], a, b0);
+          mma_tf32(acc[2 * np + 1], a, b1);
+        }
+      } else {
+        const uint2 bb = *reinterpret_cast<const uint2*>(F + (kb * 32 + lane) * 2);
+        const unsigned b0[2] = {bb.x, bb.y};
+        mma_tf32(acc[0], a, b0);
       }
     }
     __syncwarp();
@@ -291,9 +323,9 @@ __device__ __forceinline__ void mlp_forward_tc(const MlpTC& T, float* stage, con
 #pragma unroll
   for (int i = 0; i < MLP_IN; i++) row[i] = x[i];
   __syncwarp();
-  mlp_tc_layer<MLP_IN, MLP_H / 8, true>(stage, T.w1, T.b1, stage, lane);
-  mlp_tc_layer<MLP_H, MLP_H / 8, true>(stage, T.w2, T.b2, stage, lane);
-  mlp_tc_layer<MLP_H, 1, false>(stage, T.w3, T.b3, stage, lane);
+  mlp_tc_layer<MLP_IN, MLP_H / 8, true>(stage, T.f1, T.b1, stage, lane);
+  mlp_tc_layer<MLP_H, MLP_H / 8, true>(stage, T.f2, T.b2, stage, lane);
+  mlp_tc_layer<MLP_H, 1, false>(stage, T.f3, T.b3, stage, lane);
 #pragma unroll
   for (int i = 0; i < MLP_OUT; i++) y[i] = row[i];
   __syncwarp();
@@ -337,76 +369,75 @@ __device__ __forceinline__ bool rx_surrogate(const MlpW& W, const RxConst& k, in
 namespace csp {
 
 // ---- deployment: the reaction increments of a reaction step, after the voxel kernel
-// (run with its reaction switched off) and the boundary kernels.  One thread per voxel;
-// blockIdx.y = realisation.  Reads the old state, adds into the new one; species fixed
-// in the voxel's domain and, with -f, species 0 on the outer faces keep the values the
-// voxel kernel gave them.  The network runs on the tensor cores for a whole warp when
-// any of its voxels needs it.  counters[0] += voxels, counters[1] += voxels the network
-// ran for, counters[2] += voxels that took the plain integrator.
+// (run with its reaction switched off) and the boundary kernels; on other steps the
+// launches return at once.  Reads the old state and adds into the new one; species fixed
+// in the voxel's domain and, with -f, Ca on the outer faces keep the values the voxel
+// kernel gave them.
+//
+// k_react_surrogate streams the fields: a CTA takes MLP_DEPLOY_SPAN consecutive voxels
+// of one realisation (blockIdx.y); a thread takes groups of 4 consecutive voxels (16-byte
+// loads and stores of the species that the group's domains react: a warp moves 512
+// contiguous bytes per species).  A group lies in one plane (planes are padded to
+// multiples of 128 voxels) and a warp's 128 voxels are all inside the field or all
+// outside, so warp-wide steps stay convergent.  Voxels near equilibrium are finished in
+// their group; voxels of stiff domains are queued in a per-warp ring of shared memory and
+// take the plain integrator (FP64) 32 at a time, one per lane, after their group's store
+// (re-read by a lane of the same warp); voxels that need the network are listed per CTA
+// (offsets within its span) for k_react_network, which runs the network on the tensor
+// cores for tiles of 32 listed voxels.  counters[0] += voxels, counters[1] += voxels the
+// network ran for, counters[2] += voxels that took the plain integrator.
 constexpr int MLP_DEPLOY_T = 256;
-constexpr int MLP_DEPLOY_VPT = 128;      // voxels per thread (grid-stride within the realisation)
-constexpr size_t MLP_DEPLOY_SMEM = sizeof(MlpTC) + sizeof(float) * (size_t)MLP_TC_STAGE * (MLP_DEPLOY_T / 32);
+constexpr int MLP_DEPLOY_ITER = 16;      // groups of 4 voxels per thread
+constexpr long long MLP_DEPLOY_SPAN = 4ll * MLP_DEPLOY_T * MLP_DEPLOY_ITER;   // voxels per CTA
+static_assert(MLP_DEPLOY_SPAN <= 65536, "list entries are 16-bit offsets within a CTA's span");
+constexpr int MLP_RX_NS = MLP_SLOTS + 1; // species the reaction touches: Ca and slots 1..5
+constexpr unsigned MLP_RING = 256;       // ring entries (a power of two; at most 159 are held)
+constexpr size_t MLP_NETWORK_SMEM = sizeof(MlpTC) + sizeof(float) * (size_t)MLP_TC_STAGE * (MLP_DEPLOY_T / 32);
 
-// One voxel's reaction inputs and the new values they are added to.
-struct RxVoxel {
-  int d;                       // domain
-  bool mine;                   // in the grid and in a domain with buffers
-  float c, b[MLP_SLOTS];       // old Ca and buffers
-  float nc, nb[MLP_SLOTS];     // new Ca and buffers (after diffusion and boundary fluxes)
+enum : unsigned { RX_NONE = 0, RX_ELIGIBLE = 1, RX_STIFF = 2 };
+
+// The reaction constants of one domain, block-shared.
+struct RxDom {
+  RxConst k;
+  float thr[MLP_SLOTS];                  // near-equilibrium thresholds (rx_near_equilibrium)
+  float base[MLP_RX_NS], qunit[MLP_RX_NS], qinv[MLP_RX_NS];   // RealDesc::fbase / qunit / qinv
+  unsigned kind;                         // RX_NONE: no buffers; RX_ELIGIBLE: network domain; RX_STIFF
+  unsigned load;                         // species the reaction reads: Ca and the domain's buffers
+  unsigned store;                        // species it writes: load minus the domain's fixed species
 };
 
-// p = v mod D.P (the position within the plane), tracked by the caller; uo / un = the
-// old / new buffer of every species, dom = the domain bytes, base = the fields' bases
-// (RealDesc::fbase; block-shared copies).  The old values are reconstructed (base plus
-// stored deviation) for the network and the integrators; the new values stay deviations,
-// which the increments are added to.
-__device__ __forceinline__ void rx_fetch(const float* const* uo, const float* const* un,
-                                         const unsigned char* __restrict__ dom, int plane, const RxConst* sk,
-                                         const float (*base)[NS], unsigned fixq, const float (*qunit)[NS], long long v,
-                                         int p, long long nvox, RxVoxel& X) {
-  X.mine = false;
-  X.d = 0;
-  X.c = X.nc = 0.f;
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) X.b[q] = X.nb[q] = 0.f;
-  if (v >= nvox || p >= plane) return;
-  X.d = dom[v] & DOMAIN_BITS;
-  const RxConst& kc = sk[X.d];
-  bool any = false;
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) any = any || kc.tot[q] > 0.f;
-  if (!any) return;
-  X.mine = true;
-  X.c = __fadd_rn(base[X.d][0], uo[0][v]);
-  X.nc = un[0][v];
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) {
-    if (kc.tot[q] > 0.f) {
-      const float o = uo[q + 1][v];
-      X.b[q] = __fadd_rn(base[X.d][q + 1], (fixq >> (q + 1) & 1u) ? q_value(o, qunit[X.d][q + 1]) : o);
-      X.nb[q] = un[q + 1][v];     // stored form (an integer for fixed-point species)
-    }
-  }
+// Old value of species s: base plus the stored deviation (fixed-point for the species in
+// FQ & fqs).
+template <unsigned FQ>
+__device__ __forceinline__ float rx_old(const RxDom& K, int s, float stored, unsigned fqs) {
+  return __fadd_rn(K.base[s], ((FQ & fqs) >> s & 1u) ? q_value(stored, K.qunit[s]) : stored);
+}
+
+// Stored new value of species s plus an increment.
+template <unsigned FQ>
+__device__ __forceinline__ float rx_add(const RxDom& K, int s, float stored, float inc, unsigned fqs) {
+  return ((FQ & fqs) >> s & 1u) ? q_add(stored, inc, K.qinv[s]) : __fadd_rn(stored, inc);
 }
 
 // Near equilibrium (every S_s <= MLP_SKIP), with S_s <= MLP_SKIP tested as
 // lam |g| + k_on (tot - b) |G| <= thr_s, thr_s = MLP_SKIP tot_s / (dt_r^2 / 2) (no division).
-// g[] receives the reaction rates g_s (0 for absent buffers) for the explicit increment.
+// g[] receives the reaction rates g_s for the explicit increment.  Absent buffers (k_on =
+// k_off = tot = thr = 0, b = 0) give g = 0 and a term 0 <= 0, so every slot is evaluated
+// without a branch.
 __device__ __forceinline__ bool rx_near_equilibrium(const RxConst& k, const float* thr, float c, const float* b,
                                                     float* g) {
   float G = 0.f;
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
-    g[q] = k.tot[q] > 0.f ? rx_g<float>(k, q, c, b[q]) : 0.f;
+    g[q] = rx_g<float>(k, q, c, b[q]);
     G += g[q];
   }
   const float aG = fabsf(G);
   bool near = true;
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
-    if (k.tot[q] <= 0.f) continue;
     const float lam = k.koff[q] + k.kon[q] * c;
-    near = near && lam * fabsf(g[q]) + k.kon[q] * (k.tot[q] - b[q]) * aG <= thr[q];
+    near &= lam * fabsf(g[q]) + k.kon[q] * (k.tot[q] - b[q]) * aG <= thr[q];
   }
   return near;
 }
@@ -421,184 +452,416 @@ __device__ __forceinline__ void rx_fallback(const RxConst& kc, int n, double dt,
   dc = (float)dcd;
 }
 
-// New values of one voxel: its buffers and Ca plus the increments, except fixed species
-// and, with Dirichlet faces (-f), Ca on the outer faces.
-// fm = the domain's fixed-species mask (RealDesc::fixed_mask).
-__device__ __forceinline__ void rx_store(unsigned fm, const float* const* un, const RxConst& kc, long long v,
-                                         bool face, float nc, const float* nb, float dc, const float* db,
-                                         unsigned fixq, const float* qinv) {
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) {
-    const int s = q + 1;
-    if (kc.tot[q] <= 0.f || (fm >> s & 1u)) continue;
-    const_cast<float*>(un[s])[v] = (fixq >> s & 1u) ? q_add(nb[q], db[q], qinv[s]) : __fadd_rn(nb[q], db[q]);
-  }
-  if (!(fm & 1u) && !face) const_cast<float*>(un[0])[v] = __fadd_rn(nc, dc);
-}
-
 __device__ __forceinline__ bool rx_on_face(const RealDesc& D, int x, int p) {
   const int c1 = p / D.nz, c2 = p - c1 * D.nz;
   return x == 0 || x == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
 }
 
-// Each thread walks MLP_DEPLOY_VPT voxels, the next voxel's values loaded before the
-// current one is worked on.  Voxels near equilibrium and voxels of stiff domains are
-// finished at once; voxels that need the network are queued per warp (their indices in
-// shared memory) and the network runs on full tiles of 32 queued voxels, which reload
-// their state: the tensor-core passes carry no idle lanes but the last one.
+// Voxel j of a group in an eligible domain (o / nw: old / new stored values of the group's
+// species): near equilibrium, the explicit increment is added into nw and the result is
+// true; otherwise nw is left alone (the voxel needs the network).  LM != 0: the domain's
+// load and store masks are both LM (bit 0 Ca, bit q+1 slot q), known at compile time, so
+// absent slots cost nothing; LM = 0: any domain (masks read from K).
+template <unsigned FQ, unsigned LM>
+__device__ __forceinline__ bool rx_group_voxel(const RxDom& K, float dtr, unsigned fqs,
+                                               const float (&o)[MLP_RX_NS][4], float (&nw)[MLP_RX_NS][4], int j,
+                                               bool face) {
+  auto present = [&](int q) { return LM ? ((LM >> (q + 1)) & 1u) != 0u : K.k.tot[q] > 0.f; };
+  auto stored = [&](int s) { return LM ? ((LM >> s) & 1u) != 0u : ((K.store >> s) & 1u) != 0u; };
+  const float c = rx_old<FQ>(K, 0, o[0][j], fqs);
+  float b[MLP_SLOTS], g[MLP_SLOTS];
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) b[q] = present(q) ? rx_old<FQ>(K, q + 1, o[q + 1][j], fqs) : 0.f;
+  // rx_near_equilibrium restricted to the present slots (absent ones add exact zeros there)
+  float G = 0.f;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    g[q] = 0.f;
+    if (!LM || present(q)) {
+      g[q] = rx_g<float>(K.k, q, c, b[q]);
+      G += g[q];
+    }
+  }
+  const float aG = fabsf(G);
+  bool near = true;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (LM && !present(q)) continue;
+    const float lam = K.k.koff[q] + K.k.kon[q] * c;
+    near &= lam * fabsf(g[q]) + K.k.kon[q] * (K.k.tot[q] - b[q]) * aG <= K.thr[q];
+  }
+  if (!near) return false;
+  float sdb = 0.f;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (LM && !present(q)) continue;
+    const float db = dtr * g[q];
+    sdb += db;
+    if (stored(q + 1)) nw[q + 1][j] = rx_add<FQ>(K, q + 1, nw[q + 1][j], db, fqs);
+  }
+  if (stored(0) && !face) nw[0][j] = __fadd_rn(nw[0][j], -sdb);
+  return true;
+}
+
+// The compile-time layout of rx_group_voxel: Ca and the first four buffer slots, none of
+// them fixed (the reference's cytosolic buffers CMDN, ATP, Fluo, TRPN after Ca).
+constexpr unsigned MLP_LM_CYTOSOL = 0x1Fu;
+
+// Reaction step of realisation r (the condition both deployment kernels test).
+__device__ __forceinline__ bool rx_active(const RealDesc& D, const RealCtl& C) {
+  return !C.stopped && D.react_external && D.nbuf > 0 && (C.step + 1) % D.reaction_substep == 0;
+}
+
+// list / counts: per CTA (seg = blockIdx.y * gridDim.x + blockIdx.x) MLP_DEPLOY_SPAN
+// entries and the number used, written on reaction steps; tiles / queue[0]: the tiles of
+// 32 listed voxels (seg << MLP_TILE_BITS | tile within the list) and their number.
+constexpr int MLP_TILE_BITS = 9;
+static_assert(MLP_DEPLOY_SPAN / 32 <= (1 << MLP_TILE_BITS), "tile index field");
+template <unsigned FQ>
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
                                                                   const RealCtl* __restrict__ ctl,
-                                                                  const float* __restrict__ params, float tol,
+                                                                  unsigned short* __restrict__ list,
+                                                                  unsigned* __restrict__ counts,
+                                                                  unsigned* __restrict__ tiles,
+                                                                  unsigned* __restrict__ queue,
                                                                   unsigned long long* __restrict__ counters) {
-  extern __shared__ __align__(16) float dsm[];
-  MlpTC& T = *reinterpret_cast<MlpTC*>(dsm);
-  float* stage = dsm + sizeof(MlpTC) / sizeof(float) + (threadIdx.x >> 5) * MLP_TC_STAGE;
-  __shared__ RxConst sk[ND];
-  __shared__ float s_thr[ND][MLP_SLOTS];
-  __shared__ unsigned s_fm[ND];
-  __shared__ float s_base[ND][NS];
-  __shared__ float s_qunit[ND][NS], s_qinv[ND][NS];
-  __shared__ const float* s_uo[NS];
-  __shared__ const float* s_un[NS];
-  __shared__ long long s_pend[MLP_DEPLOY_T / 32][64];   // per warp: queued voxels (up to two tiles)
-  __shared__ unsigned s_vox, s_net, s_fall;
+  __shared__ RxDom s_dom[8];                 // by domain id (DOMAIN_BITS); entries >= nd: RX_NONE
+  __shared__ const float* s_uo[MLP_RX_NS];
+  __shared__ float* s_un[MLP_RX_NS];
+  __shared__ unsigned s_ring[MLP_DEPLOY_T / 32][MLP_RING];   // per warp: plain-integrator voxels
+  __shared__ unsigned s_vox, s_fall, s_list, s_tile0;
   const RealDesc& D = descs[blockIdx.y];
   const RealCtl& C = ctl[blockIdx.y];
-  const long long k = C.step, ti = k + 1;
-  const bool active = !C.stopped && D.react_external && D.nbuf > 0 && ti % D.reaction_substep == 0;
-  if (!active) return;                              // uniform over the block
+  if (!rx_active(D, C)) return;                         // uniform over the block
+  const long long seg = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+  const long long k = C.step;
   const long long nvox = (long long)D.nx * D.P;
-  const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
-  if ((long long)blockIdx.x * span >= nvox) return;  // uniform over the block
+  const long long vb0 = (long long)blockIdx.x * MLP_DEPLOY_SPAN;
+  if (vb0 >= nvox) {                                    // uniform over the block
+    if (threadIdx.x == 0) counts[seg] = 0;
+    return;
+  }
+  unsigned short* seg_list = list + seg * MLP_DEPLOY_SPAN;
   const unsigned cur = C.cur_mask[k & 1];
   const float dtr = (float)(D.dt * D.reaction_substep);
-  mlp_tc_load(T, params);
-  if (threadIdx.x < ND) {
-    const RxConst kc = rx_const(D, threadIdx.x < D.nd ? threadIdx.x : 0);
-    sk[threadIdx.x] = kc;
-    for (int q = 0; q < MLP_SLOTS; q++) s_thr[threadIdx.x][q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
-    s_fm[threadIdx.x] = D.fixed_mask[threadIdx.x < D.nd ? threadIdx.x : 0];
-    for (int s = 0; s < NS; s++) {
-      s_base[threadIdx.x][s] = D.fbase[threadIdx.x][s];
-      s_qunit[threadIdx.x][s] = D.qunit[threadIdx.x][s];
-      s_qinv[threadIdx.x][s] = D.qinv[threadIdx.x][s];
+  if (threadIdx.x < 8) {
+    const int d = threadIdx.x;
+    RxDom& S = s_dom[d];
+    const RxConst kc = rx_const(D, d < D.nd ? d : 0);
+    unsigned ld = 0;
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      S.thr[q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
+      if (kc.tot[q] > 0.f) ld |= 2u << q;
     }
+    S.k = kc;
+    for (int s = 0; s < MLP_RX_NS; s++) {
+      S.base[s] = D.fbase[d < D.nd ? d : 0][s];
+      S.qunit[s] = D.qunit[d < D.nd ? d : 0][s];
+      S.qinv[s] = D.qinv[d < D.nd ? d : 0][s];
+    }
+    const bool any = d < D.nd && ld != 0;
+    S.kind = !any ? RX_NONE : ((D.mlp_domains >> d) & 1u) ? RX_ELIGIBLE : RX_STIFF;
+    S.load = any ? (ld | 1u) : 0u;
+    S.store = S.load & ~(unsigned)D.fixed_mask[d < D.nd ? d : 0];
   }
-  if (threadIdx.x < NS) {
+  if (threadIdx.x < MLP_RX_NS) {
     const int t = threadIdx.x;
-    s_uo[t] = D.u[(cur >> t) & 1u][t];
-    s_un[t] = D.u[((cur >> t) & 1u) ^ 1u][t];
+    s_uo[t] = t < D.ns ? D.u[(cur >> t) & 1u][t] : nullptr;
+    s_un[t] = t < D.ns ? D.u[((cur >> t) & 1u) ^ 1u][t] : nullptr;
   }
-  if (threadIdx.x == 0) { s_vox = 0; s_net = 0; s_fall = 0; }
+  if (threadIdx.x == 0) { s_vox = 0; s_fall = 0; s_list = 0; }
   __syncthreads();
   const unsigned char* __restrict__ dom = D.dom;
-  const int plane = D.plane;
-  const unsigned elig_mask = D.mlp_domains;
+  const int plane = D.plane, P = D.P;
   const bool dirichlet = D.dirichlet != 0;
-  const unsigned fixq = D.fixq;
-  unsigned n_vox = 0, n_net = 0, n_fall = 0;
-  const long long v0 = (long long)blockIdx.x * span + threadIdx.x;
-  // position within the plane and plane index of the voxel being fetched, advanced by
-  // MLP_DEPLOY_T per iteration without divisions (one at the start)
-  const int P = D.P;
-  int pf = (int)(v0 % P), xf = (int)(v0 / P);
-  int pc = pf, xc = xf;
-  long long* pend = s_pend[threadIdx.x >> 5];
+  const unsigned fqs = D.fixq;
   const int lane = threadIdx.x & 31;
-  int npend = 0;                                     // warp-uniform
-  // the network on queued voxels pend[0 .. count) (lane i takes pend[i]), whole warp
-  auto flush = [&](int count) {
-    __syncwarp();
-    const bool have = lane < count;
-    const long long v = have ? pend[lane] : 0;
-    RxVoxel Y;
-    int pq = 0, xq = 0;
-    if (have) {
-      xq = (int)(v / P);
-      pq = (int)(v - (long long)xq * P);
-    }
-    rx_fetch(s_uo, s_un, dom, plane, sk, s_base, fixq, s_qunit, have ? v : nvox, pq, nvox, Y);
-    const RxConst& kc = sk[Y.d];
-    float x[MLP_IN], t[MLP_OUT], db[MLP_SLOTS], dc = 0.f;
-    if (have) rx_features(kc, Y.d, dtr, Y.c, Y.b, x);
-    else
-      for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
-    mlp_forward_tc(T, stage, x, t);
-    if (have) {
-      n_vox++;
-      n_net++;
-      if (!rx_apply_output(kc, dtr, Y.c, Y.b, t, tol, dc, db)) {
-        n_fall++;
-        rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned* ring_fall = s_ring[threadIdx.x >> 5];
+  unsigned hf = 0, tf = 0;                             // ring head / tail (warp-uniform)
+  unsigned n_vox = 0, n_fall = 0;
+  // one queued voxel: old values reconstructed, new values as stored
+  auto load1 = [&](long long vv, const RxDom& K, float& c, float* b, float& nc, float* nb) {
+    c = rx_old<FQ>(K, 0, __ldg(s_uo[0] + vv), fqs);
+    nc = s_un[0][vv];
+#pragma unroll
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      b[q] = nb[q] = 0.f;
+      if (K.k.tot[q] > 0.f) {
+        b[q] = rx_old<FQ>(K, q + 1, __ldg(s_uo[q + 1] + vv), fqs);
+        nb[q] = s_un[q + 1][vv];
       }
-      rx_store(s_fm[Y.d], s_un, kc, v, dirichlet && rx_on_face(D, xq, pq), Y.nc, Y.nb, dc, db, fixq, s_qinv[Y.d]);
+    }
+  };
+  auto store1 = [&](long long vv, const RxDom& K, float nc, const float* nb, float dc, const float* db) {
+#pragma unroll
+    for (int q = 0; q < MLP_SLOTS; q++)
+      if (K.store >> (q + 1) & 1u) s_un[q + 1][vv] = rx_add<FQ>(K, q + 1, nb[q], db[q], fqs);
+    if (K.store & 1u) {
+      const int vi = (int)vv, xq = vi / P;
+      if (!(dirichlet && rx_on_face(D, xq, vi - xq * P))) s_un[0][vv] = __fadd_rn(nc, dc);
+    }
+  };
+  // the plain integrator on ring_fall's next cnt voxels, one per lane
+  auto flush_fall = [&](unsigned cnt) {
+    __syncwarp();
+    const bool have = lane < cnt;
+    const unsigned off = have ? ring_fall[(hf + lane) & (MLP_RING - 1)] : 0u;
+    hf += cnt;
+    if (have) {
+      const long long vv = vb0 + off;
+      const RxDom& K = s_dom[dom[vv] & DOMAIN_BITS];
+      float c, nc, b[MLP_SLOTS], nb[MLP_SLOTS], dc, db[MLP_SLOTS];
+      load1(vv, K, c, b, nc, nb);
+      n_fall++;
+      rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
+      store1(vv, K, nc, nb, dc, db);
     }
     __syncwarp();
   };
-  RxVoxel X;
-  rx_fetch(s_uo, s_un, dom, plane, sk, s_base, fixq, s_qunit, v0, pf, nvox, X);
-  for (int it = 0; it < MLP_DEPLOY_VPT; it++) {
-    const long long v = v0 + (long long)it * MLP_DEPLOY_T;
-    const RxVoxel Y = X;
-    pc = pf;
-    xc = xf;
-    pf += MLP_DEPLOY_T;
-    while (pf >= P) { pf -= P; xf++; }
-    if (it + 1 < MLP_DEPLOY_VPT) rx_fetch(s_uo, s_un, dom, plane, sk, s_base, fixq, s_qunit, v + MLP_DEPLOY_T, pf, nvox, X);
-    const int d = Y.d;
-    const RxConst& kc = sk[d];
-    bool elig = false, skip = false;
-    float g[MLP_SLOTS];
-    if (Y.mine) {
-      elig = (elig_mask >> d) & 1u;
-      skip = elig && rx_near_equilibrium(kc, s_thr[d], Y.c, Y.b, g);
-    }
-    const bool net = Y.mine && elig && !skip;
-    if (Y.mine && !net) {
-      float db[MLP_SLOTS], dc;
-      n_vox++;
-      if (skip) {
-        // near equilibrium: the explicit increment
-        float sdb = 0.f;
-        for (int q = 0; q < MLP_SLOTS; q++) {
-          db[q] = kc.tot[q] > 0.f ? dtr * g[q] : 0.f;
-          sdb += db[q];
-        }
-        dc = -sdb;
-      } else {
-        // a stiff domain: the plain integrator
-        n_fall++;
-        rx_fallback(kc, D.reaction_substep, D.dt, Y.c, Y.b, dc, db);
+  long long v = vb0 + 4 * threadIdx.x;
+  int p = (int)(v % P), x = (int)(v / P);              // in-plane position and plane of voxel v
+  for (int it = 0;; it++) {
+    const bool live = v < nvox;                          // warp-uniform
+    if (live) {
+      const unsigned w4 = __ldg(reinterpret_cast<const unsigned*>(dom + v));   // 4 domain bytes
+      int dj[4];
+      unsigned need = 0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        dj[j] = p + j < plane ? (int)((w4 >> (8 * j)) & DOMAIN_BITS) : 7;
+        need |= s_dom[dj[j]].load;
       }
-      rx_store(s_fm[d], s_un, kc, v, dirichlet && rx_on_face(D, xc, pc), Y.nc, Y.nb, dc, db, fixq, s_qinv[d]);
+      float o[MLP_RX_NS][4], nw[MLP_RX_NS][4];
+#pragma unroll
+      for (int s = 0; s < MLP_RX_NS; s++) {
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+        if (need >> s & 1u) {
+          a = __ldg(reinterpret_cast<const float4*>(s_uo[s] + v));
+          b = *reinterpret_cast<const float4*>(s_un[s] + v);
+        }
+        o[s][0] = a.x; o[s][1] = a.y; o[s][2] = a.z; o[s][3] = a.w;
+        nw[s][0] = b.x; nw[s][1] = b.y; nw[s][2] = b.z; nw[s][3] = b.w;
+      }
+      bool face[4] = {false, false, false, false};
+      if (dirichlet)
+#pragma unroll
+        for (int j = 0; j < 4; j++) face[j] = rx_on_face(D, x, p + j);
+      // r: 0 no buffers, 1 finished (explicit increment), 2 network, 3 plain integrator
+      int r[4];
+      unsigned upd = 0;
+      if (dj[0] == dj[1] && dj[0] == dj[2] && dj[0] == dj[3]) {
+        const RxDom K = s_dom[dj[0]];                    // one domain: its constants in registers
+        if (K.kind == RX_ELIGIBLE && K.load == MLP_LM_CYTOSOL && K.store == MLP_LM_CYTOSOL) {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            r[j] = rx_group_voxel<FQ, MLP_LM_CYTOSOL>(K, dtr, fqs, o, nw, j, face[j]) ? 1 : 2;
+          upd = K.store;
+        } else if (K.kind == RX_ELIGIBLE) {
+#pragma unroll
+          for (int j = 0; j < 4; j++) r[j] = rx_group_voxel<FQ, 0u>(K, dtr, fqs, o, nw, j, face[j]) ? 1 : 2;
+          upd = K.store;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++) r[j] = K.kind == RX_STIFF ? 3 : 0;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const RxDom& K = s_dom[dj[j]];
+          r[j] = K.kind == RX_STIFF ? 3 : 0;
+          if (K.kind == RX_ELIGIBLE) {
+            r[j] = rx_group_voxel<FQ, 0u>(K, dtr, fqs, o, nw, j, face[j]) ? 1 : 2;
+            if (r[j] == 1) upd |= K.store;
+          }
+        }
+      }
+      unsigned mnet = 0, mfall = 0;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (r[j]) n_vox++;
+        if (r[j] == 2) mnet |= 1u << j;
+        if (r[j] == 3) mfall |= 1u << j;
+      }
+#pragma unroll
+      for (int s = 0; s < MLP_RX_NS; s++)
+        if (upd >> s & 1u)
+          *reinterpret_cast<float4*>(s_un[s] + v) = make_float4(nw[s][0], nw[s][1], nw[s][2], nw[s][3]);
+      const unsigned off = (unsigned)(v - vb0);
+      if (__any_sync(0xffffffffu, mnet != 0u)) {
+        // this CTA's network list: a warp-wide prefix sum of the counts, one shared atomic
+        const unsigned cnt = __popc(mnet);
+        unsigned incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        unsigned base = 0;
+        if (lane == 31) base = atomicAdd(&s_list, incl);
+        unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (mnet >> j & 1u) seg_list[pos++] = (unsigned short)(off + j);
+      }
+      if (__any_sync(0xffffffffu, mfall != 0u))
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const unsigned bal = __ballot_sync(0xffffffffu, mfall >> j & 1u);
+          if (mfall >> j & 1u) ring_fall[(tf + __popc(bal & lt)) & (MLP_RING - 1)] = off + j;
+          tf += __popc(bal);
+        }
     }
-    const unsigned nm = __ballot_sync(0xffffffffu, net);
-    if (net) pend[npend + __popc(nm & ((1u << lane) - 1u))] = v;
-    npend += __popc(nm);
-    // full tiles, and after the last voxel whatever is queued (one call site)
-    while (npend >= 32 || (npend > 0 && it == MLP_DEPLOY_VPT - 1)) {
-      const int cnt = min(npend, 32);
-      flush(cnt);
-      const int rest = npend - cnt;
-      const long long mv = lane < rest ? pend[32 + lane] : 0;
-      __syncwarp();
-      if (lane < rest) pend[lane] = mv;
-      __syncwarp();
-      npend = rest;
-    }
+    const bool last = !live || it == MLP_DEPLOY_ITER - 1 || v + 4 * MLP_DEPLOY_T >= nvox;   // warp-uniform
+    // full warps of queued voxels (the ring never holds more than 31 + 128), and after
+    // the last group whatever is queued
+    while (tf - hf >= 32u || (last && tf != hf)) flush_fall(min(tf - hf, 32u));
+    if (last) break;
+    v += 4 * MLP_DEPLOY_T;
+    p += 4 * MLP_DEPLOY_T;
+    while (p >= P) { p -= P; x++; }
   }
   if (n_vox) atomicAdd(&s_vox, n_vox);
-  if (n_net) atomicAdd(&s_net, n_net);
   if (n_fall) atomicAdd(&s_fall, n_fall);
   __syncthreads();
-  if (threadIdx.x == 0 && s_vox) {
-    atomicAdd(&counters[0], (unsigned long long)s_vox);
-    atomicAdd(&counters[1], (unsigned long long)s_net);
-    atomicAdd(&counters[2], (unsigned long long)s_fall);
+  const unsigned ntile = (s_list + 31u) / 32u;
+  if (threadIdx.x == 0) {
+    counts[seg] = s_list;
+    if (ntile) s_tile0 = atomicAdd(&queue[0], ntile);
+    if (s_vox) atomicAdd(&counters[0], (unsigned long long)s_vox);
+    if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
+  }
+  __syncthreads();
+  for (unsigned j = threadIdx.x; j < ntile; j += MLP_DEPLOY_T)
+    tiles[s_tile0 + j] = (unsigned)seg << MLP_TILE_BITS | j;
+}
+
+// The network voxels that k_react_surrogate listed, in tiles of 32 on the tensor cores (a
+// rejected output takes the plain integrator).  Persistent CTAs: warp w of the grid takes
+// a contiguous range of the queued tiles (tiles of one list are queued together, so a
+// warp's realisation rarely changes; its domain constants and field pointers are cached
+// per warp in shared memory); a CTA without a tile returns before it loads the weights.
+// The last CTA to finish empties the queue (queue[0]: tiles, queue[1]: CTAs done) for the
+// next step.  chunks = k_react_surrogate's gridDim.x.
+template <unsigned FQ>
+__global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDesc* __restrict__ descs,
+                                                                   const RealCtl* __restrict__ ctl,
+                                                                   const float* __restrict__ params, float tol,
+                                                                   const unsigned short* __restrict__ list,
+                                                                   const unsigned* __restrict__ counts,
+                                                                   const unsigned* __restrict__ tiles,
+                                                                   unsigned* __restrict__ queue, int chunks,
+                                                                   unsigned long long* __restrict__ counters) {
+  extern __shared__ __align__(16) float dsm[];
+  MlpTC& T = *reinterpret_cast<MlpTC*>(dsm);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* stage = dsm + sizeof(MlpTC) / sizeof(float) + warp * MLP_TC_STAGE;
+  __shared__ RxDom s_dom[MLP_DEPLOY_T / 32][8];        // per warp: the constants of its realisation
+  __shared__ const float* s_uo[MLP_DEPLOY_T / 32][MLP_RX_NS];
+  __shared__ float* s_un[MLP_DEPLOY_T / 32][MLP_RX_NS];
+  __shared__ unsigned s_net, s_fall, s_total;
+  if (threadIdx.x == 0) { s_total = queue[0]; s_net = 0; s_fall = 0; }
+  __syncthreads();
+  const unsigned total = s_total;
+  const unsigned nw = gridDim.x * (MLP_DEPLOY_T / 32), per = (total + nw - 1) / nw;
+  if (blockIdx.x * (MLP_DEPLOY_T / 32) * per < total) {  // uniform over the block
+    mlp_tc_load(T, params);
+    __syncthreads();
+    const unsigned w0 = blockIdx.x * (MLP_DEPLOY_T / 32) + warp;
+    const unsigned t_lo = w0 * per, t_hi = min(total, t_lo + per);
+    unsigned n_net = 0, n_fall = 0;
+    int rc = -1;                                         // realisation whose constants are cached
+    for (unsigned tw = t_lo; tw < t_hi; tw++) {
+      const unsigned td = tiles[tw];
+      const long long seg = td >> MLP_TILE_BITS;
+      const unsigned t0 = (td & ((1u << MLP_TILE_BITS) - 1u)) * 32u;
+      const int r = (int)(seg / chunks);
+      const RealDesc& D = descs[r];
+      if (r != rc) {                                     // warp-uniform
+        __syncwarp();
+        if (lane < 8) {
+          const int d = lane < D.nd ? lane : 0;
+          RxDom& S = s_dom[warp][lane];
+          S.k = rx_const(D, d);
+          unsigned ld = 0;
+          for (int q = 0; q < MLP_SLOTS; q++)
+            if (S.k.tot[q] > 0.f) ld |= 2u << q;
+          for (int s = 0; s < MLP_RX_NS; s++) {
+            S.base[s] = D.fbase[d][s];
+            S.qunit[s] = D.qunit[d][s];
+            S.qinv[s] = D.qinv[d][s];
+          }
+          S.load = ld ? (ld | 1u) : 0u;
+          S.store = S.load & ~(unsigned)D.fixed_mask[d];
+        } else if (lane < 8 + MLP_RX_NS) {
+          const int t = lane - 8;
+          const unsigned cur = ctl[r].cur_mask[ctl[r].step & 1];
+          s_uo[warp][t] = t < D.ns ? D.u[(cur >> t) & 1u][t] : nullptr;
+          s_un[warp][t] = t < D.ns ? D.u[((cur >> t) & 1u) ^ 1u][t] : nullptr;
+        }
+        __syncwarp();
+        rc = r;
+      }
+      const unsigned cnt = counts[seg];
+      const long long vb0 = (seg - (long long)r * chunks) * MLP_DEPLOY_SPAN;
+      const float dtr = (float)(D.dt * D.reaction_substep);
+      const unsigned fqs = D.fixq;
+      const bool have = t0 + lane < cnt;
+      const long long v = vb0 + (have ? list[seg * MLP_DEPLOY_SPAN + t0 + lane] : 0);
+      const int d = have ? (D.dom[v] & DOMAIN_BITS) : 0;
+      const RxDom& K = s_dom[warp][d];
+      float c = 0.f, nc = 0.f, b[MLP_SLOTS], nb[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
+#pragma unroll
+      for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
+#pragma unroll
+      for (int q = 0; q < MLP_SLOTS; q++) b[q] = nb[q] = 0.f;
+      if (have) {
+        c = rx_old<FQ>(K, 0, __ldg(s_uo[warp][0] + v), fqs);
+        nc = s_un[warp][0][v];
+#pragma unroll
+        for (int q = 0; q < MLP_SLOTS; q++) {
+          if (K.k.tot[q] <= 0.f) continue;
+          b[q] = rx_old<FQ>(K, q + 1, __ldg(s_uo[warp][q + 1] + v), fqs);
+          nb[q] = s_un[warp][q + 1][v];
+        }
+        rx_features(K.k, d, dtr, c, b, x);
+      }
+      mlp_forward_tc(T, stage, x, t);
+      if (have) {
+        n_net++;
+        float dc, db[MLP_SLOTS];
+        if (!rx_apply_output(K.k, dtr, c, b, t, tol, dc, db)) {
+          n_fall++;
+          rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
+        }
+#pragma unroll
+        for (int q = 0; q < MLP_SLOTS; q++)
+          if (K.store >> (q + 1) & 1u) s_un[warp][q + 1][v] = rx_add<FQ>(K, q + 1, nb[q], db[q], fqs);
+        const int vi = (int)v, xq = vi / D.P;
+        if ((K.store & 1u) && !(D.dirichlet && rx_on_face(D, xq, vi - xq * D.P)))
+          s_un[warp][0][v] = __fadd_rn(nc, dc);
+      }
+    }
+    if (n_net) atomicAdd(&s_net, n_net);
+    if (n_fall) atomicAdd(&s_fall, n_fall);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_net) {
+      atomicAdd(&counters[1], (unsigned long long)s_net);
+      if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
+    }
+  }
+  if (threadIdx.x == 0) {
+    // every CTA has read queue[0] before it counts itself done
+    __threadfence();
+    if (atomicAdd(&queue[1], 1u) == gridDim.x - 1) {
+      queue[0] = 0;
+      queue[1] = 0;
+    }
   }
 }
 
-// Forward passes for checks: y[n][5] of x[n][8], FP32 (tc = 0) or tensor cores (tc = 1).
+// Forward passes for checks: y[n][5] of x[n][8], FP32 (tc = 0) or tensor cores (tc = 1,
+// the tiles of k_react_network).
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_mlp_forward(const float* __restrict__ params,
                                                               const float* __restrict__ x, long long n, int tc,
                                                               float* __restrict__ y) {
@@ -617,7 +880,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_mlp_forward(const float* __res
   if (i < n)
     for (int j = 0; j < MLP_OUT; j++) y[i * MLP_OUT + j] = yi[j];
 }
-constexpr size_t MLP_FORWARD_SMEM = MLP_DEPLOY_SMEM + sizeof(MlpW);
+constexpr size_t MLP_FORWARD_SMEM = MLP_NETWORK_SMEM + sizeof(MlpW);
 
 // ---- training ----
 

@@ -160,6 +160,7 @@ struct csp_handle {
   StepRec* d_rec = nullptr;          // per realisation: what its running step does
   int max_plane_vox = 0;
   long long max_vox = 0;
+  long long max_field = 0;           // max n0*P (padded planes)
   int kernel = 0;                 // 0 staged, 1 direct
   int inject_wait = 0;            // csp_test_wait_timeout armed (direct launches, no graph)
   // csp_set_phase_timing: the first steps of every advance call run as direct launches
@@ -180,8 +181,14 @@ struct csp_handle {
   // learned reaction surrogate (csp_set_surrogate)
   int surrogate = 0;
   float surrogate_tol = 1e-4f;
+  unsigned surrogate_fq = 0;         // k_react_surrogate<FQ> of the ensemble's fixed-point species
   float* d_mlp = nullptr;                   // MLP_NPARAM parameters
   unsigned long long* d_mlp_cnt = nullptr;  // voxels, network evaluations, fallbacks
+  unsigned short* d_sur_list = nullptr;     // per k_react_surrogate CTA: its network voxels
+  unsigned* d_sur_counts = nullptr;         // per k_react_surrogate CTA: listed voxels
+  unsigned* d_sur_tiles = nullptr;          // tiles of 32 listed voxels (k_react_network's work)
+  unsigned* d_sur_queue = nullptr;          // tiles queued, k_react_network CTAs done
+  int sur_network_ctas = 0;                 // persistent CTAs of k_react_network
   // training pairs harvested from the fields (csp_mlp_harvest): features [cap][8], targets [cap][5]
   float* d_hx = nullptr;
   float* d_ht = nullptr;
@@ -423,6 +430,7 @@ extern "C" int csp_create(const csp_model* models, const csp_options* options, i
     dom_total += hr0.field_elems;
     h->max_plane_vox = std::max(h->max_plane_vox, plane);
     h->max_vox = std::max(h->max_vox, (long long)n0 * plane);
+    h->max_field = std::max(h->max_field, (long long)n0 * P);
   }
   // -- device allocation (one arena for all fields) --
   cudaError_t e;
@@ -1060,12 +1068,27 @@ static void launch_channel_rows(csp_handle* h, int r0, int r1) {
                                                                         std::max(h->nch, 1));
 }
 
+// The surrogate instantiations for the fixed-point species of the ensemble (none, TRPN's
+// slot alone, or any slot).
+using SurrogateKernel = void (*)(const RealDesc*, const RealCtl*, unsigned short*, unsigned*, unsigned*, unsigned*,
+                                 unsigned long long*);
+using NetworkKernel = void (*)(const RealDesc*, const RealCtl*, const float*, float, const unsigned short*,
+                               const unsigned*, const unsigned*, unsigned*, int, unsigned long long*);
+static SurrogateKernel surrogate_kernel(unsigned fq) {
+  return fq == 0u ? k_react_surrogate<0u> : fq == 0x10u ? k_react_surrogate<0x10u> : k_react_surrogate<0x3Eu>;
+}
+static NetworkKernel network_kernel(unsigned fq) {
+  return fq == 0u ? k_react_network<0u> : fq == 0x10u ? k_react_network<0x10u> : k_react_network<0x3Eu>;
+}
+
 static void launch_surrogate(csp_handle* h, int r0, int r1) {
   if (!h->surrogate) return;
-  const long long span = (long long)MLP_DEPLOY_T * MLP_DEPLOY_VPT;
-  dim3 grid((unsigned)((h->max_vox + span - 1) / span), (unsigned)(r1 - r0));
-  k_react_surrogate<<<grid, MLP_DEPLOY_T, MLP_DEPLOY_SMEM, h->stream>>>(h->d_desc + r0, h->d_ctl + r0, h->d_mlp,
-                                                                        h->surrogate_tol, h->d_mlp_cnt);
+  const int chunks = (int)((h->max_field + MLP_DEPLOY_SPAN - 1) / MLP_DEPLOY_SPAN);
+  surrogate_kernel(h->surrogate_fq)<<<dim3((unsigned)chunks, (unsigned)(r1 - r0)), MLP_DEPLOY_T, 0, h->stream>>>(
+      h->d_desc + r0, h->d_ctl + r0, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles, h->d_sur_queue, h->d_mlp_cnt);
+  network_kernel(h->surrogate_fq)<<<h->sur_network_ctas, MLP_DEPLOY_T, MLP_NETWORK_SMEM, h->stream>>>(
+      h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
+      h->d_sur_queue, chunks, h->d_mlp_cnt);
 }
 
 static void launch_epilogue(csp_handle* h, int r0, int r1, int* step_flags) {
@@ -2023,13 +2046,28 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
     int rc = surrogate_supported(h);
     if (rc) return rc;
     if (!h->d_mlp) {
+      const long long chunks = (h->max_field + MLP_DEPLOY_SPAN - 1) / MLP_DEPLOY_SPAN;
       if (cudaMalloc(&h->d_mlp, MLP_NPARAM * sizeof(float)) != cudaSuccess ||
-          cudaMalloc(&h->d_mlp_cnt, 3 * sizeof(unsigned long long)) != cudaSuccess)
+          cudaMalloc(&h->d_mlp_cnt, 3 * sizeof(unsigned long long)) != cudaSuccess ||
+          cudaMalloc(&h->d_sur_list, (size_t)chunks * h->n * MLP_DEPLOY_SPAN * sizeof(unsigned short)) != cudaSuccess ||
+          cudaMalloc(&h->d_sur_counts, (size_t)chunks * h->n * sizeof(unsigned)) != cudaSuccess ||
+          cudaMalloc(&h->d_sur_tiles, (size_t)chunks * h->n * (MLP_DEPLOY_SPAN / 32) * sizeof(unsigned)) != cudaSuccess ||
+          cudaMalloc(&h->d_sur_queue, 2 * sizeof(unsigned)) != cudaSuccess)
         return fail(h, CSP_ENOMEM, "surrogate buffers");
+      if ((unsigned long long)chunks * h->n >= (1ull << (32 - MLP_TILE_BITS)))
+        return fail(h, CSP_ENOTSUP, "surrogate: more than 2^%d blocks of %lld voxels", 32 - MLP_TILE_BITS, MLP_DEPLOY_SPAN);
       CUDA_TRY(h, cudaMemsetAsync(h->d_mlp_cnt, 0, 3 * sizeof(unsigned long long), h->stream));
+      CUDA_TRY(h, cudaMemsetAsync(h->d_sur_queue, 0, 2 * sizeof(unsigned), h->stream));
+      int dev = 0, sms = 0;
+      CUDA_TRY(h, cudaGetDevice(&dev));
+      CUDA_TRY(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      h->sur_network_ctas = 2 * std::max(sms, 1);
     }
-    CUDA_TRY(h, cudaFuncSetAttribute(k_react_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)MLP_DEPLOY_SMEM));
+    unsigned fq = 0;
+    for (int r = 0; r < h->n; r++) fq |= h->real[r].desc.fixq & 0x3Eu;
+    h->surrogate_fq = fq == 0u ? 0u : fq == 0x10u ? 0x10u : 0x3Eu;
+    CUDA_TRY(h, cudaFuncSetAttribute(network_kernel(h->surrogate_fq), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)MLP_NETWORK_SMEM));
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     h->surrogate_tol = (float)tol;
   }
@@ -2337,7 +2375,8 @@ extern "C" void csp_destroy(csp_handle* h) {
   if (h->ev_snap) cudaEventDestroy(h->ev_snap);
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
-  cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt);
+  cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt); cudaFree(h->d_sur_list); cudaFree(h->d_sur_counts);
+  cudaFree(h->d_sur_tiles); cudaFree(h->d_sur_queue);
   cudaFree(h->d_hx); cudaFree(h->d_ht);
   for (auto& e : h->phase_ev)
     if (e) cudaEventDestroy(e);
