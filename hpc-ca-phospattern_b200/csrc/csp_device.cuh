@@ -23,6 +23,9 @@ constexpr int PLANE_ALIGN = 128;
 constexpr int DOMAIN_BITS = 7;      // domain id = domain byte & DOMAIN_BITS
 constexpr int CLASS_L = 1024;       // plane positions per chunk of the chunk class table
 constexpr unsigned char CLASS_MIXED = 0xff;
+// Surrogate domain kinds (RealDesc::sur_kind) and voxel classes (RealDesc::rx_class).
+enum : unsigned { RX_NONE = 0, RX_ELIGIBLE = 1, RX_STIFF = 2 };
+enum : unsigned { RX_CLASS_NONE = 0, RX_CLASS_EXPLICIT = 1, RX_CLASS_NETWORK = 2, RX_CLASS_PLAIN = 3 };
 
 enum FluxKind : int { FLUX_NONE = 0, FLUX_RYR = 1, FLUX_P_RYR = 2, FLUX_SERCA = 3 };
 
@@ -49,8 +52,17 @@ struct RealDesc {
   signed char dsi_of[NS];            // diffusive index of species s, or -1
   signed char rtab[ND][NS];          // fast reaction table: buffer index bi with bsp0 = s in domain d, or -1
   int react_fast;                    // every buffer binds species 0 and bound species are distinct per domain
-  int react_external;                // reaction increments come from the surrogate kernel (csp_mlp.cuh)
   unsigned mlp_domains;              // bit d: domain d's reactions are mild enough for the surrogate
+  // Reaction surrogate (csp_mlp.cuh).  With sur set, the voxel kernels also classify every
+  // voxel on a reaction step into rx_class (RX_CLASS_*) from the increments they apply:
+  // near equilibrium (the explicit increment stands), network, or plain integrator; the
+  // class scan then corrects the voxels of the last two classes.  For the buffer bound to
+  // s in d: sur_cs = tot - base_s, sur_thr2 = 2 MLP_SKIP tot (the near-equilibrium bound
+  // times dt_r^2); sur_kind[d] = RX_NONE / RX_ELIGIBLE / RX_STIFF.
+  int sur;
+  unsigned char* rx_class;           // [nx][P]; positions >= plane stay 0
+  float sur_cs[ND][NS], sur_thr2[ND][NS];
+  unsigned char sur_kind[ND];
   // Density-boundary fluxes evaluated inside the voxel kernels.  A voxel's domain byte
   // holds the domain id in bits 0-2 and a flux pattern index in bits 3-7 (0 = none).
   // fpat[pattern][k] for neighbour direction k: 0 = no flux, else (slot + 1), with bit 7

@@ -78,6 +78,12 @@ __device__ __forceinline__ F2 f2_fma(F2 a, F2 b, F2 c) {
   return r;
 }
 
+__device__ __forceinline__ F2 f2_abs(F2 a) {
+  F2 r;
+  r.v = a.v & 0x7fffffff7fffffffull;
+  return r;
+}
+
 // diffuse_uniform on two voxels: zs = z- + z+, ys, xs the other axis sums.
 __device__ __forceinline__ F2 diffuse_uniform2(F2 c, F2 m2, F2 u, F2 zs, F2 ys, F2 xs) {
   const F2 az = f2_fma(m2, u, zs), ay = f2_fma(m2, u, ys), ax = f2_fma(m2, u, xs);
@@ -130,7 +136,7 @@ __host__ __device__ inline StepInfo step_info(const RealDesc& D, long long time_
   StepInfo si;
   unsigned diffusing;
   step_masks(D, time_ind, si.pre, si.updated, diffusing);
-  si.react = (D.nbuf > 0 && time_ind % D.reaction_substep == 0 && !D.react_external) ? 1 : 0;
+  si.react = (D.nbuf > 0 && time_ind % D.reaction_substep == 0) ? 1 : 0;
   si.react_fast = (si.react && D.react_fast && (si.pre & 1u)) ? 1 : 0;
   return si;
 }
@@ -154,9 +160,44 @@ __device__ __forceinline__ double pair_flux(const RealDesc& D, int slot, double 
                                           : ryr_flux(D.dt, D.h, u0, u1, D.fslot_p[slot]);
 }
 
-template <int N, class LoadU, class LoadD>
+// Surrogate class of one voxel of domain d on a reaction step (RealDesc::sur) from the
+// increments the fast reactions apply (dJ_s = dt_r J_s, buffer_dj; ca = the voxel's Ca,
+// val = the stored deviations): the near-equilibrium test of the surrogate,
+// lam |g_s| + k_on (tot - b_s) |sum g| <= MLP_SKIP tot / (dt_r^2 / 2) for every bound s,
+// times dt_r^2: |kon_dt ca + koff_dt| |dJ_s| + kon_dt (tot - b_s) |sum dJ| <= sur_thr2.
+// The staged kernel's two-lane form rounds every step the same way.
+template <int N>
+__device__ __forceinline__ unsigned rx_classify(const RealDesc& D, int d, float ca, const float (&val)[N]) {
+  const unsigned kind = D.sur_kind[d];
+  if (kind != RX_ELIGIBLE) return kind == RX_STIFF ? RX_CLASS_PLAIN : RX_CLASS_NONE;
+  const unsigned rm = D.rmask[d];
+  const float dca = val[0];
+  float G = 0.f;
+#pragma unroll
+  for (int s = 1; s < N; s++) {
+    if (!(rm >> s & 1u)) continue;
+    const float4 k = D.rk[d][s];
+    G = __fadd_rn(G, buffer_dj(k.x, k.y, k.z, k.w, val[s], dca, ca));
+  }
+  const float aG = fabsf(G);
+  bool near = true;
+#pragma unroll
+  for (int s = 1; s < N; s++) {
+    if (!(rm >> s & 1u)) continue;
+    const float4 k = D.rk[d][s];
+    const float in = __fmaf_rn(k.x, ca, k.y);
+    const float dJ = buffer_dj(k.x, k.y, k.z, k.w, val[s], dca, ca);
+    const float lhs = __fmaf_rn(__fmul_rn(k.x, __fsub_rn(val[s], D.sur_cs[d][s])), aG, __fmul_rn(fabsf(in), fabsf(dJ)));
+    near &= lhs <= D.sur_thr2[d][s];
+  }
+  return near ? RX_CLASS_EXPLICIT : RX_CLASS_NETWORK;
+}
+
+// SUR: on fast-reaction steps of a realisation with RealDesc::sur, cls receives the
+// voxel's surrogate class (rx_classify); otherwise it is left alone.
+template <int N, bool SUR = false, class LoadU, class LoadD>
 __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& si, unsigned valid, bool on_face,
-                                             LoadU ld, LoadD ldd, float (&out)[N]) {
+                                             LoadU ld, LoadD ldd, float (&out)[N], unsigned* cls = nullptr) {
   const int braw = ldd(6);
   const int d = braw & DOMAIN_BITS;
   const int pat = braw >> 3;
@@ -212,6 +253,7 @@ __device__ __forceinline__ void voxel_update(const RealDesc& D, const StepInfo& 
   if (si.react) {
     if (si.react_fast) {
       const float dca = val[0], ca = __fadd_rn(D.fbase[d][0], dca);
+      if (SUR && D.sur) *cls = rx_classify<N>(D, d, ca, val);
       const unsigned rm = D.rmask[d];
 #pragma unroll
       for (int s = 1; s < N; s++) {
@@ -275,11 +317,13 @@ __global__ void __launch_bounds__(256) k_voxels_direct(const RealDesc* __restric
   };
   auto ldd = [&](int kk) -> int { return __ldg(D.dom + idx + (kk < 6 ? off[kk] : 0)); };
   float out[NS];
-  voxel_update<NS>(D, si, valid, on_face, ld, ldd, out);
+  unsigned cls = RX_CLASS_NONE;
+  voxel_update<NS, true>(D, si, valid, on_face, ld, ldd, out, &cls);
 #pragma unroll
   for (int s = 0; s < NS; s++) {
     if (s < D.ns && (si.updated >> s & 1u)) D.u[((cur >> s) & 1u) ^ 1u][s][idx] = out[s];
   }
+  if (D.sur && si.react_fast) D.rx_class[idx] = (unsigned char)cls;
 }
 
 // Channel gating of one channel at step time_ind (evaluate_RyR_stochastically,

@@ -368,78 +368,64 @@ __device__ __forceinline__ bool rx_surrogate(const MlpW& W, const RxConst& k, in
 
 namespace csp {
 
-// ---- deployment: the reaction increments of a reaction step, after the voxel kernel
-// (run with its reaction switched off) and the boundary kernels; on other steps the
-// launches return at once.  Reads the old state and adds into the new one; species fixed
-// in the voxel's domain and, with -f, Ca on the outer faces keep the values the voxel
-// kernel gave them.
+// ---- deployment.  With the surrogate on (RealDesc::sur) the voxel kernel still applies
+// the explicit increment dJ_s (buffer_dj) on a reaction step and also classifies every
+// voxel (rx_classify): near equilibrium (the explicit increment stands), network (an
+// eligible domain away from equilibrium) or plain integrator (a stiff domain).  After the
+// boundary kernels, k_react_surrogate scans the class bytes; the voxels of the last two
+// classes receive the correction (increment - dJ_s) for every bound species s and
+// (sum dJ_s - sum increments) for Ca, from the old state: species fixed in the voxel's
+// domain and, with -f, Ca on the outer faces keep the values the voxel kernel gave them.
 //
-// k_react_surrogate streams the fields: a CTA takes MLP_DEPLOY_SPAN consecutive voxels
-// of one realisation (blockIdx.y); a thread takes groups of 4 consecutive voxels (16-byte
-// loads and stores of the species that the group's domains react: a warp moves 512
-// contiguous bytes per species).  A group lies in one plane (planes are padded to
-// multiples of 128 voxels) and a warp's 128 voxels are all inside the field or all
-// outside, so warp-wide steps stay convergent.  Voxels near equilibrium are finished in
-// their group; voxels of stiff domains are queued in a per-warp ring of shared memory and
-// take the plain integrator (FP64) 32 at a time, one per lane, after their group's store
-// (re-read by a lane of the same warp); voxels that need the network are listed per CTA
-// (offsets within its span) for k_react_network, which runs the network on the tensor
-// cores for tiles of 32 listed voxels.  counters[0] += voxels, counters[1] += voxels the
-// network ran for, counters[2] += voxels that took the plain integrator.
+// k_react_surrogate: a CTA takes MLP_DEPLOY_SPAN consecutive voxels of one realisation
+// (blockIdx.y); a thread reads the class bytes of MLP_SCAN_VPT consecutive voxels (a warp
+// reads 256 contiguous bytes) and lists the voxels to correct (offsets within the CTA's
+// span); the CTA queues its list as tiles of 32 for k_react_network, whose warps share the
+// tiles of every list evenly (stiff domains are spatially clustered: one CTA alone would
+// run their FP64 integrations one after the other).  counters[0] += voxels with
+// buffers, counters[1] += voxels the network ran for, counters[2] += voxels that took
+// the plain integrator.
 constexpr int MLP_DEPLOY_T = 256;
-constexpr int MLP_DEPLOY_ITER = 16;      // groups of 4 voxels per thread
-constexpr long long MLP_DEPLOY_SPAN = 4ll * MLP_DEPLOY_T * MLP_DEPLOY_ITER;   // voxels per CTA
+constexpr int MLP_SCAN_VPT = 8;          // class bytes per thread and iteration
+constexpr int MLP_DEPLOY_ITER = 8;
+constexpr long long MLP_DEPLOY_SPAN = (long long)MLP_SCAN_VPT * MLP_DEPLOY_T * MLP_DEPLOY_ITER;   // voxels per CTA
 static_assert(MLP_DEPLOY_SPAN <= 65536, "list entries are 16-bit offsets within a CTA's span");
 constexpr int MLP_RX_NS = MLP_SLOTS + 1; // species the reaction touches: Ca and slots 1..5
-constexpr unsigned MLP_RING = 256;       // ring entries (a power of two; at most 159 are held)
 constexpr size_t MLP_NETWORK_SMEM = sizeof(MlpTC) + sizeof(float) * (size_t)MLP_TC_STAGE * (MLP_DEPLOY_T / 32);
 
-enum : unsigned { RX_NONE = 0, RX_ELIGIBLE = 1, RX_STIFF = 2 };
-
-// The reaction constants of one domain, block-shared.
+// The reaction constants of one domain (block- or warp-shared).
 struct RxDom {
   RxConst k;
-  float thr[MLP_SLOTS];                  // near-equilibrium thresholds (rx_near_equilibrium)
+  float4 rk[MLP_RX_NS];                  // RealDesc::rk of the bound species (buffer_dj)
   float base[MLP_RX_NS], qunit[MLP_RX_NS], qinv[MLP_RX_NS];   // RealDesc::fbase / qunit / qinv
-  unsigned kind;                         // RX_NONE: no buffers; RX_ELIGIBLE: network domain; RX_STIFF
-  unsigned load;                         // species the reaction reads: Ca and the domain's buffers
-  unsigned store;                        // species it writes: load minus the domain's fixed species
+  unsigned store;                        // species corrected: Ca and the bound species, minus the fixed ones
 };
 
-// Old value of species s: base plus the stored deviation (fixed-point for the species in
-// FQ & fqs).
+__device__ __forceinline__ void rx_dom_fill(const RealDesc& D, int d, RxDom& S) {
+  const int dd = d < D.nd ? d : 0;
+  S.k = rx_const(D, dd);
+  unsigned ld = 0;
+  for (int q = 0; q < MLP_SLOTS; q++)
+    if (S.k.tot[q] > 0.f) ld |= 2u << q;
+  for (int s = 0; s < MLP_RX_NS; s++) {
+    S.rk[s] = D.rk[dd][s];
+    S.base[s] = D.fbase[dd][s];
+    S.qunit[s] = D.qunit[dd][s];
+    S.qinv[s] = D.qinv[dd][s];
+  }
+  S.store = (d < D.nd && ld) ? (ld | 1u) & ~(unsigned)D.fixed_mask[dd] : 0u;
+}
+
+// Deviation of species s from its stored form (fixed-point for the species in FQ & fqs).
 template <unsigned FQ>
-__device__ __forceinline__ float rx_old(const RxDom& K, int s, float stored, unsigned fqs) {
-  return __fadd_rn(K.base[s], ((FQ & fqs) >> s & 1u) ? q_value(stored, K.qunit[s]) : stored);
+__device__ __forceinline__ float rx_dev(const RxDom& K, int s, float stored, unsigned fqs) {
+  return ((FQ & fqs) >> s & 1u) ? q_value(stored, K.qunit[s]) : stored;
 }
 
 // Stored new value of species s plus an increment.
 template <unsigned FQ>
 __device__ __forceinline__ float rx_add(const RxDom& K, int s, float stored, float inc, unsigned fqs) {
   return ((FQ & fqs) >> s & 1u) ? q_add(stored, inc, K.qinv[s]) : __fadd_rn(stored, inc);
-}
-
-// Near equilibrium (every S_s <= MLP_SKIP), with S_s <= MLP_SKIP tested as
-// lam |g| + k_on (tot - b) |G| <= thr_s, thr_s = MLP_SKIP tot_s / (dt_r^2 / 2) (no division).
-// g[] receives the reaction rates g_s for the explicit increment.  Absent buffers (k_on =
-// k_off = tot = thr = 0, b = 0) give g = 0 and a term 0 <= 0, so every slot is evaluated
-// without a branch.
-__device__ __forceinline__ bool rx_near_equilibrium(const RxConst& k, const float* thr, float c, const float* b,
-                                                    float* g) {
-  float G = 0.f;
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) {
-    g[q] = rx_g<float>(k, q, c, b[q]);
-    G += g[q];
-  }
-  const float aG = fabsf(G);
-  bool near = true;
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) {
-    const float lam = k.koff[q] + k.kon[q] * c;
-    near &= lam * fabsf(g[q]) + k.kon[q] * (k.tot[q] - b[q]) * aG <= thr[q];
-  }
-  return near;
 }
 
 // The plain integrator's increments (the fallback), FP64, rounded to FP32.
@@ -457,59 +443,49 @@ __device__ __forceinline__ bool rx_on_face(const RealDesc& D, int x, int p) {
   return x == 0 || x == D.nx - 1 || c1 == 0 || c1 == D.ny - 1 || c2 == 0 || c2 == D.nz - 1;
 }
 
-// Voxel j of a group in an eligible domain (o / nw: old / new stored values of the group's
-// species): near equilibrium, the explicit increment is added into nw and the result is
-// true; otherwise nw is left alone (the voxel needs the network).  LM != 0: the domain's
-// load and store masks are both LM (bit 0 Ca, bit q+1 slot q), known at compile time, so
-// absent slots cost nothing; LM = 0: any domain (masks read from K).
-template <unsigned FQ, unsigned LM>
-__device__ __forceinline__ bool rx_group_voxel(const RxDom& K, float dtr, unsigned fqs,
-                                               const float (&o)[MLP_RX_NS][4], float (&nw)[MLP_RX_NS][4], int j,
-                                               bool face) {
-  auto present = [&](int q) { return LM ? ((LM >> (q + 1)) & 1u) != 0u : K.k.tot[q] > 0.f; };
-  auto stored = [&](int s) { return LM ? ((LM >> s) & 1u) != 0u : ((K.store >> s) & 1u) != 0u; };
-  const float c = rx_old<FQ>(K, 0, o[0][j], fqs);
-  float b[MLP_SLOTS], g[MLP_SLOTS];
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) b[q] = present(q) ? rx_old<FQ>(K, q + 1, o[q + 1][j], fqs) : 0.f;
-  // rx_near_equilibrium restricted to the present slots (absent ones add exact zeros there)
-  float G = 0.f;
+// One voxel's old state: deviations dev[] (Ca and the slots' species) and the values
+// c = Ca, b[q] (0 for absent slots).
+template <unsigned FQ>
+__device__ __forceinline__ void rx_load_old(const RxDom& K, const float* const* uo, long long v, unsigned fqs,
+                                            float* dev, float& c, float* b) {
+  dev[0] = __ldg(uo[0] + v);
+  c = __fadd_rn(K.base[0], dev[0]);
 #pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) {
-    g[q] = 0.f;
-    if (!LM || present(q)) {
-      g[q] = rx_g<float>(K.k, q, c, b[q]);
-      G += g[q];
+    dev[q + 1] = 0.f;
+    b[q] = 0.f;
+    if (K.k.tot[q] > 0.f) {
+      dev[q + 1] = rx_dev<FQ>(K, q + 1, __ldg(uo[q + 1] + v), fqs);
+      b[q] = __fadd_rn(K.base[q + 1], dev[q + 1]);
     }
   }
-  const float aG = fabsf(G);
-  bool near = true;
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) {
-    if (LM && !present(q)) continue;
-    const float lam = K.k.koff[q] + K.k.kon[q] * c;
-    near &= lam * fabsf(g[q]) + K.k.kon[q] * (K.k.tot[q] - b[q]) * aG <= K.thr[q];
-  }
-  if (!near) return false;
-  float sdb = 0.f;
-#pragma unroll
-  for (int q = 0; q < MLP_SLOTS; q++) {
-    if (LM && !present(q)) continue;
-    const float db = dtr * g[q];
-    sdb += db;
-    if (stored(q + 1)) nw[q + 1][j] = rx_add<FQ>(K, q + 1, nw[q + 1][j], db, fqs);
-  }
-  if (stored(0) && !face) nw[0][j] = __fadd_rn(nw[0][j], -sdb);
-  return true;
 }
 
-// The compile-time layout of rx_group_voxel: Ca and the first four buffer slots, none of
-// them fixed (the reference's cytosolic buffers CMDN, ATP, Fluo, TRPN after Ca).
-constexpr unsigned MLP_LM_CYTOSOL = 0x1Fu;
+// Replace the explicit increments the voxel kernel applied to voxel v by the surrogate's
+// (db[], dc): the explicit ones are recomputed from the same deviations and constants,
+// so they are the ones that were added.
+template <unsigned FQ>
+__device__ __forceinline__ void rx_correct(const RxDom& K, const RealDesc& D, float* const* un, long long v,
+                                           unsigned fqs, const float* dev, float c, const float* db, float dc) {
+  float sdj = 0.f;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    if (K.k.tot[q] <= 0.f) continue;
+    const float4 k = K.rk[q + 1];
+    const float dJ = buffer_dj(k.x, k.y, k.z, k.w, dev[q + 1], dev[0], c);
+    sdj = __fadd_rn(sdj, dJ);
+    if (K.store >> (q + 1) & 1u) un[q + 1][v] = rx_add<FQ>(K, q + 1, un[q + 1][v], __fsub_rn(db[q], dJ), fqs);
+  }
+  if (K.store & 1u) {
+    const int vi = (int)v, xq = vi / D.P;
+    if (!(D.dirichlet && rx_on_face(D, xq, vi - xq * D.P))) un[0][v] = __fadd_rn(un[0][v], __fadd_rn(sdj, dc));
+  }
+}
 
-// Reaction step of realisation r (the condition both deployment kernels test).
+// Reaction step with the surrogate on, on the fast reactions (the steps the voxel kernel
+// classifies).
 __device__ __forceinline__ bool rx_active(const RealDesc& D, const RealCtl& C) {
-  return !C.stopped && D.react_external && D.nbuf > 0 && (C.step + 1) % D.reaction_substep == 0;
+  return !C.stopped && D.sur && step_info(D, C.step + 1).react_fast;
 }
 
 // list / counts: per CTA (seg = blockIdx.y * gridDim.x + blockIdx.x) MLP_DEPLOY_SPAN
@@ -517,7 +493,6 @@ __device__ __forceinline__ bool rx_active(const RealDesc& D, const RealCtl& C) {
 // 32 listed voxels (seg << MLP_TILE_BITS | tile within the list) and their number.
 constexpr int MLP_TILE_BITS = 9;
 static_assert(MLP_DEPLOY_SPAN / 32 <= (1 << MLP_TILE_BITS), "tile index field");
-template <unsigned FQ>
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
                                                                   const RealCtl* __restrict__ ctl,
                                                                   unsigned short* __restrict__ list,
@@ -525,224 +500,76 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
                                                                   unsigned* __restrict__ tiles,
                                                                   unsigned* __restrict__ queue,
                                                                   unsigned long long* __restrict__ counters) {
-  __shared__ RxDom s_dom[8];                 // by domain id (DOMAIN_BITS); entries >= nd: RX_NONE
-  __shared__ const float* s_uo[MLP_RX_NS];
-  __shared__ float* s_un[MLP_RX_NS];
-  __shared__ unsigned s_ring[MLP_DEPLOY_T / 32][MLP_RING];   // per warp: plain-integrator voxels
-  __shared__ unsigned s_vox, s_fall, s_list, s_tile0;
+  __shared__ unsigned s_vox, s_list, s_tile0;
   const RealDesc& D = descs[blockIdx.y];
   const RealCtl& C = ctl[blockIdx.y];
   if (!rx_active(D, C)) return;                         // uniform over the block
   const long long seg = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-  const long long k = C.step;
   const long long nvox = (long long)D.nx * D.P;
   const long long vb0 = (long long)blockIdx.x * MLP_DEPLOY_SPAN;
   if (vb0 >= nvox) {                                    // uniform over the block
     if (threadIdx.x == 0) counts[seg] = 0;
     return;
   }
-  unsigned short* seg_list = list + seg * MLP_DEPLOY_SPAN;
-  const unsigned cur = C.cur_mask[k & 1];
-  const float dtr = (float)(D.dt * D.reaction_substep);
-  if (threadIdx.x < 8) {
-    const int d = threadIdx.x;
-    RxDom& S = s_dom[d];
-    const RxConst kc = rx_const(D, d < D.nd ? d : 0);
-    unsigned ld = 0;
-    for (int q = 0; q < MLP_SLOTS; q++) {
-      S.thr[q] = MLP_SKIP * kc.tot[q] / (0.5f * dtr * dtr);
-      if (kc.tot[q] > 0.f) ld |= 2u << q;
-    }
-    S.k = kc;
-    for (int s = 0; s < MLP_RX_NS; s++) {
-      S.base[s] = D.fbase[d < D.nd ? d : 0][s];
-      S.qunit[s] = D.qunit[d < D.nd ? d : 0][s];
-      S.qinv[s] = D.qinv[d < D.nd ? d : 0][s];
-    }
-    const bool any = d < D.nd && ld != 0;
-    S.kind = !any ? RX_NONE : ((D.mlp_domains >> d) & 1u) ? RX_ELIGIBLE : RX_STIFF;
-    S.load = any ? (ld | 1u) : 0u;
-    S.store = S.load & ~(unsigned)D.fixed_mask[d < D.nd ? d : 0];
-  }
-  if (threadIdx.x < MLP_RX_NS) {
-    const int t = threadIdx.x;
-    s_uo[t] = t < D.ns ? D.u[(cur >> t) & 1u][t] : nullptr;
-    s_un[t] = t < D.ns ? D.u[((cur >> t) & 1u) ^ 1u][t] : nullptr;
-  }
-  if (threadIdx.x == 0) { s_vox = 0; s_fall = 0; s_list = 0; }
+  if (threadIdx.x == 0) { s_vox = 0; s_list = 0; }
   __syncthreads();
-  const unsigned char* __restrict__ dom = D.dom;
-  const int plane = D.plane, P = D.P;
-  const bool dirichlet = D.dirichlet != 0;
-  const unsigned fqs = D.fixq;
-  const int lane = threadIdx.x & 31;
-  const unsigned lt = (1u << lane) - 1u;
-  unsigned* ring_fall = s_ring[threadIdx.x >> 5];
-  unsigned hf = 0, tf = 0;                             // ring head / tail (warp-uniform)
-  unsigned n_vox = 0, n_fall = 0;
-  // one queued voxel: old values reconstructed, new values as stored
-  auto load1 = [&](long long vv, const RxDom& K, float& c, float* b, float& nc, float* nb) {
-    c = rx_old<FQ>(K, 0, __ldg(s_uo[0] + vv), fqs);
-    nc = s_un[0][vv];
+  unsigned short* seg_list = list + seg * MLP_DEPLOY_SPAN;
+  const unsigned char* __restrict__ cls = D.rx_class;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned n_vox = 0;
+  for (int it = 0; it < MLP_DEPLOY_ITER; it++) {
+    const long long w0 = vb0 + (long long)it * MLP_SCAN_VPT * MLP_DEPLOY_T + (long long)warp * MLP_SCAN_VPT * 32;
+    if (w0 >= nvox) break;                               // warp-uniform
+    const long long v = w0 + MLP_SCAN_VPT * lane;
+    uint2 w = make_uint2(0u, 0u);
+    if (v < nvox) w = __ldg(reinterpret_cast<const uint2*>(cls + v));
+    unsigned m = 0;
 #pragma unroll
-    for (int q = 0; q < MLP_SLOTS; q++) {
-      b[q] = nb[q] = 0.f;
-      if (K.k.tot[q] > 0.f) {
-        b[q] = rx_old<FQ>(K, q + 1, __ldg(s_uo[q + 1] + vv), fqs);
-        nb[q] = s_un[q + 1][vv];
-      }
+    for (int j = 0; j < MLP_SCAN_VPT; j++) {
+      const unsigned c = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
+      if (c) n_vox++;
+      if (c >= RX_CLASS_NETWORK) m |= 1u << j;
     }
-  };
-  auto store1 = [&](long long vv, const RxDom& K, float nc, const float* nb, float dc, const float* db) {
+    if (__any_sync(0xffffffffu, m != 0u)) {
+      // a warp-wide prefix sum of the counts, one shared atomic
+      const unsigned cnt = __popc(m);
+      unsigned incl = cnt;
 #pragma unroll
-    for (int q = 0; q < MLP_SLOTS; q++)
-      if (K.store >> (q + 1) & 1u) s_un[q + 1][vv] = rx_add<FQ>(K, q + 1, nb[q], db[q], fqs);
-    if (K.store & 1u) {
-      const int vi = (int)vv, xq = vi / P;
-      if (!(dirichlet && rx_on_face(D, xq, vi - xq * P))) s_un[0][vv] = __fadd_rn(nc, dc);
-    }
-  };
-  // the plain integrator on ring_fall's next cnt voxels, one per lane
-  auto flush_fall = [&](unsigned cnt) {
-    __syncwarp();
-    const bool have = lane < cnt;
-    const unsigned off = have ? ring_fall[(hf + lane) & (MLP_RING - 1)] : 0u;
-    hf += cnt;
-    if (have) {
-      const long long vv = vb0 + off;
-      const RxDom& K = s_dom[dom[vv] & DOMAIN_BITS];
-      float c, nc, b[MLP_SLOTS], nb[MLP_SLOTS], dc, db[MLP_SLOTS];
-      load1(vv, K, c, b, nc, nb);
-      n_fall++;
-      rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
-      store1(vv, K, nc, nb, dc, db);
-    }
-    __syncwarp();
-  };
-  long long v = vb0 + 4 * threadIdx.x;
-  int p = (int)(v % P), x = (int)(v / P);              // in-plane position and plane of voxel v
-  for (int it = 0;; it++) {
-    const bool live = v < nvox;                          // warp-uniform
-    if (live) {
-      const unsigned w4 = __ldg(reinterpret_cast<const unsigned*>(dom + v));   // 4 domain bytes
-      int dj[4];
-      unsigned need = 0;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        dj[j] = p + j < plane ? (int)((w4 >> (8 * j)) & DOMAIN_BITS) : 7;
-        need |= s_dom[dj[j]].load;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
       }
-      float o[MLP_RX_NS][4], nw[MLP_RX_NS][4];
-#pragma unroll
-      for (int s = 0; s < MLP_RX_NS; s++) {
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-        if (need >> s & 1u) {
-          a = __ldg(reinterpret_cast<const float4*>(s_uo[s] + v));
-          b = *reinterpret_cast<const float4*>(s_un[s] + v);
-        }
-        o[s][0] = a.x; o[s][1] = a.y; o[s][2] = a.z; o[s][3] = a.w;
-        nw[s][0] = b.x; nw[s][1] = b.y; nw[s][2] = b.z; nw[s][3] = b.w;
-      }
-      bool face[4] = {false, false, false, false};
-      if (dirichlet)
-#pragma unroll
-        for (int j = 0; j < 4; j++) face[j] = rx_on_face(D, x, p + j);
-      // r: 0 no buffers, 1 finished (explicit increment), 2 network, 3 plain integrator
-      int r[4];
-      unsigned upd = 0;
-      if (dj[0] == dj[1] && dj[0] == dj[2] && dj[0] == dj[3]) {
-        const RxDom K = s_dom[dj[0]];                    // one domain: its constants in registers
-        if (K.kind == RX_ELIGIBLE && K.load == MLP_LM_CYTOSOL && K.store == MLP_LM_CYTOSOL) {
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            r[j] = rx_group_voxel<FQ, MLP_LM_CYTOSOL>(K, dtr, fqs, o, nw, j, face[j]) ? 1 : 2;
-          upd = K.store;
-        } else if (K.kind == RX_ELIGIBLE) {
-#pragma unroll
-          for (int j = 0; j < 4; j++) r[j] = rx_group_voxel<FQ, 0u>(K, dtr, fqs, o, nw, j, face[j]) ? 1 : 2;
-          upd = K.store;
-        } else {
-#pragma unroll
-          for (int j = 0; j < 4; j++) r[j] = K.kind == RX_STIFF ? 3 : 0;
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const RxDom& K = s_dom[dj[j]];
-          r[j] = K.kind == RX_STIFF ? 3 : 0;
-          if (K.kind == RX_ELIGIBLE) {
-            r[j] = rx_group_voxel<FQ, 0u>(K, dtr, fqs, o, nw, j, face[j]) ? 1 : 2;
-            if (r[j] == 1) upd |= K.store;
-          }
-        }
-      }
-      unsigned mnet = 0, mfall = 0;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        if (r[j]) n_vox++;
-        if (r[j] == 2) mnet |= 1u << j;
-        if (r[j] == 3) mfall |= 1u << j;
-      }
-#pragma unroll
-      for (int s = 0; s < MLP_RX_NS; s++)
-        if (upd >> s & 1u)
-          *reinterpret_cast<float4*>(s_un[s] + v) = make_float4(nw[s][0], nw[s][1], nw[s][2], nw[s][3]);
+      unsigned base = 0;
+      if (lane == 31) base = atomicAdd(&s_list, incl);
+      unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
       const unsigned off = (unsigned)(v - vb0);
-      if (__any_sync(0xffffffffu, mnet != 0u)) {
-        // this CTA's network list: a warp-wide prefix sum of the counts, one shared atomic
-        const unsigned cnt = __popc(mnet);
-        unsigned incl = cnt;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += t;
-        }
-        unsigned base = 0;
-        if (lane == 31) base = atomicAdd(&s_list, incl);
-        unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (mnet >> j & 1u) seg_list[pos++] = (unsigned short)(off + j);
-      }
-      if (__any_sync(0xffffffffu, mfall != 0u))
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const unsigned bal = __ballot_sync(0xffffffffu, mfall >> j & 1u);
-          if (mfall >> j & 1u) ring_fall[(tf + __popc(bal & lt)) & (MLP_RING - 1)] = off + j;
-          tf += __popc(bal);
-        }
+      for (int j = 0; j < MLP_SCAN_VPT; j++)
+        if (m >> j & 1u) seg_list[pos++] = (unsigned short)(off + j);
     }
-    const bool last = !live || it == MLP_DEPLOY_ITER - 1 || v + 4 * MLP_DEPLOY_T >= nvox;   // warp-uniform
-    // full warps of queued voxels (the ring never holds more than 31 + 128), and after
-    // the last group whatever is queued
-    while (tf - hf >= 32u || (last && tf != hf)) flush_fall(min(tf - hf, 32u));
-    if (last) break;
-    v += 4 * MLP_DEPLOY_T;
-    p += 4 * MLP_DEPLOY_T;
-    while (p >= P) { p -= P; x++; }
   }
   if (n_vox) atomicAdd(&s_vox, n_vox);
-  if (n_fall) atomicAdd(&s_fall, n_fall);
   __syncthreads();
   const unsigned ntile = (s_list + 31u) / 32u;
   if (threadIdx.x == 0) {
     counts[seg] = s_list;
     if (ntile) s_tile0 = atomicAdd(&queue[0], ntile);
     if (s_vox) atomicAdd(&counters[0], (unsigned long long)s_vox);
-    if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
   }
   __syncthreads();
   for (unsigned j = threadIdx.x; j < ntile; j += MLP_DEPLOY_T)
     tiles[s_tile0 + j] = (unsigned)seg << MLP_TILE_BITS | j;
 }
 
-// The network voxels that k_react_surrogate listed, in tiles of 32 on the tensor cores (a
-// rejected output takes the plain integrator).  Persistent CTAs: warp w of the grid takes
-// a contiguous range of the queued tiles (tiles of one list are queued together, so a
-// warp's realisation rarely changes; its domain constants and field pointers are cached
-// per warp in shared memory); a CTA without a tile returns before it loads the weights.
-// The last CTA to finish empties the queue (queue[0]: tiles, queue[1]: CTAs done) for the
-// next step.  chunks = k_react_surrogate's gridDim.x.
+// The voxels that k_react_surrogate listed, in tiles of 32: network voxels on the tensor
+// cores (a tile runs the network when any of its voxels needs it; a rejected output takes
+// the plain integrator), stiff-domain voxels on the plain integrator (FP64), one per lane;
+// each is corrected from the old state (rx_correct).  Persistent CTAs: warp w of the grid takes a contiguous range of the queued tiles (tiles
+// of one list are queued together, so a warp's realisation rarely changes; its domain
+// constants and field pointers are cached per warp in shared memory); a CTA without a
+// tile returns before it loads the weights.  The last CTA to finish empties the queue
+// (queue[0]: tiles, queue[1]: CTAs done) for the next step.  chunks = k_react_surrogate's
+// gridDim.x.
 template <unsigned FQ>
 __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDesc* __restrict__ descs,
                                                                    const RealCtl* __restrict__ ctl,
@@ -780,19 +607,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
       if (r != rc) {                                     // warp-uniform
         __syncwarp();
         if (lane < 8) {
-          const int d = lane < D.nd ? lane : 0;
-          RxDom& S = s_dom[warp][lane];
-          S.k = rx_const(D, d);
-          unsigned ld = 0;
-          for (int q = 0; q < MLP_SLOTS; q++)
-            if (S.k.tot[q] > 0.f) ld |= 2u << q;
-          for (int s = 0; s < MLP_RX_NS; s++) {
-            S.base[s] = D.fbase[d][s];
-            S.qunit[s] = D.qunit[d][s];
-            S.qinv[s] = D.qinv[d][s];
-          }
-          S.load = ld ? (ld | 1u) : 0u;
-          S.store = S.load & ~(unsigned)D.fixed_mask[d];
+          rx_dom_fill(D, lane, s_dom[warp][lane]);
         } else if (lane < 8 + MLP_RX_NS) {
           const int t = lane - 8;
           const unsigned cur = ctl[r].cur_mask[ctl[r].step & 1];
@@ -809,44 +624,33 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
       const bool have = t0 + lane < cnt;
       const long long v = vb0 + (have ? list[seg * MLP_DEPLOY_SPAN + t0 + lane] : 0);
       const int d = have ? (D.dom[v] & DOMAIN_BITS) : 0;
+      const bool net = have && D.rx_class[v] == RX_CLASS_NETWORK;
       const RxDom& K = s_dom[warp][d];
-      float c = 0.f, nc = 0.f, b[MLP_SLOTS], nb[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
+      float dev[MLP_RX_NS], c = 0.f, b[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
 #pragma unroll
       for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
 #pragma unroll
-      for (int q = 0; q < MLP_SLOTS; q++) b[q] = nb[q] = 0.f;
+      for (int q = 0; q < MLP_SLOTS; q++) b[q] = 0.f;
       if (have) {
-        c = rx_old<FQ>(K, 0, __ldg(s_uo[warp][0] + v), fqs);
-        nc = s_un[warp][0][v];
-#pragma unroll
-        for (int q = 0; q < MLP_SLOTS; q++) {
-          if (K.k.tot[q] <= 0.f) continue;
-          b[q] = rx_old<FQ>(K, q + 1, __ldg(s_uo[warp][q + 1] + v), fqs);
-          nb[q] = s_un[warp][q + 1][v];
-        }
-        rx_features(K.k, d, dtr, c, b, x);
+        rx_load_old<FQ>(K, s_uo[warp], v, fqs, dev, c, b);
+        if (net) rx_features(K.k, d, dtr, c, b, x);
       }
-      mlp_forward_tc(T, stage, x, t);
+      if (__any_sync(0xffffffffu, net)) mlp_forward_tc(T, stage, x, t);
       if (have) {
-        n_net++;
         float dc, db[MLP_SLOTS];
-        if (!rx_apply_output(K.k, dtr, c, b, t, tol, dc, db)) {
+        if (net) n_net++;
+        if (!net || !rx_apply_output(K.k, dtr, c, b, t, tol, dc, db)) {
           n_fall++;
           rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
         }
-#pragma unroll
-        for (int q = 0; q < MLP_SLOTS; q++)
-          if (K.store >> (q + 1) & 1u) s_un[warp][q + 1][v] = rx_add<FQ>(K, q + 1, nb[q], db[q], fqs);
-        const int vi = (int)v, xq = vi / D.P;
-        if ((K.store & 1u) && !(D.dirichlet && rx_on_face(D, xq, vi - xq * D.P)))
-          s_un[warp][0][v] = __fadd_rn(nc, dc);
+        rx_correct<FQ>(K, D, s_un[warp], v, fqs, dev, c, db, dc);
       }
     }
     if (n_net) atomicAdd(&s_net, n_net);
     if (n_fall) atomicAdd(&s_fall, n_fall);
     __syncthreads();
-    if (threadIdx.x == 0 && s_net) {
-      atomicAdd(&counters[1], (unsigned long long)s_net);
+    if (threadIdx.x == 0) {
+      if (s_net) atomicAdd(&counters[1], (unsigned long long)s_net);
       if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
     }
   }

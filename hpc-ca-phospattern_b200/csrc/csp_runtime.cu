@@ -181,13 +181,14 @@ struct csp_handle {
   // learned reaction surrogate (csp_set_surrogate)
   int surrogate = 0;
   float surrogate_tol = 1e-4f;
-  unsigned surrogate_fq = 0;         // k_react_surrogate<FQ> of the ensemble's fixed-point species
+  unsigned surrogate_fq = 0;         // k_react_network<FQ> of the ensemble's fixed-point species
   float* d_mlp = nullptr;                   // MLP_NPARAM parameters
   unsigned long long* d_mlp_cnt = nullptr;  // voxels, network evaluations, fallbacks
   unsigned short* d_sur_list = nullptr;     // per k_react_surrogate CTA: its network voxels
   unsigned* d_sur_counts = nullptr;         // per k_react_surrogate CTA: listed voxels
   unsigned* d_sur_tiles = nullptr;          // tiles of 32 listed voxels (k_react_network's work)
   unsigned* d_sur_queue = nullptr;          // tiles queued, k_react_network CTAs done
+  unsigned char* d_rx_class = nullptr;      // surrogate class bytes (RealDesc::rx_class), layout of d_dom
   int sur_network_ctas = 0;                 // persistent CTAs of k_react_network
   // training pairs harvested from the fields (csp_mlp_harvest): features [cap][8], targets [cap][5]
   float* d_hx = nullptr;
@@ -1035,7 +1036,7 @@ static void launch_voxels(csp_handle* h, int r0 = 0, int r1 = -1) {
     dim3 grid((unsigned)((h->max_vox + 255) / 256), (unsigned)(r1 - r0));
     k_voxels_direct<<<grid, 256, 0, h->stream>>>(h->d_desc + r0, h->d_ctl + r0, h->d_err);
   } else {
-    staged_launch(h->plan, h->d_desc, h->d_ctl, h->d_err, h->stream, h->inject_wait != 0, r0, r1);
+    staged_launch(h->plan, h->d_desc, h->d_ctl, h->d_err, h->stream, h->inject_wait != 0, r0, r1, h->surrogate != 0);
   }
 }
 
@@ -1068,15 +1069,10 @@ static void launch_channel_rows(csp_handle* h, int r0, int r1) {
                                                                         std::max(h->nch, 1));
 }
 
-// The surrogate instantiations for the fixed-point species of the ensemble (none, TRPN's
-// slot alone, or any slot).
-using SurrogateKernel = void (*)(const RealDesc*, const RealCtl*, unsigned short*, unsigned*, unsigned*, unsigned*,
-                                 unsigned long long*);
+// The network kernel's instantiations for the fixed-point species of the ensemble (none,
+// TRPN's slot alone, or any slot).
 using NetworkKernel = void (*)(const RealDesc*, const RealCtl*, const float*, float, const unsigned short*,
                                const unsigned*, const unsigned*, unsigned*, int, unsigned long long*);
-static SurrogateKernel surrogate_kernel(unsigned fq) {
-  return fq == 0u ? k_react_surrogate<0u> : fq == 0x10u ? k_react_surrogate<0x10u> : k_react_surrogate<0x3Eu>;
-}
 static NetworkKernel network_kernel(unsigned fq) {
   return fq == 0u ? k_react_network<0u> : fq == 0x10u ? k_react_network<0x10u> : k_react_network<0x3Eu>;
 }
@@ -1084,7 +1080,7 @@ static NetworkKernel network_kernel(unsigned fq) {
 static void launch_surrogate(csp_handle* h, int r0, int r1) {
   if (!h->surrogate) return;
   const int chunks = (int)((h->max_field + MLP_DEPLOY_SPAN - 1) / MLP_DEPLOY_SPAN);
-  surrogate_kernel(h->surrogate_fq)<<<dim3((unsigned)chunks, (unsigned)(r1 - r0)), MLP_DEPLOY_T, 0, h->stream>>>(
+  k_react_surrogate<<<dim3((unsigned)chunks, (unsigned)(r1 - r0)), MLP_DEPLOY_T, 0, h->stream>>>(
       h->d_desc + r0, h->d_ctl + r0, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles, h->d_sur_queue, h->d_mlp_cnt);
   network_kernel(h->surrogate_fq)<<<h->sur_network_ctas, MLP_DEPLOY_T, MLP_NETWORK_SMEM, h->stream>>>(
       h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
@@ -2032,6 +2028,11 @@ static int surrogate_supported(csp_handle* h) {
     const RealDesc& D = h->real[r].desc;
     if (D.nbuf == 0) continue;
     if (!D.react_fast) return fail(h, CSP_ENOTSUP, "realisation %d: the surrogate needs every buffer bound to species 0", r);
+    int dca = -1;
+    for (int i = 0; i < D.ndiff; i++)
+      if (D.diff_species[i] == 0) dca = i;
+    if (dca < 0 || D.reaction_substep % D.substeps[dca] != 0)
+      return fail(h, CSP_ENOTSUP, "realisation %d: the surrogate needs species 0 to diffuse on every reaction step", r);
     for (int d = 0; d < D.nd; d++)
       for (int s = MLP_SLOTS + 1; s < NS; s++)
         if (D.rtab[d][s] >= 0) return fail(h, CSP_ENOTSUP, "realisation %d: buffer species %d beyond the 5 slots", r, s);
@@ -2071,12 +2072,34 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     h->surrogate_tol = (float)tol;
   }
+  if (on && !h->d_rx_class) {
+    size_t bytes = 0;
+    for (int r = 0; r < h->n; r++) bytes += h->real[r].field_elems;
+    if (cudaMalloc(&h->d_rx_class, bytes + 16) != cudaSuccess) return fail(h, CSP_ENOMEM, "surrogate class bytes");
+    CUDA_TRY(h, cudaMemsetAsync(h->d_rx_class, 0, bytes + 16, h->stream));
+  }
   h->surrogate = on;
   std::vector<RealDesc> descs(h->n);
   for (int r = 0; r < h->n; r++) {
-    h->real[r].desc.react_external = on;
-    h->real[r].desc.mlp_domains = mlp_eligible_domains(h->real[r].desc);
-    descs[r] = h->real[r].desc;
+    RealDesc& D = h->real[r].desc;
+    D.sur = on;
+    D.mlp_domains = mlp_eligible_domains(D);
+    // the class bytes share the domain bytes' layout and offsets
+    D.rx_class = on ? h->d_rx_class + (D.dom - h->d_dom) : nullptr;
+    for (int d = 0; d < ND; d++) {
+      bool any = false;
+      for (int sp = 0; sp < NS; sp++) {
+        D.sur_cs[d][sp] = 0.f;
+        D.sur_thr2[d][sp] = 0.f;
+        if (d >= D.nd || !(D.rmask[d] >> sp & 1u)) continue;
+        const int t = D.rtab[d][sp] * D.nd + d;
+        D.sur_cs[d][sp] = (float)((double)D.tot[t] - D.base[d][sp]);
+        D.sur_thr2[d][sp] = (float)(2.0 * (double)MLP_SKIP * (double)D.tot[t]);
+        any = true;
+      }
+      D.sur_kind[d] = (unsigned char)(!any ? RX_NONE : ((D.mlp_domains >> d) & 1u) ? RX_ELIGIBLE : RX_STIFF);
+    }
+    descs[r] = D;
   }
   CUDA_TRY(h, cudaMemcpyAsync(h->d_desc, descs.data(), h->n * sizeof(RealDesc), cudaMemcpyHostToDevice, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
@@ -2376,7 +2399,7 @@ extern "C" void csp_destroy(csp_handle* h) {
   if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->snap_stream) cudaStreamDestroy(h->snap_stream);
   cudaFree(h->d_mlp); cudaFree(h->d_mlp_cnt); cudaFree(h->d_sur_list); cudaFree(h->d_sur_counts);
-  cudaFree(h->d_sur_tiles); cudaFree(h->d_sur_queue);
+  cudaFree(h->d_sur_tiles); cudaFree(h->d_sur_queue); cudaFree(h->d_rx_class);
   cudaFree(h->d_hx); cudaFree(h->d_ht);
   for (auto& e : h->phase_ev)
     if (e) cudaEventDestroy(e);

@@ -58,6 +58,7 @@ struct StagedPlan {
   int nunits = 0;
   std::vector<int> unit_first;  // [n+1]: the units of realisation r are [unit_first[r], unit_first[r+1])
   StagedLaunchFn launch = nullptr;
+  StagedLaunchFn launch_sur = nullptr;      // the variant that also classifies voxels for the surrogate
   StagedLaunchFn launch_inject = nullptr;   // null: no test-hook variant for this plan
   unsigned fixq = 0;                        // union of the realisations' fixed-point species
 };
@@ -143,11 +144,56 @@ __device__ __forceinline__ unsigned ld_u32_any(const unsigned char* p) {
   return __funnelshift_r(w[0], w[1], 8u * (unsigned)(a & 3));
 }
 
+// rx_classify on the four voxels of a group in one domain d, in two-lane FP32 with the
+// same rounding (ca0 / ca1: Ca of voxels 0,1 / 2,3): the class of voxel j in byte j.
+template <int MS>
+__device__ __forceinline__ unsigned rx_classify4(const RealDesc& D, int d, F2 ca0, F2 ca1, const float (&val)[MS][4]) {
+  const unsigned kind = D.sur_kind[d];
+  if (kind != RX_ELIGIBLE) return kind == RX_STIFF ? RX_CLASS_PLAIN * 0x01010101u : 0u;
+  const unsigned rm = D.rmask[d];
+  const F2 dca0 = f2(val[0][0], val[0][1]), dca1 = f2(val[0][2], val[0][3]);
+  F2 G0 = f2(0.f, 0.f), G1 = G0;
+#pragma unroll
+  for (int s = 1; s < MS; s++) {
+    if (!(rm >> s & 1u)) continue;
+    const float4 kk = D.rk[d][s];
+    const F2 nkon = f2(kk.x, kk.x), nkoff = f2(kk.y, kk.y), a = f2(kk.z, kk.z), j0 = f2(kk.w, kk.w);
+    G0 = f2_add(G0, buffer_dj2(nkon, nkoff, a, j0, f2(val[s][0], val[s][1]), dca0, ca0));
+    G1 = f2_add(G1, buffer_dj2(nkon, nkoff, a, j0, f2(val[s][2], val[s][3]), dca1, ca1));
+  }
+  const F2 aG0 = f2_abs(G0), aG1 = f2_abs(G1);
+  bool n[4] = {true, true, true, true};
+#pragma unroll
+  for (int s = 1; s < MS; s++) {
+    if (!(rm >> s & 1u)) continue;
+    const float4 kk = D.rk[d][s];
+    const F2 nkon = f2(kk.x, kk.x), nkoff = f2(kk.y, kk.y), a = f2(kk.z, kk.z), j0 = f2(kk.w, kk.w);
+    const F2 cs = f2(D.sur_cs[d][s], D.sur_cs[d][s]);
+    const float thr = D.sur_thr2[d][s];
+    const F2 db0 = f2(val[s][0], val[s][1]), db1 = f2(val[s][2], val[s][3]);
+    const F2 in0 = f2_fma(nkon, ca0, nkoff), in1 = f2_fma(nkon, ca1, nkoff);
+    const F2 dj0 = f2_fma(db0, in0, f2_fma(a, dca0, j0)), dj1 = f2_fma(db1, in1, f2_fma(a, dca1, j0));
+    const F2 l0 = f2_fma(f2_mul(nkon, f2_sub(db0, cs)), aG0, f2_mul(f2_abs(in0), f2_abs(dj0)));
+    const F2 l1 = f2_fma(f2_mul(nkon, f2_sub(db1, cs)), aG1, f2_mul(f2_abs(in1), f2_abs(dj1)));
+    float x0, x1, x2, x3;
+    f2_split(l0, x0, x1);
+    f2_split(l1, x2, x3);
+    n[0] &= x0 <= thr;
+    n[1] &= x1 <= thr;
+    n[2] &= x2 <= thr;
+    n[3] &= x3 <= thr;
+  }
+  unsigned w = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) w |= (n[j] ? RX_CLASS_EXPLICIT : RX_CLASS_NETWORK) << (8 * j);
+  return w;
+}
+
 // INJ = true builds the test hook's variant (csp_test_wait_timeout); the kernel in use is
 // INJ = false, which has none of that code.  FQ: the species that may be stored in fixed
 // point (RealDesc::fixq is a subset), known at compile time so that the code for every
 // other species has no fixed-point branch (a run-time mask over all species cost 18 %).
-template <int MS, int T, bool INJ, unsigned FQ>
+template <int MS, int T, bool INJ, unsigned FQ, bool SUR>
 __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl,
                                                         const int4* __restrict__ units, StagedGeom g,
                                                         int* __restrict__ err) {
@@ -385,6 +431,8 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             o2[0][0] = f2_sub(o2[0][0], dj0);
             o2[0][1] = f2_sub(o2[0][1], dj1);
           }
+          if (SUR && D.sur)
+            *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) = rx_classify4<MS>(D, d0, ca0, ca1, val);
         }
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -604,13 +652,22 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             f2_split(o2[s][0], out[s][0], out[s][1]);
             f2_split(o2[s][1], out[s][2], out[s][3]);
           }
+          if (SUR && D.sur)
+            *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) = rx_classify4<MS>(D, d, ca0, ca1, val);
         }
+        unsigned cls4 = 0;   // SUR, per-voxel reactions: the group's class bytes
 #pragma unroll
         for (int j = 0; j < 4; j++) {
           const int d = dj[j];
           if (si.react && !(si.react_fast && one_dom)) {
             if (si.react_fast) {
               const float ca = __fadd_rn(D.fbase[d][0], val[0][j]);
+              if (SUR && D.sur) {
+                float vj[MS];
+#pragma unroll
+                for (int s = 0; s < MS; s++) vj[s] = val[s][j];
+                cls4 |= rx_classify<MS>(D, d, ca, vj) << (8 * j);
+              }
               const unsigned rm = D.rmask[d];
 #pragma unroll
               for (int s = 1; s < MS; s++) {
@@ -640,6 +697,8 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           }
           if (D.dirichlet && (vzy[j] | xval) != 63u) out[0][j] = D.dinit[d][0];
         }
+        if (SUR && D.sur && si.react_fast && !one_dom)
+          *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) = cls4;
 #pragma unroll
         for (int s = 0; s < MS; s++) {
           if (!(lmask >> s & 1u)) continue;
@@ -671,10 +730,12 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             return dc[ia[kk]];
           };
           float oj[MS];
-          voxel_update<MS>(D, si, valid, valid != 63u, ld, ldd, oj);
+          unsigned cls = RX_CLASS_NONE;
+          voxel_update<MS, SUR>(D, si, valid, valid != 63u, ld, ldd, oj, &cls);
 #pragma unroll
           for (int s = 0; s < MS; s++)
             if (lmask >> s & 1u) D.u[((cur >> s) & 1u) ^ 1u][s][(long long)x * D.P + pj] = oj[s];
+          if (SUR && D.sur && si.react_fast) D.rx_class[(long long)x * D.P + pj] = (unsigned char)cls;
         }
       }
       // plane x-1 is no longer needed: refill its stage with plane x-1+NST.  The barrier
@@ -707,36 +768,45 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
 
 // Launch over the work units [u0, u1) (all units: one step of every realisation; the units
 // of a range of realisations: one step of those only).
-template <int MS, int T, bool INJ, unsigned FQ>
+template <int MS, int T, bool INJ, unsigned FQ, bool SUR>
 cudaError_t staged_launch_t(const StagedPlan& pl, int u0, int u1, const RealDesc* d, RealCtl* c, int* e,
                             cudaStream_t s) {
   if (u1 <= u0) return cudaSuccess;
   StagedGeom g = pl.g;
   g.nunits = u1 - u0;
-  k_voxels_staged<MS, T, INJ, FQ><<<std::min(g.nunits, pl.slots), T, g.smem, s>>>(d, c, pl.d_units + u0, g, e);
+  k_voxels_staged<MS, T, INJ, FQ, SUR><<<std::min(g.nunits, pl.slots), T, g.smem, s>>>(d, c, pl.d_units + u0, g, e);
   return cudaGetLastError();
 }
 
 template <int MS, int T, unsigned FQ, bool WITH_INJ>
 cudaError_t staged_configure(StagedPlan& pl) {
-  cudaError_t e = cudaFuncSetAttribute(k_voxels_staged<MS, T, false, FQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       pl.g.smem);
+  cudaError_t e = cudaFuncSetAttribute(k_voxels_staged<MS, T, false, FQ, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, pl.g.smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_voxels_staged<MS, T, false, FQ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           pl.g.smem);
   if (e != cudaSuccess) return e;
   if (WITH_INJ) {
-    e = cudaFuncSetAttribute(k_voxels_staged<MS, T, WITH_INJ, FQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_voxels_staged<MS, T, WITH_INJ, FQ, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              pl.g.smem);
     if (e != cudaSuccess) return e;
   }
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_voxels_staged<MS, T, false, FQ>, T, pl.g.smem);
+  int per_sm = 0, per_sm_sur = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_voxels_staged<MS, T, false, FQ, false>, T, pl.g.smem);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_sur, k_voxels_staged<MS, T, false, FQ, true>, T,
+                                                    pl.g.smem);
+  if (e != cudaSuccess) return e;
+  per_sm = std::min(per_sm, per_sm_sur);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   pl.slots = per_sm * sms;
-  pl.launch = &staged_launch_t<MS, T, false, FQ>;
-  pl.launch_inject = WITH_INJ ? &staged_launch_t<MS, T, WITH_INJ, FQ> : nullptr;
+  pl.launch = &staged_launch_t<MS, T, false, FQ, false>;
+  pl.launch_sur = &staged_launch_t<MS, T, false, FQ, true>;
+  pl.launch_inject = WITH_INJ ? &staged_launch_t<MS, T, WITH_INJ, FQ, false> : nullptr;
   return cudaSuccess;
 }
 
@@ -804,11 +874,13 @@ inline cudaError_t staged_prepare(StagedPlan& pl) {
   return e;
 }
 
-// One step of the realisations [r0, r1) (default: all).
+// One step of the realisations [r0, r1) (default: all); sur: the variant that classifies
+// voxels for the reaction surrogate.
 inline void staged_launch(const StagedPlan& pl, const RealDesc* d, RealCtl* c, int* e, cudaStream_t s,
-                          bool inject = false, int r0 = 0, int r1 = -1) {
+                          bool inject = false, int r0 = 0, int r1 = -1, bool sur = false) {
   if (r1 < 0) r1 = (int)pl.unit_first.size() - 1;
-  (inject && pl.launch_inject ? pl.launch_inject : pl.launch)(pl, pl.unit_first[r0], pl.unit_first[r1], d, c, e, s);
+  (inject && pl.launch_inject ? pl.launch_inject : sur ? pl.launch_sur : pl.launch)(pl, pl.unit_first[r0],
+                                                                                   pl.unit_first[r1], d, c, e, s);
 }
 
 inline void staged_release(StagedPlan& pl) {

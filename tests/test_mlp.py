@@ -13,7 +13,12 @@ GPU:
     dt_update_react = 10 dt is much closer to the plain integrator than the reference's
     single explicit step (the method without the network);
   * deployment: a simulation with the surrogate stays as close to the run that reacts
-    every step as the plain 10 dt run, or closer, and conserves total calcium.
+    every step as the plain 10 dt run, or closer, and conserves total calcium;
+  * deployment per voxel: one reaction step with the surrogate against the same step
+    without it, from the same state, voxel by voxel against the oracle: the explicit
+    increment stands near equilibrium (bitwise), stiff domains take the FP64 plain
+    integrator, the others the network's increment (or the plain integrator where it is
+    rejected).
 """
 import os
 
@@ -194,6 +199,83 @@ def test_surrogate_deployed_in_simulation(pkg, synth):
     # operator splitting of reacting every 10 steps, which the network does not see)
     assert err_sur.max() < 0.95 * err_plain.max()
     assert np.sqrt(np.mean(rms_sur ** 2)) < np.sqrt(np.mean(rms_plain ** 2))
+
+
+@pytest.mark.gpu
+def test_surrogate_corrections_per_voxel(pkg, synth):
+    """From one state, one reaction step with and without the surrogate: the difference at
+    every voxel is the surrogate's increment minus the explicit one (the reference's update
+    at dt_r), from the old state.  Near equilibrium (every S_s <= 1e-8 by the oracle, away
+    from the bound) the difference is exactly zero; in the stiff jSR it is the FP64 plain
+    integrator's; elsewhere the network's (FP64 forward of the same weights, TF32 on the
+    device) or, where its output fails the residual test, the plain integrator's."""
+    p, _ = trained(pkg, synth)
+    spec, opts = spark_case(synth)
+    a, b = pkg.Simulation(spec, opts), pkg.Simulation(spec, opts)
+    a.set_surrogate(p, 1e-4)
+    n = a.info().reaction_substep
+    k = 40 * n - 1                                             # step k + 1 is a reaction step
+    a.advance(k)
+    b.advance(k)
+    u0 = a.state()
+    nch = a.info().num_channels
+    chans = {bi: a.channels(bi) for bi in range(len(nch)) if nch[bi] > 0}
+    for sim in (a, b):
+        sim.set_state(u0)
+        for bi, st in chans.items():
+            sim.set_channels(bi, st)
+    c0 = a.surrogate_counts()
+    a.advance(1)
+    b.advance(1)
+    c1 = a.surrogate_counts()
+    diff = a.state() - b.state()
+    a.close()
+    b.close()
+    dtr = n * DT
+    vox = spec["voxels"]
+    counts = {"near": 0, "stiff": 0, "network": 0, "plain": 0, "border": 0}
+    for (i, j, l) in np.argwhere(np.isin(vox, [0, 1, 2, 3])):
+        d = int(vox[i, j, l])
+        kk = om.constants(spec, d)
+        on = kk[2] > 0
+        c = float(np.float32(u0[0, i, j, l]))
+        bb = np.zeros(om.NSLOT)
+        bb[:4] = u0[1:5, i, j, l]
+        bb = np.where(on, bb, 0.0)
+        dc_e, db_e = om.plain(kk, 1, dtr, c, bb)
+        got = diff[1:5, i, j, l]
+        tot = np.where(on, kk[2], 1.0)[:4]
+        if not om.eligible(kk, dtr):
+            dc_r, db_r = om.plain(kk, n, DT, c, bb)
+            want = (db_r - db_e)[:4]
+            assert np.all(np.abs(got - want) <= 1e-6 * tot + 1e-3 * np.abs(want)), (d, got, want)
+            counts["stiff"] += 1
+            continue
+        smax = float(np.max(om.scale(kk, dtr, c, bb)))
+        if smax <= 0.5e-8:
+            assert np.all(diff[:, i, j, l] == 0.0), (d, smax, diff[:, i, j, l])
+            counts["near"] += 1
+            continue
+        if smax < 2e-8:
+            counts["border"] += 1                              # FP32 and FP64 may classify either way
+            continue
+        dc_n, db_n, ok = om.surrogate(p.astype(np.float64), kk, d, dtr, c, bb, 1e-4)
+        dc_r, db_r = om.plain(kk, n, DT, c, bb)
+        want_n, want_r = (db_n - db_e)[:4], (db_r - db_e)[:4]
+        # TF32 against FP64: the network's correction t_s errs by ~1e-3 of its scale S_s
+        s_tot = (om.scale(kk, dtr, c, bb) * np.where(on, kk[2], 0.0))[:4]
+        close_n = np.all(np.abs(got - want_n) <= 2e-6 * tot + 2e-2 * np.abs(want_n) + 1e-2 * s_tot)
+        close_r = np.all(np.abs(got - want_r) <= 2e-6 * tot + 1e-3 * np.abs(want_r))
+        assert close_n or close_r, (d, smax, ok, got, want_n, want_r)
+        counts["network" if close_n else "plain"] += 1
+    print(counts, "device counts of the step:", [y - x for x, y in zip(c0, c1)])
+    assert counts["near"] > 0 and counts["stiff"] > 0 and counts["network"] > 0
+    # the step's device counts: every buffer voxel classified, one network evaluation per
+    # voxel away from equilibrium, the jSR on the plain integrator
+    dvx, dev, dfb = [y - x for x, y in zip(c0, c1)]
+    assert dvx == int(np.sum(np.isin(vox, [0, 1, 2, 3])))
+    assert counts["network"] + counts["plain"] <= dev <= counts["network"] + counts["plain"] + counts["border"]
+    assert dfb >= counts["stiff"]
 
 
 @pytest.mark.gpu
