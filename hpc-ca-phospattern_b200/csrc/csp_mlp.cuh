@@ -378,7 +378,7 @@ namespace csp {
 // domain and, with -f, Ca on the outer faces keep the values the voxel kernel gave them.
 //
 // k_react_surrogate: a CTA takes MLP_DEPLOY_SPAN consecutive voxels of one realisation
-// (blockIdx.y); a thread reads the class bytes of MLP_SCAN_VPT consecutive voxels (a warp
+// at a time; a thread reads the class bytes of MLP_SCAN_VPT consecutive voxels (a warp
 // reads 256 contiguous bytes) and lists the voxels to correct (offsets within the CTA's
 // span); the CTA queues its list as tiles of 32 for k_react_network, whose warps share the
 // tiles of every list evenly (stiff domains are spatially clustered: one CTA alone would
@@ -488,77 +488,86 @@ __device__ __forceinline__ bool rx_active(const RealDesc& D, const RealCtl& C) {
   return !C.stopped && D.sur && step_info(D, C.step + 1).react_fast;
 }
 
-// list / counts: per CTA (seg = blockIdx.y * gridDim.x + blockIdx.x) MLP_DEPLOY_SPAN
-// entries and the number used, written on reaction steps; tiles / queue[0]: the tiles of
+// list / counts: per segment (seg = r * chunks + chunk) MLP_DEPLOY_SPAN entries and the
+// number used, written on reaction steps; tiles / queue[0]: the tiles of
 // 32 listed voxels (seg << MLP_TILE_BITS | tile within the list) and their number.
 constexpr int MLP_TILE_BITS = 9;
 static_assert(MLP_DEPLOY_SPAN / 32 <= (1 << MLP_TILE_BITS), "tile index field");
+// Persistent: CTA b takes the segments seg = b, b + gridDim.x, ... (seg = r * chunks +
+// chunk, chunk = the CTA-sized span of realisation r); on a step with no reaction step
+// anywhere the CTAs return after one parallel check of the realisations.
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
-                                                                  const RealCtl* __restrict__ ctl,
-                                                                  unsigned short* __restrict__ list,
+                                                                  const RealCtl* __restrict__ ctl, int chunks,
+                                                                  int nreal, unsigned short* __restrict__ list,
                                                                   unsigned* __restrict__ counts,
                                                                   unsigned* __restrict__ tiles,
                                                                   unsigned* __restrict__ queue,
                                                                   unsigned long long* __restrict__ counters) {
   __shared__ unsigned s_vox, s_list, s_tile0;
-  const RealDesc& D = descs[blockIdx.y];
-  const RealCtl& C = ctl[blockIdx.y];
-  if (!rx_active(D, C)) return;                         // uniform over the block
-  const long long seg = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-  const long long nvox = (long long)D.nx * D.P;
-  const long long vb0 = (long long)blockIdx.x * MLP_DEPLOY_SPAN;
-  if (vb0 >= nvox) {                                    // uniform over the block
-    if (threadIdx.x == 0) counts[seg] = 0;
-    return;
-  }
-  if (threadIdx.x == 0) { s_vox = 0; s_list = 0; }
-  __syncthreads();
-  unsigned short* seg_list = list + seg * MLP_DEPLOY_SPAN;
-  const unsigned char* __restrict__ cls = D.rx_class;
+  bool any = false;
+  for (int r = threadIdx.x; r < nreal; r += MLP_DEPLOY_T) any = any || rx_active(descs[r], ctl[r]);
+  if (!__syncthreads_or(any)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned n_vox = 0;
-  for (int it = 0; it < MLP_DEPLOY_ITER; it++) {
-    const long long w0 = vb0 + (long long)it * MLP_SCAN_VPT * MLP_DEPLOY_T + (long long)warp * MLP_SCAN_VPT * 32;
-    if (w0 >= nvox) break;                               // warp-uniform
-    const long long v = w0 + MLP_SCAN_VPT * lane;
-    uint2 w = make_uint2(0u, 0u);
-    if (v < nvox) w = __ldg(reinterpret_cast<const uint2*>(cls + v));
-    unsigned m = 0;
-#pragma unroll
-    for (int j = 0; j < MLP_SCAN_VPT; j++) {
-      const unsigned c = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
-      if (c) n_vox++;
-      if (c >= RX_CLASS_NETWORK) m |= 1u << j;
+  const long long nseg = (long long)chunks * nreal;
+  for (long long seg = blockIdx.x; seg < nseg; seg += gridDim.x) {
+    const int r = (int)(seg / chunks);
+    const RealDesc& D = descs[r];
+    if (!rx_active(D, ctl[r])) continue;                // uniform over the block
+    const long long nvox = (long long)D.nx * D.P;
+    const long long vb0 = (seg - (long long)r * chunks) * MLP_DEPLOY_SPAN;
+    if (vb0 >= nvox) {                                  // uniform over the block
+      if (threadIdx.x == 0) counts[seg] = 0;
+      continue;
     }
-    if (__any_sync(0xffffffffu, m != 0u)) {
-      // a warp-wide prefix sum of the counts, one shared atomic
-      const unsigned cnt = __popc(m);
-      unsigned incl = cnt;
+    if (threadIdx.x == 0) { s_vox = 0; s_list = 0; }
+    __syncthreads();
+    unsigned short* seg_list = list + seg * MLP_DEPLOY_SPAN;
+    const unsigned char* __restrict__ cls = D.rx_class;
+    unsigned n_vox = 0;
+    for (int it = 0; it < MLP_DEPLOY_ITER; it++) {
+      const long long w0 = vb0 + (long long)it * MLP_SCAN_VPT * MLP_DEPLOY_T + (long long)warp * MLP_SCAN_VPT * 32;
+      if (w0 >= nvox) break;                             // warp-uniform
+      const long long v = w0 + MLP_SCAN_VPT * lane;
+      uint2 w = make_uint2(0u, 0u);
+      if (v < nvox) w = __ldg(reinterpret_cast<const uint2*>(cls + v));
+      unsigned m = 0;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
+      for (int j = 0; j < MLP_SCAN_VPT; j++) {
+        const unsigned c = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
+        if (c) n_vox++;
+        if (c >= RX_CLASS_NETWORK) m |= 1u << j;
       }
-      unsigned base = 0;
-      if (lane == 31) base = atomicAdd(&s_list, incl);
-      unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
-      const unsigned off = (unsigned)(v - vb0);
+      if (__any_sync(0xffffffffu, m != 0u)) {
+        // a warp-wide prefix sum of the counts, one shared atomic
+        const unsigned cnt = __popc(m);
+        unsigned incl = cnt;
 #pragma unroll
-      for (int j = 0; j < MLP_SCAN_VPT; j++)
-        if (m >> j & 1u) seg_list[pos++] = (unsigned short)(off + j);
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += t;
+        }
+        unsigned base = 0;
+        if (lane == 31) base = atomicAdd(&s_list, incl);
+        unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
+        const unsigned off = (unsigned)(v - vb0);
+#pragma unroll
+        for (int j = 0; j < MLP_SCAN_VPT; j++)
+          if (m >> j & 1u) seg_list[pos++] = (unsigned short)(off + j);
+      }
     }
+    if (n_vox) atomicAdd(&s_vox, n_vox);
+    __syncthreads();
+    const unsigned ntile = (s_list + 31u) / 32u;
+    if (threadIdx.x == 0) {
+      counts[seg] = s_list;
+      if (ntile) s_tile0 = atomicAdd(&queue[0], ntile);
+      if (s_vox) atomicAdd(&counters[0], (unsigned long long)s_vox);
+    }
+    __syncthreads();
+    for (unsigned j = threadIdx.x; j < ntile; j += MLP_DEPLOY_T)
+      tiles[s_tile0 + j] = (unsigned)seg << MLP_TILE_BITS | j;
+    __syncthreads();                                     // s_* are reused by the next segment
   }
-  if (n_vox) atomicAdd(&s_vox, n_vox);
-  __syncthreads();
-  const unsigned ntile = (s_list + 31u) / 32u;
-  if (threadIdx.x == 0) {
-    counts[seg] = s_list;
-    if (ntile) s_tile0 = atomicAdd(&queue[0], ntile);
-    if (s_vox) atomicAdd(&counters[0], (unsigned long long)s_vox);
-  }
-  __syncthreads();
-  for (unsigned j = threadIdx.x; j < ntile; j += MLP_DEPLOY_T)
-    tiles[s_tile0 + j] = (unsigned)seg << MLP_TILE_BITS | j;
 }
 
 // The voxels that k_react_surrogate listed, in tiles of 32: network voxels on the tensor
@@ -598,11 +607,32 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
     const unsigned t_lo = w0 * per, t_hi = min(total, t_lo + per);
     unsigned n_net = 0, n_fall = 0;
     int rc = -1;                                         // realisation whose constants are cached
-    for (unsigned tw = t_lo; tw < t_hi; tw++) {
+    // a tile's chain of dependent loads (tile, list entry, domain and class bytes), fetched
+    // one tile ahead so that it is in flight while the previous tile runs
+    struct Tile {
+      long long seg, v;
+      int r, d;
+      bool have, net;
+    };
+    auto fetch = [&](unsigned tw) {
+      Tile f;
       const unsigned td = tiles[tw];
-      const long long seg = td >> MLP_TILE_BITS;
+      f.seg = td >> MLP_TILE_BITS;
       const unsigned t0 = (td & ((1u << MLP_TILE_BITS) - 1u)) * 32u;
-      const int r = (int)(seg / chunks);
+      f.r = (int)(f.seg / chunks);
+      const RealDesc& D = descs[f.r];
+      f.have = t0 + lane < counts[f.seg];
+      f.v = (f.seg - (long long)f.r * chunks) * MLP_DEPLOY_SPAN + (f.have ? list[f.seg * MLP_DEPLOY_SPAN + t0 + lane] : 0);
+      f.d = f.have ? (D.dom[f.v] & DOMAIN_BITS) : 0;
+      f.net = f.have && D.rx_class[f.v] == RX_CLASS_NETWORK;
+      return f;
+    };
+    Tile nx{};
+    if (t_lo < t_hi) nx = fetch(t_lo);
+    for (unsigned tw = t_lo; tw < t_hi; tw++) {
+      const Tile cu = nx;
+      if (tw + 1 < t_hi) nx = fetch(tw + 1);
+      const int r = cu.r;
       const RealDesc& D = descs[r];
       if (r != rc) {                                     // warp-uniform
         __syncwarp();
@@ -617,14 +647,11 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
         __syncwarp();
         rc = r;
       }
-      const unsigned cnt = counts[seg];
-      const long long vb0 = (seg - (long long)r * chunks) * MLP_DEPLOY_SPAN;
       const float dtr = (float)(D.dt * D.reaction_substep);
       const unsigned fqs = D.fixq;
-      const bool have = t0 + lane < cnt;
-      const long long v = vb0 + (have ? list[seg * MLP_DEPLOY_SPAN + t0 + lane] : 0);
-      const int d = have ? (D.dom[v] & DOMAIN_BITS) : 0;
-      const bool net = have && D.rx_class[v] == RX_CLASS_NETWORK;
+      const bool have = cu.have, net = cu.net;
+      const long long v = cu.v;
+      const int d = cu.d;
       const RxDom& K = s_dom[warp][d];
       float dev[MLP_RX_NS], c = 0.f, b[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
 #pragma unroll

@@ -1080,8 +1080,10 @@ static NetworkKernel network_kernel(unsigned fq) {
 static void launch_surrogate(csp_handle* h, int r0, int r1) {
   if (!h->surrogate) return;
   const int chunks = (int)((h->max_field + MLP_DEPLOY_SPAN - 1) / MLP_DEPLOY_SPAN);
-  k_react_surrogate<<<dim3((unsigned)chunks, (unsigned)(r1 - r0)), MLP_DEPLOY_T, 0, h->stream>>>(
-      h->d_desc + r0, h->d_ctl + r0, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles, h->d_sur_queue, h->d_mlp_cnt);
+  const long long nseg = (long long)chunks * (r1 - r0);
+  k_react_surrogate<<<(unsigned)std::min<long long>(nseg, 2 * h->sur_network_ctas), MLP_DEPLOY_T, 0, h->stream>>>(
+      h->d_desc + r0, h->d_ctl + r0, chunks, r1 - r0, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles, h->d_sur_queue,
+      h->d_mlp_cnt);
   network_kernel(h->surrogate_fq)<<<h->sur_network_ctas, MLP_DEPLOY_T, MLP_NETWORK_SMEM, h->stream>>>(
       h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
       h->d_sur_queue, chunks, h->d_mlp_cnt);

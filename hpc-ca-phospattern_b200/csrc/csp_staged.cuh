@@ -145,22 +145,16 @@ __device__ __forceinline__ unsigned ld_u32_any(const unsigned char* p) {
 }
 
 // rx_classify on the four voxels of a group in one domain d, in two-lane FP32 with the
-// same rounding (ca0 / ca1: Ca of voxels 0,1 / 2,3): the class of voxel j in byte j.
+// same rounding (ca0 / ca1: Ca of voxels 0,1 / 2,3; G0 / G1: their sums of the increments
+// dJ_s in slot order, accumulated by the reaction loop that applies them): the class of
+// voxel j in byte j.
 template <int MS>
-__device__ __forceinline__ unsigned rx_classify4(const RealDesc& D, int d, F2 ca0, F2 ca1, const float (&val)[MS][4]) {
+__device__ __forceinline__ unsigned rx_classify4(const RealDesc& D, int d, F2 ca0, F2 ca1, const float (&val)[MS][4],
+                                                 F2 G0, F2 G1) {
   const unsigned kind = D.sur_kind[d];
   if (kind != RX_ELIGIBLE) return kind == RX_STIFF ? RX_CLASS_PLAIN * 0x01010101u : 0u;
   const unsigned rm = D.rmask[d];
   const F2 dca0 = f2(val[0][0], val[0][1]), dca1 = f2(val[0][2], val[0][3]);
-  F2 G0 = f2(0.f, 0.f), G1 = G0;
-#pragma unroll
-  for (int s = 1; s < MS; s++) {
-    if (!(rm >> s & 1u)) continue;
-    const float4 kk = D.rk[d][s];
-    const F2 nkon = f2(kk.x, kk.x), nkoff = f2(kk.y, kk.y), a = f2(kk.z, kk.z), j0 = f2(kk.w, kk.w);
-    G0 = f2_add(G0, buffer_dj2(nkon, nkoff, a, j0, f2(val[s][0], val[s][1]), dca0, ca0));
-    G1 = f2_add(G1, buffer_dj2(nkon, nkoff, a, j0, f2(val[s][2], val[s][3]), dca1, ca1));
-  }
   const F2 aG0 = f2_abs(G0), aG1 = f2_abs(G1);
   bool n[4] = {true, true, true, true};
 #pragma unroll
@@ -419,6 +413,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           const float cb = D.fbase[d0][0];
           const F2 ca0 = f2_add(f2(cb, cb), dca0), ca1 = f2_add(f2(cb, cb), dca1);
           const unsigned rm = D.rmask[d0];
+          F2 G0 = f2(0.f, 0.f), G1 = G0;    // SUR: sums of the increments
 #pragma unroll
           for (int s = 1; s < MS; s++) {
             if (!(rm >> s & 1u)) continue;
@@ -430,9 +425,14 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             o2[s][1] = f2_add(o2[s][1], dj1);
             o2[0][0] = f2_sub(o2[0][0], dj0);
             o2[0][1] = f2_sub(o2[0][1], dj1);
+            if (SUR) {
+              G0 = f2_add(G0, dj0);
+              G1 = f2_add(G1, dj1);
+            }
           }
           if (SUR && D.sur)
-            *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) = rx_classify4<MS>(D, d0, ca0, ca1, val);
+            *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) =
+                rx_classify4<MS>(D, d0, ca0, ca1, val, G0, G1);
         }
 #pragma unroll
         for (int s = 0; s < MS; s++) {
@@ -635,6 +635,7 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
           const float cb = D.fbase[d][0];
           const F2 ca0 = f2_add(f2(cb, cb), dca0), ca1 = f2_add(f2(cb, cb), dca1);
           const unsigned rm = D.rmask[d];
+          F2 G0 = f2(0.f, 0.f), G1 = G0;    // SUR: sums of the increments
 #pragma unroll
           for (int s = 1; s < MS; s++) {
             if (!(rm >> s & 1u)) continue;
@@ -646,6 +647,10 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             o2[s][1] = f2_add(o2[s][1], dj1);
             o2[0][0] = f2_sub(o2[0][0], dj0);
             o2[0][1] = f2_sub(o2[0][1], dj1);
+            if (SUR) {
+              G0 = f2_add(G0, dj0);
+              G1 = f2_add(G1, dj1);
+            }
           }
 #pragma unroll
           for (int s = 0; s < MS; s++) {
@@ -653,7 +658,8 @@ __global__ void __launch_bounds__(T, 2) k_voxels_staged(const RealDesc* __restri
             f2_split(o2[s][1], out[s][2], out[s][3]);
           }
           if (SUR && D.sur)
-            *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) = rx_classify4<MS>(D, d, ca0, ca1, val);
+            *reinterpret_cast<unsigned*>(D.rx_class + (long long)x * D.P + p0) =
+                rx_classify4<MS>(D, d, ca0, ca1, val, G0, G1);
         }
         unsigned cls4 = 0;   // SUR, per-voxel reactions: the group's class bytes
 #pragma unroll
