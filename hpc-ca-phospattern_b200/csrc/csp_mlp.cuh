@@ -121,13 +121,19 @@ __host__ __device__ inline void rx_plain(const RxConst& k, int n, double h, doub
   double b[MLP_SLOTS];
   for (int q = 0; q < MLP_SLOTS; q++) b[q] = b0[q];
   double cc = c;
+  // absent slots (tot = 0) would add exact zeros: they are skipped
+  bool on[MLP_SLOTS];
+  for (int q = 0; q < MLP_SLOTS; q++) on[q] = k.tot[q] > 0.f;
   for (int i = 0; i < n; i++) {
     double g[MLP_SLOTS], sg = 0.0;
     for (int q = 0; q < MLP_SLOTS; q++) {
-      g[q] = k.tot[q] > 0.f ? rx_g<double>(k, q, cc, b[q]) : 0.0;
+      g[q] = 0.0;
+      if (!on[q]) continue;
+      g[q] = rx_g<double>(k, q, cc, b[q]);
       sg += g[q];
     }
-    for (int q = 0; q < MLP_SLOTS; q++) b[q] += h * g[q];
+    for (int q = 0; q < MLP_SLOTS; q++)
+      if (on[q]) b[q] += h * g[q];
     cc -= h * sg;
   }
   for (int q = 0; q < MLP_SLOTS; q++) db[q] = b[q] - b0[q];
@@ -380,11 +386,12 @@ namespace csp {
 // k_react_surrogate: a CTA takes MLP_DEPLOY_SPAN consecutive voxels of one realisation
 // at a time; a thread reads the class bytes of MLP_SCAN_VPT consecutive voxels (a warp
 // reads 256 contiguous bytes) and lists the voxels to correct (offsets within the CTA's
-// span); the CTA queues its list as tiles of 32 for k_react_network, whose warps share the
-// tiles of every list evenly (stiff domains are spatially clustered: one CTA alone would
-// run their FP64 integrations one after the other).  counters[0] += voxels with
-// buffers, counters[1] += voxels the network ran for, counters[2] += voxels that took
-// the plain integrator.
+// span), network and plain-integrator voxels apart, queued as tiles of 32: network tiles
+// for k_react_network (tensor cores), plain tiles for k_react_plain (FP64).  Both
+// spread every list's tiles over all their warps: stiff domains are spatially clustered,
+// and one CTA alone would run their integrations one after the other.  counters[0] +=
+// voxels with buffers, counters[1] += voxels the network ran for, counters[2] += voxels
+// that took the plain integrator.
 constexpr int MLP_DEPLOY_T = 256;
 constexpr int MLP_SCAN_VPT = 8;          // class bytes per thread and iteration
 constexpr int MLP_DEPLOY_ITER = 8;
@@ -488,22 +495,28 @@ __device__ __forceinline__ bool rx_active(const RealDesc& D, const RealCtl& C) {
   return !C.stopped && D.sur && step_info(D, C.step + 1).react_fast;
 }
 
-// list / counts: per segment (seg = r * chunks + chunk) MLP_DEPLOY_SPAN entries and the
-// number used, written on reaction steps; tiles / queue[0]: the tiles of
-// 32 listed voxels (seg << MLP_TILE_BITS | tile within the list) and their number.
+// list / counts: per segment (seg = r * chunks + chunk) MLP_DEPLOY_SPAN entries: the
+// network voxels from the front, the plain-integrator voxels from the back;
+// counts[2 seg] / counts[2 seg + 1] their numbers, written on reaction steps.  tiles /
+// queue[0]: the network tiles of 32 listed voxels (seg << MLP_TILE_BITS | tile within
+// the list) and their number; tiles + MLP_PLAIN_TILES / queue[2]: the same for the plain
+// integrator.  queue[1] / queue[3]: CTAs of k_react_network / k_react_plain done.
 constexpr int MLP_TILE_BITS = 9;
 static_assert(MLP_DEPLOY_SPAN / 32 <= (1 << MLP_TILE_BITS), "tile index field");
+
 // Persistent: CTA b takes the segments seg = b, b + gridDim.x, ... (seg = r * chunks +
 // chunk, chunk = the CTA-sized span of realisation r); on a step with no reaction step
-// anywhere the CTAs return after one parallel check of the realisations.
+// anywhere the CTAs return after one parallel check of the realisations.  tiles_plain =
+// the plain-integrator half of the tile array.
 __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc* __restrict__ descs,
                                                                   const RealCtl* __restrict__ ctl, int chunks,
                                                                   int nreal, unsigned short* __restrict__ list,
                                                                   unsigned* __restrict__ counts,
                                                                   unsigned* __restrict__ tiles,
+                                                                  unsigned* __restrict__ tiles_plain,
                                                                   unsigned* __restrict__ queue,
                                                                   unsigned long long* __restrict__ counters) {
-  __shared__ unsigned s_vox, s_list, s_tile0;
+  __shared__ unsigned s_vox, s_list[2], s_tile0[2];
   bool any = false;
   for (int r = threadIdx.x; r < nreal; r += MLP_DEPLOY_T) any = any || rx_active(descs[r], ctl[r]);
   if (!__syncthreads_or(any)) return;
@@ -516,10 +529,10 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
     const long long nvox = (long long)D.nx * D.P;
     const long long vb0 = (seg - (long long)r * chunks) * MLP_DEPLOY_SPAN;
     if (vb0 >= nvox) {                                  // uniform over the block
-      if (threadIdx.x == 0) counts[seg] = 0;
+      if (threadIdx.x == 0) counts[2 * seg] = counts[2 * seg + 1] = 0;
       continue;
     }
-    if (threadIdx.x == 0) { s_vox = 0; s_list = 0; }
+    if (threadIdx.x == 0) { s_vox = 0; s_list[0] = s_list[1] = 0; }
     __syncthreads();
     unsigned short* seg_list = list + seg * MLP_DEPLOY_SPAN;
     const unsigned char* __restrict__ cls = D.rx_class;
@@ -530,16 +543,20 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
       const long long v = w0 + MLP_SCAN_VPT * lane;
       uint2 w = make_uint2(0u, 0u);
       if (v < nvox) w = __ldg(reinterpret_cast<const uint2*>(cls + v));
-      unsigned m = 0;
+      unsigned m[2] = {0u, 0u};                          // network, plain integrator
 #pragma unroll
       for (int j = 0; j < MLP_SCAN_VPT; j++) {
         const unsigned c = ((j < 4 ? w.x : w.y) >> (8 * (j & 3))) & 0xffu;
         if (c) n_vox++;
-        if (c >= RX_CLASS_NETWORK) m |= 1u << j;
+        if (c == RX_CLASS_NETWORK) m[0] |= 1u << j;
+        if (c == RX_CLASS_PLAIN) m[1] |= 1u << j;
       }
-      if (__any_sync(0xffffffffu, m != 0u)) {
+      const unsigned off = (unsigned)(v - vb0);
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        if (!__any_sync(0xffffffffu, m[k] != 0u)) continue;
         // a warp-wide prefix sum of the counts, one shared atomic
-        const unsigned cnt = __popc(m);
+        const unsigned cnt = __popc(m[k]);
         unsigned incl = cnt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -547,38 +564,95 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T) k_react_surrogate(const RealDesc
           if (lane >= o) incl += t;
         }
         unsigned base = 0;
-        if (lane == 31) base = atomicAdd(&s_list, incl);
+        if (lane == 31) base = atomicAdd(&s_list[k], incl);
         unsigned pos = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
-        const unsigned off = (unsigned)(v - vb0);
 #pragma unroll
-        for (int j = 0; j < MLP_SCAN_VPT; j++)
-          if (m >> j & 1u) seg_list[pos++] = (unsigned short)(off + j);
+        for (int j = 0; j < MLP_SCAN_VPT; j++) {
+          if (!(m[k] >> j & 1u)) continue;
+          seg_list[k == 0 ? pos : MLP_DEPLOY_SPAN - 1 - pos] = (unsigned short)(off + j);
+          pos++;
+        }
       }
     }
     if (n_vox) atomicAdd(&s_vox, n_vox);
     __syncthreads();
-    const unsigned ntile = (s_list + 31u) / 32u;
+    const unsigned nt0 = (s_list[0] + 31u) / 32u, nt1 = (s_list[1] + 31u) / 32u;
     if (threadIdx.x == 0) {
-      counts[seg] = s_list;
-      if (ntile) s_tile0 = atomicAdd(&queue[0], ntile);
+      counts[2 * seg] = s_list[0];
+      counts[2 * seg + 1] = s_list[1];
+      if (nt0) s_tile0[0] = atomicAdd(&queue[0], nt0);
+      if (nt1) s_tile0[1] = atomicAdd(&queue[2], nt1);
       if (s_vox) atomicAdd(&counters[0], (unsigned long long)s_vox);
     }
     __syncthreads();
-    for (unsigned j = threadIdx.x; j < ntile; j += MLP_DEPLOY_T)
-      tiles[s_tile0 + j] = (unsigned)seg << MLP_TILE_BITS | j;
+    for (unsigned j = threadIdx.x; j < nt0 + nt1; j += MLP_DEPLOY_T) {
+      if (j < nt0) tiles[s_tile0[0] + j] = (unsigned)seg << MLP_TILE_BITS | j;
+      else tiles_plain[s_tile0[1] + (j - nt0)] = (unsigned)seg << MLP_TILE_BITS | (j - nt0);
+    }
     __syncthreads();                                     // s_* are reused by the next segment
   }
 }
 
-// The voxels that k_react_surrogate listed, in tiles of 32: network voxels on the tensor
-// cores (a tile runs the network when any of its voxels needs it; a rejected output takes
-// the plain integrator), stiff-domain voxels on the plain integrator (FP64), one per lane;
-// each is corrected from the old state (rx_correct).  Persistent CTAs: warp w of the grid takes a contiguous range of the queued tiles (tiles
-// of one list are queued together, so a warp's realisation rarely changes; its domain
-// constants and field pointers are cached per warp in shared memory); a CTA without a
-// tile returns before it loads the weights.  The last CTA to finish empties the queue
-// (queue[0]: tiles, queue[1]: CTAs done) for the next step.  chunks = k_react_surrogate's
-// gridDim.x.
+// A warp's cache of one realisation (its domain constants and field pointers), filled by
+// its lanes 0..7 and 8..13 when the realisation changes.
+struct RxWarpCache {
+  RxDom dom[8];
+  const float* uo[MLP_RX_NS];
+  float* un[MLP_RX_NS];
+};
+__device__ __forceinline__ void rx_cache_fill(const RealDesc& D, const RealCtl& C, RxWarpCache& W, int lane) {
+  __syncwarp();
+  if (lane < 8) {
+    rx_dom_fill(D, lane, W.dom[lane]);
+  } else if (lane < 8 + MLP_RX_NS) {
+    const int t = lane - 8;
+    const unsigned cur = C.cur_mask[C.step & 1];
+    W.uo[t] = t < D.ns ? D.u[(cur >> t) & 1u][t] : nullptr;
+    W.un[t] = t < D.ns ? D.u[((cur >> t) & 1u) ^ 1u][t] : nullptr;
+  }
+  __syncwarp();
+}
+
+// One tile's chain of dependent loads (tile, list entry, domain byte); back = the entry
+// counts from the back of the list (plain-integrator voxels).
+struct RxTile {
+  long long v;
+  int r, d;
+  bool have;
+};
+__device__ __forceinline__ RxTile rx_fetch_tile(const RealDesc* __restrict__ descs,
+                                                const unsigned short* __restrict__ list,
+                                                const unsigned* __restrict__ counts, unsigned td, int chunks,
+                                                int back, int lane) {
+  RxTile f;
+  const long long seg = td >> MLP_TILE_BITS;
+  const unsigned i = (td & ((1u << MLP_TILE_BITS) - 1u)) * 32u + lane;
+  f.r = (int)(seg / chunks);
+  f.have = i < counts[2 * seg + back];
+  const unsigned e = f.have ? list[seg * MLP_DEPLOY_SPAN + (back ? MLP_DEPLOY_SPAN - 1 - i : i)] : 0u;
+  f.v = (seg - (long long)f.r * chunks) * MLP_DEPLOY_SPAN + e;
+  f.d = f.have ? (descs[f.r].dom[f.v] & DOMAIN_BITS) : 0;
+  return f;
+}
+
+// Empties a queue for the next step once every CTA of the grid has read it (the last one
+// to finish resets it): q[0] tiles, q[1] CTAs done.
+__device__ __forceinline__ void rx_queue_done(unsigned* q) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&q[1], 1u) == gridDim.x - 1) {
+      q[0] = 0;
+      q[1] = 0;
+    }
+  }
+}
+
+// The network voxels that k_react_surrogate listed, in tiles of 32 on the tensor cores (a
+// rejected output takes the plain integrator), each corrected from the old state
+// (rx_correct).  Persistent CTAs: warp w of the grid takes a contiguous range of the
+// queued tiles (tiles of one list are queued together, so a warp's realisation rarely
+// changes); a CTA without a tile returns before it loads the weights.  The next tile's
+// index chain is fetched while a tile runs.  chunks = the segments per realisation.
 template <unsigned FQ>
 __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDesc* __restrict__ descs,
                                                                    const RealCtl* __restrict__ ctl,
@@ -592,9 +666,7 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
   MlpTC& T = *reinterpret_cast<MlpTC*>(dsm);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* stage = dsm + sizeof(MlpTC) / sizeof(float) + warp * MLP_TC_STAGE;
-  __shared__ RxDom s_dom[MLP_DEPLOY_T / 32][8];        // per warp: the constants of its realisation
-  __shared__ const float* s_uo[MLP_DEPLOY_T / 32][MLP_RX_NS];
-  __shared__ float* s_un[MLP_DEPLOY_T / 32][MLP_RX_NS];
+  __shared__ RxWarpCache s_wc[MLP_DEPLOY_T / 32];
   __shared__ unsigned s_net, s_fall, s_total;
   if (threadIdx.x == 0) { s_total = queue[0]; s_net = 0; s_fall = 0; }
   __syncthreads();
@@ -603,74 +675,41 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
   if (blockIdx.x * (MLP_DEPLOY_T / 32) * per < total) {  // uniform over the block
     mlp_tc_load(T, params);
     __syncthreads();
-    const unsigned w0 = blockIdx.x * (MLP_DEPLOY_T / 32) + warp;
-    const unsigned t_lo = w0 * per, t_hi = min(total, t_lo + per);
+    RxWarpCache& W = s_wc[warp];
+    const unsigned t_lo = (blockIdx.x * (MLP_DEPLOY_T / 32) + warp) * per, t_hi = min(total, t_lo + per);
     unsigned n_net = 0, n_fall = 0;
     int rc = -1;                                         // realisation whose constants are cached
-    // a tile's chain of dependent loads (tile, list entry, domain and class bytes), fetched
-    // one tile ahead so that it is in flight while the previous tile runs
-    struct Tile {
-      long long seg, v;
-      int r, d;
-      bool have, net;
-    };
-    auto fetch = [&](unsigned tw) {
-      Tile f;
-      const unsigned td = tiles[tw];
-      f.seg = td >> MLP_TILE_BITS;
-      const unsigned t0 = (td & ((1u << MLP_TILE_BITS) - 1u)) * 32u;
-      f.r = (int)(f.seg / chunks);
-      const RealDesc& D = descs[f.r];
-      f.have = t0 + lane < counts[f.seg];
-      f.v = (f.seg - (long long)f.r * chunks) * MLP_DEPLOY_SPAN + (f.have ? list[f.seg * MLP_DEPLOY_SPAN + t0 + lane] : 0);
-      f.d = f.have ? (D.dom[f.v] & DOMAIN_BITS) : 0;
-      f.net = f.have && D.rx_class[f.v] == RX_CLASS_NETWORK;
-      return f;
-    };
-    Tile nx{};
-    if (t_lo < t_hi) nx = fetch(t_lo);
+    RxTile nx{};
+    if (t_lo < t_hi) nx = rx_fetch_tile(descs, list, counts, tiles[t_lo], chunks, 0, lane);
     for (unsigned tw = t_lo; tw < t_hi; tw++) {
-      const Tile cu = nx;
-      if (tw + 1 < t_hi) nx = fetch(tw + 1);
-      const int r = cu.r;
-      const RealDesc& D = descs[r];
-      if (r != rc) {                                     // warp-uniform
-        __syncwarp();
-        if (lane < 8) {
-          rx_dom_fill(D, lane, s_dom[warp][lane]);
-        } else if (lane < 8 + MLP_RX_NS) {
-          const int t = lane - 8;
-          const unsigned cur = ctl[r].cur_mask[ctl[r].step & 1];
-          s_uo[warp][t] = t < D.ns ? D.u[(cur >> t) & 1u][t] : nullptr;
-          s_un[warp][t] = t < D.ns ? D.u[((cur >> t) & 1u) ^ 1u][t] : nullptr;
-        }
-        __syncwarp();
-        rc = r;
+      const RxTile cu = nx;
+      if (tw + 1 < t_hi) nx = rx_fetch_tile(descs, list, counts, tiles[tw + 1], chunks, 0, lane);
+      const RealDesc& D = descs[cu.r];
+      if (cu.r != rc) {                                  // warp-uniform
+        rx_cache_fill(D, ctl[cu.r], W, lane);
+        rc = cu.r;
       }
       const float dtr = (float)(D.dt * D.reaction_substep);
       const unsigned fqs = D.fixq;
-      const bool have = cu.have, net = cu.net;
-      const long long v = cu.v;
-      const int d = cu.d;
-      const RxDom& K = s_dom[warp][d];
+      const RxDom& K = W.dom[cu.d];
       float dev[MLP_RX_NS], c = 0.f, b[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
 #pragma unroll
       for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
 #pragma unroll
       for (int q = 0; q < MLP_SLOTS; q++) b[q] = 0.f;
-      if (have) {
-        rx_load_old<FQ>(K, s_uo[warp], v, fqs, dev, c, b);
-        if (net) rx_features(K.k, d, dtr, c, b, x);
+      if (cu.have) {
+        rx_load_old<FQ>(K, W.uo, cu.v, fqs, dev, c, b);
+        rx_features(K.k, cu.d, dtr, c, b, x);
       }
-      if (__any_sync(0xffffffffu, net)) mlp_forward_tc(T, stage, x, t);
-      if (have) {
+      mlp_forward_tc(T, stage, x, t);
+      if (cu.have) {
         float dc, db[MLP_SLOTS];
-        if (net) n_net++;
-        if (!net || !rx_apply_output(K.k, dtr, c, b, t, tol, dc, db)) {
+        n_net++;
+        if (!rx_apply_output(K.k, dtr, c, b, t, tol, dc, db)) {
           n_fall++;
           rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
         }
-        rx_correct<FQ>(K, D, s_un[warp], v, fqs, dev, c, db, dc);
+        rx_correct<FQ>(K, D, W.un, cu.v, fqs, dev, c, db, dc);
       }
     }
     if (n_net) atomicAdd(&s_net, n_net);
@@ -681,14 +720,59 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
       if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
     }
   }
-  if (threadIdx.x == 0) {
-    // every CTA has read queue[0] before it counts itself done
-    __threadfence();
-    if (atomicAdd(&queue[1], 1u) == gridDim.x - 1) {
-      queue[0] = 0;
-      queue[1] = 0;
+  rx_queue_done(queue);
+}
+
+// The plain-integrator voxels that k_react_surrogate listed (stiff domains), one per lane
+// (FP64), each corrected from the old state.  No weights and no activation tiles: the
+// CTAs hold a few KB of shared memory, so many more warps per SM hide the latency of
+// the voxels' dependent loads than the network kernel can.  Same tile distribution as
+// k_react_network, over the queue q (q[0] tiles, q[1] CTAs done).
+template <unsigned FQ>
+__global__ void __launch_bounds__(MLP_DEPLOY_T, 4) k_react_plain(const RealDesc* __restrict__ descs,
+                                                              const RealCtl* __restrict__ ctl,
+                                                              const unsigned short* __restrict__ list,
+                                                              const unsigned* __restrict__ counts,
+                                                              const unsigned* __restrict__ tiles,
+                                                              unsigned* __restrict__ q, int chunks,
+                                                              unsigned long long* __restrict__ counters) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ RxWarpCache s_wc[MLP_DEPLOY_T / 32];
+  __shared__ unsigned s_fall, s_total;
+  if (threadIdx.x == 0) { s_total = q[0]; s_fall = 0; }
+  __syncthreads();
+  const unsigned total = s_total;
+  const unsigned nw = gridDim.x * (MLP_DEPLOY_T / 32), per = (total + nw - 1) / nw;
+  if (blockIdx.x * (MLP_DEPLOY_T / 32) * per < total) {  // uniform over the block
+    RxWarpCache& W = s_wc[warp];
+    const unsigned t_lo = (blockIdx.x * (MLP_DEPLOY_T / 32) + warp) * per, t_hi = min(total, t_lo + per);
+    unsigned n_fall = 0;
+    int rc = -1;
+    RxTile nx{};
+    if (t_lo < t_hi) nx = rx_fetch_tile(descs, list, counts, tiles[t_lo], chunks, 1, lane);
+    for (unsigned tw = t_lo; tw < t_hi; tw++) {
+      const RxTile cu = nx;
+      if (tw + 1 < t_hi) nx = rx_fetch_tile(descs, list, counts, tiles[tw + 1], chunks, 1, lane);
+      const RealDesc& D = descs[cu.r];
+      if (cu.r != rc) {                                  // warp-uniform
+        rx_cache_fill(D, ctl[cu.r], W, lane);
+        rc = cu.r;
+      }
+      if (cu.have) {
+        const RxDom& K = W.dom[cu.d];
+        const unsigned fqs = D.fixq;
+        float dev[MLP_RX_NS], c, b[MLP_SLOTS], dc, db[MLP_SLOTS];
+        rx_load_old<FQ>(K, W.uo, cu.v, fqs, dev, c, b);
+        n_fall++;
+        rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
+        rx_correct<FQ>(K, D, W.un, cu.v, fqs, dev, c, db, dc);
+      }
     }
+    if (n_fall) atomicAdd(&s_fall, n_fall);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
   }
+  rx_queue_done(q);
 }
 
 // Forward passes for checks: y[n][5] of x[n][8], FP32 (tc = 0) or tensor cores (tc = 1,

@@ -185,11 +185,13 @@ struct csp_handle {
   float* d_mlp = nullptr;                   // MLP_NPARAM parameters
   unsigned long long* d_mlp_cnt = nullptr;  // voxels, network evaluations, fallbacks
   unsigned short* d_sur_list = nullptr;     // per k_react_surrogate CTA: its network voxels
-  unsigned* d_sur_counts = nullptr;         // per k_react_surrogate CTA: listed voxels
-  unsigned* d_sur_tiles = nullptr;          // tiles of 32 listed voxels (k_react_network's work)
-  unsigned* d_sur_queue = nullptr;          // tiles queued, k_react_network CTAs done
+  unsigned* d_sur_counts = nullptr;         // per segment: listed network / plain-integrator voxels
+  unsigned* d_sur_tiles = nullptr;          // tiles of 32 listed voxels: network half, then plain half
+  long long sur_tile_cap = 0;               // tiles per half
+  unsigned* d_sur_queue = nullptr;          // network tiles, k_react_network CTAs done, plain tiles, k_react_plain CTAs done
   unsigned char* d_rx_class = nullptr;      // surrogate class bytes (RealDesc::rx_class), layout of d_dom
   int sur_network_ctas = 0;                 // persistent CTAs of k_react_network
+  int sur_plain_ctas = 0;                   // persistent CTAs of k_react_plain
   // training pairs harvested from the fields (csp_mlp_harvest): features [cap][8], targets [cap][5]
   float* d_hx = nullptr;
   float* d_ht = nullptr;
@@ -1076,13 +1078,23 @@ using NetworkKernel = void (*)(const RealDesc*, const RealCtl*, const float*, fl
 static NetworkKernel network_kernel(unsigned fq) {
   return fq == 0u ? k_react_network<0u> : fq == 0x10u ? k_react_network<0x10u> : k_react_network<0x3Eu>;
 }
+using PlainKernel = void (*)(const RealDesc*, const RealCtl*, const unsigned short*, const unsigned*,
+                             const unsigned*, unsigned*, int, unsigned long long*);
+static PlainKernel plain_kernel(unsigned fq) {
+  return fq == 0u ? k_react_plain<0u> : fq == 0x10u ? k_react_plain<0x10u> : k_react_plain<0x3Eu>;
+}
 
 static void launch_surrogate(csp_handle* h, int r0, int r1) {
   if (!h->surrogate) return;
   const int chunks = (int)((h->max_field + MLP_DEPLOY_SPAN - 1) / MLP_DEPLOY_SPAN);
   const long long nseg = (long long)chunks * (r1 - r0);
+  unsigned* tiles_plain = h->d_sur_tiles + h->sur_tile_cap;
   k_react_surrogate<<<(unsigned)std::min<long long>(nseg, 2 * h->sur_network_ctas), MLP_DEPLOY_T, 0, h->stream>>>(
-      h->d_desc + r0, h->d_ctl + r0, chunks, r1 - r0, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles, h->d_sur_queue,
+      h->d_desc + r0, h->d_ctl + r0, chunks, r1 - r0, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles, tiles_plain,
+      h->d_sur_queue,
+      h->d_mlp_cnt);
+  plain_kernel(h->surrogate_fq)<<<h->sur_plain_ctas, MLP_DEPLOY_T, 0, h->stream>>>(
+      h->d_desc + r0, h->d_ctl + r0, h->d_sur_list, h->d_sur_counts, tiles_plain, h->d_sur_queue + 2, chunks,
       h->d_mlp_cnt);
   network_kernel(h->surrogate_fq)<<<h->sur_network_ctas, MLP_DEPLOY_T, MLP_NETWORK_SMEM, h->stream>>>(
       h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
@@ -2053,14 +2065,15 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
       if (cudaMalloc(&h->d_mlp, MLP_NPARAM * sizeof(float)) != cudaSuccess ||
           cudaMalloc(&h->d_mlp_cnt, 3 * sizeof(unsigned long long)) != cudaSuccess ||
           cudaMalloc(&h->d_sur_list, (size_t)chunks * h->n * MLP_DEPLOY_SPAN * sizeof(unsigned short)) != cudaSuccess ||
-          cudaMalloc(&h->d_sur_counts, (size_t)chunks * h->n * sizeof(unsigned)) != cudaSuccess ||
-          cudaMalloc(&h->d_sur_tiles, (size_t)chunks * h->n * (MLP_DEPLOY_SPAN / 32) * sizeof(unsigned)) != cudaSuccess ||
-          cudaMalloc(&h->d_sur_queue, 2 * sizeof(unsigned)) != cudaSuccess)
+          cudaMalloc(&h->d_sur_counts, (size_t)chunks * h->n * 2 * sizeof(unsigned)) != cudaSuccess ||
+          cudaMalloc(&h->d_sur_tiles, (size_t)chunks * h->n * (MLP_DEPLOY_SPAN / 32) * 2 * sizeof(unsigned)) != cudaSuccess ||
+          cudaMalloc(&h->d_sur_queue, 4 * sizeof(unsigned)) != cudaSuccess)
         return fail(h, CSP_ENOMEM, "surrogate buffers");
       if ((unsigned long long)chunks * h->n >= (1ull << (32 - MLP_TILE_BITS)))
         return fail(h, CSP_ENOTSUP, "surrogate: more than 2^%d blocks of %lld voxels", 32 - MLP_TILE_BITS, MLP_DEPLOY_SPAN);
       CUDA_TRY(h, cudaMemsetAsync(h->d_mlp_cnt, 0, 3 * sizeof(unsigned long long), h->stream));
-      CUDA_TRY(h, cudaMemsetAsync(h->d_sur_queue, 0, 2 * sizeof(unsigned), h->stream));
+      CUDA_TRY(h, cudaMemsetAsync(h->d_sur_queue, 0, 4 * sizeof(unsigned), h->stream));
+      h->sur_tile_cap = chunks * (long long)h->n * (MLP_DEPLOY_SPAN / 32);
       int dev = 0, sms = 0;
       CUDA_TRY(h, cudaGetDevice(&dev));
       CUDA_TRY(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -2071,6 +2084,13 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
     h->surrogate_fq = fq == 0u ? 0u : fq == 0x10u ? 0x10u : 0x3Eu;
     CUDA_TRY(h, cudaFuncSetAttribute(network_kernel(h->surrogate_fq), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)MLP_NETWORK_SMEM));
+    {
+      int dev = 0, sms = 0, per_sm = 0;
+      CUDA_TRY(h, cudaGetDevice(&dev));
+      CUDA_TRY(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plain_kernel(h->surrogate_fq), MLP_DEPLOY_T, 0));
+      h->sur_plain_ctas = std::max(per_sm, 1) * std::max(sms, 1);
+    }
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     h->surrogate_tol = (float)tol;
   }
