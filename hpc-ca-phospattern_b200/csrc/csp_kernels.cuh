@@ -164,8 +164,12 @@ __device__ __forceinline__ double pair_flux(const RealDesc& D, int slot, double 
 // increments the fast reactions apply (dJ_s = dt_r J_s, buffer_dj; ca = the voxel's Ca,
 // val = the stored deviations): the near-equilibrium test of the surrogate,
 // lam |g_s| + k_on (tot - b_s) |sum g| <= MLP_SKIP tot / (dt_r^2 / 2) for every bound s,
-// times dt_r^2: |kon_dt ca + koff_dt| |dJ_s| + kon_dt (tot - b_s) |sum dJ| <= sur_thr2.
-// The staged kernel's two-lane form rounds every step the same way.
+// times dt_r^2, as the sign of the margin
+// sur_thr2 - kon_dt (tot - b_s) |sum dJ| - (kon_dt ca + koff_dt) |dJ_s|
+// = fma(in, |dJ_s|, fma(nkon (cs - db), |sum dJ|, sur_thr2)), in = nkon ca + nkoff (the
+// voxel is near equilibrium when no margin is negative; a NaN margin counts as
+// non-negative, which keeps the explicit increment).  The staged kernel's two-lane form
+// rounds every step the same way.
 template <int N>
 __device__ __forceinline__ unsigned rx_classify(const RealDesc& D, int d, float ca, const float (&val)[N]) {
   const unsigned kind = D.sur_kind[d];
@@ -180,17 +184,18 @@ __device__ __forceinline__ unsigned rx_classify(const RealDesc& D, int d, float 
     G = __fadd_rn(G, buffer_dj(k.x, k.y, k.z, k.w, val[s], dca, ca));
   }
   const float aG = fabsf(G);
-  bool near = true;
+  unsigned neg = 0;   // sign bits of the margins
 #pragma unroll
   for (int s = 1; s < N; s++) {
     if (!(rm >> s & 1u)) continue;
     const float4 k = D.rk[d][s];
     const float in = __fmaf_rn(k.x, ca, k.y);
     const float dJ = buffer_dj(k.x, k.y, k.z, k.w, val[s], dca, ca);
-    const float lhs = __fmaf_rn(__fmul_rn(k.x, __fsub_rn(val[s], D.sur_cs[d][s])), aG, __fmul_rn(fabsf(in), fabsf(dJ)));
-    near &= lhs <= D.sur_thr2[d][s];
+    const float margin = __fmaf_rn(in, fabsf(dJ), __fmaf_rn(__fmul_rn(k.x, __fsub_rn(D.sur_cs[d][s], val[s])), aG,
+                                                            D.sur_thr2[d][s]));
+    neg |= __float_as_uint(margin);
   }
-  return near ? RX_CLASS_EXPLICIT : RX_CLASS_NETWORK;
+  return (neg >> 31) ? RX_CLASS_NETWORK : RX_CLASS_EXPLICIT;
 }
 
 // SUR: on fast-reaction steps of a realisation with RealDesc::sur, cls receives the

@@ -156,31 +156,22 @@ __device__ __forceinline__ unsigned rx_classify4(const RealDesc& D, int d, F2 ca
   const unsigned rm = D.rmask[d];
   const F2 dca0 = f2(val[0][0], val[0][1]), dca1 = f2(val[0][2], val[0][3]);
   const F2 aG0 = f2_abs(G0), aG1 = f2_abs(G1);
-  bool n[4] = {true, true, true, true};
+  unsigned long long neg0 = 0, neg1 = 0;   // sign bits of the margins, OR-ed over the slots
 #pragma unroll
   for (int s = 1; s < MS; s++) {
     if (!(rm >> s & 1u)) continue;
     const float4 kk = D.rk[d][s];
     const F2 nkon = f2(kk.x, kk.x), nkoff = f2(kk.y, kk.y), a = f2(kk.z, kk.z), j0 = f2(kk.w, kk.w);
-    const F2 cs = f2(D.sur_cs[d][s], D.sur_cs[d][s]);
-    const float thr = D.sur_thr2[d][s];
+    const F2 cs = f2(D.sur_cs[d][s], D.sur_cs[d][s]), thr = f2(D.sur_thr2[d][s], D.sur_thr2[d][s]);
     const F2 db0 = f2(val[s][0], val[s][1]), db1 = f2(val[s][2], val[s][3]);
     const F2 in0 = f2_fma(nkon, ca0, nkoff), in1 = f2_fma(nkon, ca1, nkoff);
     const F2 dj0 = f2_fma(db0, in0, f2_fma(a, dca0, j0)), dj1 = f2_fma(db1, in1, f2_fma(a, dca1, j0));
-    const F2 l0 = f2_fma(f2_mul(nkon, f2_sub(db0, cs)), aG0, f2_mul(f2_abs(in0), f2_abs(dj0)));
-    const F2 l1 = f2_fma(f2_mul(nkon, f2_sub(db1, cs)), aG1, f2_mul(f2_abs(in1), f2_abs(dj1)));
-    float x0, x1, x2, x3;
-    f2_split(l0, x0, x1);
-    f2_split(l1, x2, x3);
-    n[0] &= x0 <= thr;
-    n[1] &= x1 <= thr;
-    n[2] &= x2 <= thr;
-    n[3] &= x3 <= thr;
+    neg0 |= f2_fma(in0, f2_abs(dj0), f2_fma(f2_mul(nkon, f2_sub(cs, db0)), aG0, thr)).v;
+    neg1 |= f2_fma(in1, f2_abs(dj1), f2_fma(f2_mul(nkon, f2_sub(cs, db1)), aG1, thr)).v;
   }
-  unsigned w = 0;
-#pragma unroll
-  for (int j = 0; j < 4; j++) w |= (n[j] ? RX_CLASS_EXPLICIT : RX_CLASS_NETWORK) << (8 * j);
-  return w;
+  const unsigned e = RX_CLASS_EXPLICIT, nt = RX_CLASS_NETWORK;
+  return ((neg0 >> 31 & 1u) ? nt : e) | ((neg0 >> 63) ? nt : e) << 8 | ((neg1 >> 31 & 1u) ? nt : e) << 16 |
+         ((neg1 >> 63) ? nt : e) << 24;
 }
 
 // INJ = true builds the test hook's variant (csp_test_wait_timeout); the kernel in use is

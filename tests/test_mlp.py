@@ -208,29 +208,35 @@ def test_surrogate_corrections_per_voxel(pkg, synth):
     at dt_r), from the old state.  Near equilibrium (every S_s <= 1e-8 by the oracle, away
     from the bound) the difference is exactly zero; in the stiff jSR it is the FP64 plain
     integrator's; elsewhere the network's (FP64 forward of the same weights, TF32 on the
-    device) or, where its output fails the residual test, the plain integrator's."""
+    device) or, where its output fails the residual test, the plain integrator's.  The
+    direct voxel kernel gives the staged kernel's step bitwise."""
     p, _ = trained(pkg, synth)
     spec, opts = spark_case(synth)
-    a, b = pkg.Simulation(spec, opts), pkg.Simulation(spec, opts)
+    a, b, e = pkg.Simulation(spec, opts), pkg.Simulation(spec, opts), pkg.Simulation(spec, opts)
     a.set_surrogate(p, 1e-4)
+    e.set_surrogate(p, 1e-4)
+    e.set_kernel(1)                                            # the direct voxel kernel classifies too
     n = a.info().reaction_substep
     k = 40 * n - 1                                             # step k + 1 is a reaction step
-    a.advance(k)
-    b.advance(k)
+    for sim in (a, b, e):
+        sim.advance(k)
     u0 = a.state()
     nch = a.info().num_channels
     chans = {bi: a.channels(bi) for bi in range(len(nch)) if nch[bi] > 0}
-    for sim in (a, b):
+    for sim in (a, b, e):
         sim.set_state(u0)
         for bi, st in chans.items():
             sim.set_channels(bi, st)
     c0 = a.surrogate_counts()
-    a.advance(1)
-    b.advance(1)
+    for sim in (a, b, e):
+        sim.advance(1)
     c1 = a.surrogate_counts()
-    diff = a.state() - b.state()
-    a.close()
-    b.close()
+    ua = a.state()
+    diff = ua - b.state()
+    # the staged and the direct kernels classify alike: the same step, bitwise
+    np.testing.assert_array_equal(ua, e.state())
+    for sim in (a, b, e):
+        sim.close()
     dtr = n * DT
     vox = spec["voxels"]
     counts = {"near": 0, "stiff": 0, "network": 0, "plain": 0, "border": 0}
