@@ -66,13 +66,14 @@ def mlp_gradient(params, x, t):
 
 
 def mlp_forward(params, x, tensor_cores=False):
-    """Network outputs on device (csp_mlp_forward): FP32 or TF32 tensor cores."""
+    """Network outputs on device (csp_mlp_forward): FP32 (False / 0), TF32 warp mma.sync
+    tiles (True / 1) or TF32 tcgen05 tiles with tensor-memory accumulators (2)."""
     lib = load()
     p = np.ascontiguousarray(params, dtype=np.float32)
     x = np.ascontiguousarray(x, dtype=np.float32)
     y = np.zeros((x.shape[0], 5), dtype=np.float32)
     P = C.POINTER(C.c_float)
-    rc = lib.csp_mlp_forward(p.ctypes.data_as(P), x.ctypes.data_as(P), int(x.shape[0]), 1 if tensor_cores else 0,
+    rc = lib.csp_mlp_forward(p.ctypes.data_as(P), x.ctypes.data_as(P), int(x.shape[0]), int(tensor_cores),
                              y.ctypes.data_as(P))
     if rc != 0:
         raise CspError(rc, _status(lib, None))
@@ -193,6 +194,11 @@ class Simulation:
             return
         self._mlp = np.ascontiguousarray(params, dtype=np.float32)
         self._check(self.lib.csp_set_surrogate(self.h, self._mlp.ctypes.data_as(C.POINTER(C.c_float)), float(tol)))
+
+    def set_surrogate_tensor_cores(self, kind):
+        """The network tiles' tensor cores: 1 warp mma.sync (default), 2 tcgen05 with
+        tensor-memory accumulators (csp_set_surrogate_tensor_cores)."""
+        self._check(self.lib.csp_set_surrogate_tensor_cores(self.h, int(kind)))
 
     def surrogate_counts(self):
         """(voxel increments, network evaluations, plain-integrator fallbacks)."""

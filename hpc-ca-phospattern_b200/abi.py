@@ -284,6 +284,7 @@ def declare(lib):
         "csp_mlp_forward": (C.c_int, [P(C.c_float), P(C.c_float), C.c_int64, C.c_int32, P(C.c_float)]),
         "csp_set_surrogate": (C.c_int, [h, P(C.c_float), C.c_double]),
         "csp_surrogate_counts": (C.c_int, [h, P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
+        "csp_set_surrogate_tensor_cores": (C.c_int, [h, C.c_int32]),
         "csp_autotune": (C.c_int, [h, C.c_int32, P(csp_tune_report)]),
         "csp_destroy": (None, [h]),
     }

@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include "csp_device.cuh"
+#include "csp_staged.cuh"   // mbarrier helpers and the bounded wait
 
 namespace csp {
 
@@ -335,6 +336,226 @@ __device__ __forceinline__ void mlp_forward_tc(const MlpTC& T, float* stage, con
 #pragma unroll
   for (int i = 0; i < MLP_OUT; i++) y[i] = row[i];
   __syncwarp();
+}
+
+// ---- tcgen05 forward pass: 128 samples per CTA of 128 threads (one warpgroup).  One
+// thread issues tcgen05.mma (kind::tf32, FP32 accumulation in 64 columns of tensor
+// memory) for a layer; the MMAs' completion arrives on an mbarrier (tcgen05.commit); each
+// warp then reads its 32 TMEM lanes (rows: one sample per thread) with tcgen05.ld, adds
+// the bias, applies the ReLU and writes the row back to shared memory as the next layer's
+// A operand.  Operands sit in shared memory in the canonical K-major layout without
+// swizzle: element (row, k) of a matrix of R rows at byte
+//   (k / 4) * 16 R + (row / 8) * 128 + (row % 8) * 16 + (k % 4) * 4,
+// i.e. core matrices of 8 rows x 16 bytes, 128 bytes apart along the rows (the stride
+// byte offset) and 16 R bytes apart along K (the leading byte offset); one MMA takes
+// K = 8 (two core matrices along K).  Layers: [128 x 8] [8 x 64], [128 x 64] [64 x 64],
+// [128 x 64] [64 x 16] (outputs 5..15 zero).
+constexpr int UM_T = 128;                          // threads (and samples) per CTA
+constexpr int UM_B1 = 0;                           // B of layer 1: 64 x 8 tf32, 2 KB
+constexpr int UM_B2 = UM_B1 + 64 * 8 * 4;          // B of layer 2: 64 x 64, 16 KB
+constexpr int UM_B3 = UM_B2 + 64 * 64 * 4;         // B of layer 3: 16 x 64, 4 KB
+constexpr int UM_ACT = UM_B3 + 16 * 64 * 4;        // A: 128 x 64 activations, 32 KB
+constexpr int UM_BIAS = UM_ACT + 128 * 64 * 4;     // b1[64], b2[64], b3[16] (FP32)
+constexpr int UM_BAR = UM_BIAS + 1024;             // mbarrier, then the TMEM base address
+constexpr int UM_SMEM = UM_BAR + 128;
+constexpr int UM_TMEM_COLS = 64;
+
+__host__ __device__ constexpr unsigned um_off(int row, int k, int rows) {
+  return (unsigned)((k >> 2) * (rows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+// shared-memory matrix descriptor (sm100): start, leading / stride byte offsets (>> 4),
+// version 1, no swizzle
+__device__ __forceinline__ unsigned long long um_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
+  return (unsigned long long)((saddr >> 4) & 0x3FFFu) | ((unsigned long long)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((unsigned long long)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// instruction descriptor, kind::tf32: D FP32, A and B TF32, both K-major, M x N
+__host__ __device__ constexpr unsigned um_idesc(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(M >> 4) << 24);
+}
+__device__ __forceinline__ void um_mma(unsigned tmem_d, unsigned long long da, unsigned long long db, unsigned idesc,
+                                       unsigned accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate) : "memory");
+}
+__device__ __forceinline__ void um_commit(unsigned bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void um_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void um_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+// 16 consecutive columns of this thread's TMEM lane, waited for
+__device__ __forceinline__ void um_ld16(unsigned taddr, float (&v)[16]) {
+  unsigned r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr) : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// The weights of params as the three B operands (TF32 bit patterns) and the biases;
+// every thread of the CTA takes part.
+__device__ __forceinline__ void um_load_weights(unsigned char* sm, const float* __restrict__ p) {
+  const MlpW& W = *reinterpret_cast<const MlpW*>(p);
+  for (int i = threadIdx.x; i < 64 * 8; i += blockDim.x) {       // B1 (n, k) = w1[k][n]
+    const int n = i % 64, k = i / 64;
+    *reinterpret_cast<unsigned*>(sm + UM_B1 + um_off(n, k, 64)) = tf32_bits(W.w1[k * MLP_H + n]);
+  }
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+    const int n = i % 64, k = i / 64;
+    *reinterpret_cast<unsigned*>(sm + UM_B2 + um_off(n, k, 64)) = tf32_bits(W.w2[k * MLP_H + n]);
+  }
+  for (int i = threadIdx.x; i < 16 * 64; i += blockDim.x) {
+    const int n = i % 16, k = i / 16;
+    *reinterpret_cast<unsigned*>(sm + UM_B3 + um_off(n, k, 16)) = n < MLP_OUT ? tf32_bits(W.w3[k * MLP_OUT + n]) : 0u;
+  }
+  float* bias = reinterpret_cast<float*>(sm + UM_BIAS);
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+    bias[i] = W.b1[i];
+    bias[64 + i] = W.b2[i];
+  }
+  for (int i = threadIdx.x; i < 16; i += blockDim.x) bias[128 + i] = i < MLP_OUT ? W.b3[i] : 0.f;
+}
+
+// One layer: D = A[:, :K] B^T over K / 8 MMAs, issued by thread 0; true once they completed
+// (bounded wait: false after WAIT_NS, the caller gives up).  phase: the mbarrier's parity.
+template <int K, int N, int BROWS>
+__device__ __forceinline__ bool um_layer(unsigned char* sm, unsigned tmem, unsigned& phase, int b_off) {
+  const unsigned base = smem_u32(sm);
+  if (threadIdx.x == 0) {
+    um_fence_after();
+#pragma unroll
+    for (int ks = 0; ks < K / 8; ks++) {
+      const unsigned long long da = um_desc(base + UM_ACT + (unsigned)(2 * ks) * (128 * 16), 128 * 16, 128);
+      const unsigned long long db = um_desc(base + b_off + (unsigned)(2 * ks) * (BROWS * 16), BROWS * 16, 128);
+      um_mma(tmem, da, db, um_idesc(128, N), ks > 0 ? 1u : 0u);
+    }
+    um_commit(base + UM_BAR);
+  }
+  const bool ok = mbar_wait_bounded(base + UM_BAR, phase, WAIT_NS);
+  phase ^= 1u;
+  um_fence_after();
+  return ok;
+}
+
+// ReLU(D + bias) of this thread's row back into the A operand as TF32 (64 columns).
+__device__ __forceinline__ void um_hidden(unsigned char* sm, unsigned tmem, const float* bias) {
+  const int row = threadIdx.x;
+  const unsigned taddr = tmem + ((unsigned)(row & ~31) << 16);
+#pragma unroll
+  for (int c0 = 0; c0 < 64; c0 += 16) {
+    float v[16];
+    um_ld16(taddr + c0, v);
+#pragma unroll
+    for (int c = 0; c < 16; c += 4) {
+      uint4 q;
+      q.x = tf32_bits(fmaxf(v[c] + bias[c0 + c], 0.f));
+      q.y = tf32_bits(fmaxf(v[c + 1] + bias[c0 + c + 1], 0.f));
+      q.z = tf32_bits(fmaxf(v[c + 2] + bias[c0 + c + 2], 0.f));
+      q.w = tf32_bits(fmaxf(v[c + 3] + bias[c0 + c + 3], 0.f));
+      *reinterpret_cast<uint4*>(sm + UM_ACT + um_off(row, c0 + c, 128)) = q;
+    }
+  }
+}
+
+// Forward pass of the CTA's 128 samples (thread t: sample t, inputs x, outputs y); every
+// thread of the CTA calls it.  false: an MMA did not complete within WAIT_NS.
+__device__ __forceinline__ bool mlp_forward_umma(unsigned char* sm, unsigned tmem, unsigned& phase, const float* x,
+                                                 float* y) {
+  const int row = threadIdx.x;
+  const float* bias = reinterpret_cast<const float*>(sm + UM_BIAS);
+  {
+    uint4 a, b;
+    a.x = tf32_bits(x[0]); a.y = tf32_bits(x[1]); a.z = tf32_bits(x[2]); a.w = tf32_bits(x[3]);
+    b.x = tf32_bits(x[4]); b.y = tf32_bits(x[5]); b.z = tf32_bits(x[6]); b.w = tf32_bits(x[7]);
+    *reinterpret_cast<uint4*>(sm + UM_ACT + um_off(row, 0, 128)) = a;
+    *reinterpret_cast<uint4*>(sm + UM_ACT + um_off(row, 4, 128)) = b;
+  }
+  bool ok = true;
+  // before each layer: every thread's rows written (generic proxy -> async proxy) and its
+  // TMEM reads of the previous layer done
+  um_fence_before();
+  fence_proxy_async();
+  __syncthreads();
+  ok = um_layer<MLP_IN, 64, 64>(sm, tmem, phase, UM_B1) && ok;
+  if (ok) um_hidden(sm, tmem, bias);
+  um_fence_before();
+  fence_proxy_async();
+  ok = __syncthreads_and(ok);
+  if (ok) ok = um_layer<MLP_H, 64, 64>(sm, tmem, phase, UM_B2);
+  if (ok) um_hidden(sm, tmem, bias + 64);
+  um_fence_before();
+  fence_proxy_async();
+  ok = __syncthreads_and(ok);
+  if (ok) ok = um_layer<MLP_H, 16, 16>(sm, tmem, phase, UM_B3);
+  if (ok) {
+    float v[16];
+    um_ld16(tmem + ((unsigned)(row & ~31) << 16), v);
+#pragma unroll
+    for (int q = 0; q < MLP_OUT; q++) y[q] = v[q] + bias[128 + q];
+  }
+  return __syncthreads_and(ok);
+}
+
+// TMEM for the CTA (warp 0 allocates and, at the end, frees UM_TMEM_COLS columns).
+__device__ __forceinline__ unsigned um_tmem_alloc(unsigned char* sm) {
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 ::"r"(smem_u32(sm + UM_BAR + 8)), "r"(UM_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  um_fence_before();
+  __syncthreads();
+  um_fence_after();
+  return *reinterpret_cast<volatile unsigned*>(sm + UM_BAR + 8);
+}
+__device__ __forceinline__ void um_tmem_free(unsigned tmem) {
+  um_fence_before();
+  __syncthreads();
+  um_fence_after();
+  if (threadIdx.x < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS) : "memory");
+}
+
+// Forward passes for checks on the tcgen05 path: y[n][5] of x[n][8]; err[0] |= 1 when an
+// MMA did not complete in time (the CTA then waits once more for it, frees its TMEM and
+// stops).
+__global__ void __launch_bounds__(UM_T) k_mlp_forward_umma(const float* __restrict__ params,
+                                                           const float* __restrict__ x, long long n,
+                                                           float* __restrict__ y, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char um_sm[];
+  um_load_weights(um_sm, params);
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(um_sm + UM_BAR), 1);
+    fence_mbar_init();
+  }
+  fence_proxy_async();
+  __syncthreads();
+  const unsigned tmem = um_tmem_alloc(um_sm);
+  unsigned phase = 0;
+  for (long long t0 = (long long)blockIdx.x * UM_T; t0 < n; t0 += (long long)gridDim.x * UM_T) {
+    const long long i = t0 + threadIdx.x;
+    float xi[MLP_IN], yi[MLP_OUT];
+#pragma unroll
+    for (int j = 0; j < MLP_IN; j++) xi[j] = i < n ? x[i * MLP_IN + j] : 0.f;
+    if (!mlp_forward_umma(um_sm, tmem, phase, xi, yi)) {
+      // a late MMA may still write TMEM: wait for it once more (bounded) before freeing
+      if (threadIdx.x == 0) {
+        mbar_wait_bounded(smem_u32(um_sm + UM_BAR), phase ^ 1u, WAIT_NS);
+        atomicOr(err, 1);
+      }
+      break;
+    }
+    if (i < n)
+#pragma unroll
+      for (int j = 0; j < MLP_OUT; j++) y[i * MLP_OUT + j] = yi[j];
+  }
+  um_tmem_free(tmem);
 }
 
 // Increment of the network output t, with the acceptance test (see the header comment).
@@ -712,6 +933,98 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
         rx_correct<FQ>(K, D, W.un, cu.v, fqs, dev, c, db, dc);
       }
     }
+    if (n_net) atomicAdd(&s_net, n_net);
+    if (n_fall) atomicAdd(&s_fall, n_fall);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      if (s_net) atomicAdd(&counters[1], (unsigned long long)s_net);
+      if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
+    }
+  }
+  rx_queue_done(queue);
+}
+
+// k_react_network on the 5th-generation tensor cores: a CTA of 128 threads takes groups of
+// four queued tiles, one per warp (each warp fetches its tile's voxels and caches its
+// realisation's constants as in k_react_network), and runs the network for the group's
+// 128 voxels as one tcgen05 MMA chain per layer (mlp_forward_umma); rejected outputs take
+// the plain integrator.  Persistent CTAs: CTA b takes a contiguous range of the groups.
+// An MMA that does not complete within WAIT_NS sets ERR_TIMEOUT in err and stops the CTA
+// (after a second bounded wait for it and with its TMEM freed).
+template <unsigned FQ>
+__global__ void __launch_bounds__(UM_T) k_react_network_umma(const RealDesc* __restrict__ descs,
+                                                             const RealCtl* __restrict__ ctl,
+                                                             const float* __restrict__ params, float tol,
+                                                             const unsigned short* __restrict__ list,
+                                                             const unsigned* __restrict__ counts,
+                                                             const unsigned* __restrict__ tiles,
+                                                             unsigned* __restrict__ queue, int chunks,
+                                                             unsigned long long* __restrict__ counters,
+                                                             int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char um_sm[];
+  __shared__ RxWarpCache s_wc[UM_T / 32];
+  __shared__ unsigned s_net, s_fall, s_total;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) { s_total = queue[0]; s_net = 0; s_fall = 0; }
+  __syncthreads();
+  const unsigned total = s_total, groups = (total + 3u) / 4u;
+  const unsigned per = (groups + gridDim.x - 1) / gridDim.x;
+  const unsigned g_lo = blockIdx.x * per, g_hi = min(groups, g_lo + per);
+  if (g_lo < g_hi) {                                     // uniform over the block
+    um_load_weights(um_sm, params);
+    if (threadIdx.x == 0) {
+      mbar_init(smem_u32(um_sm + UM_BAR), 1);
+      fence_mbar_init();
+    }
+    fence_proxy_async();
+    __syncthreads();
+    const unsigned tmem = um_tmem_alloc(um_sm);
+    unsigned phase = 0, n_net = 0, n_fall = 0;
+    RxWarpCache& W = s_wc[warp];
+    int rc = -1;                                         // realisation whose constants this warp caches
+    RxTile nx{};
+    if (4 * g_lo + warp < total) nx = rx_fetch_tile(descs, list, counts, tiles[4 * g_lo + warp], chunks, 0, lane);
+    for (unsigned g = g_lo; g < g_hi; g++) {
+      const bool tile = 4 * g + warp < total;            // warp-uniform
+      RxTile cu = nx;
+      if (!tile) cu.have = false;
+      if (g + 1 < g_hi && 4 * (g + 1) + warp < total)
+        nx = rx_fetch_tile(descs, list, counts, tiles[4 * (g + 1) + warp], chunks, 0, lane);
+      float dev[MLP_RX_NS], c = 0.f, b[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
+#pragma unroll
+      for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
+#pragma unroll
+      for (int q = 0; q < MLP_SLOTS; q++) b[q] = 0.f;
+      const RealDesc& D = descs[tile ? cu.r : 0];
+      if (tile && cu.r != rc) {                          // warp-uniform
+        rx_cache_fill(D, ctl[cu.r], W, lane);
+        rc = cu.r;
+      }
+      const float dtr = (float)(D.dt * D.reaction_substep);
+      const unsigned fqs = D.fixq;
+      const RxDom& K = W.dom[cu.d];
+      if (cu.have) {
+        rx_load_old<FQ>(K, W.uo, cu.v, fqs, dev, c, b);
+        rx_features(K.k, cu.d, dtr, c, b, x);
+      }
+      if (!mlp_forward_umma(um_sm, tmem, phase, x, t)) {
+        if (threadIdx.x == 0) {
+          mbar_wait_bounded(smem_u32(um_sm + UM_BAR), phase ^ 1u, WAIT_NS);
+          atomicOr(err, ERR_TIMEOUT);
+        }
+        break;
+      }
+      if (cu.have) {
+        float dc, db[MLP_SLOTS];
+        n_net++;
+        if (!rx_apply_output(K.k, dtr, c, b, t, tol, dc, db)) {
+          n_fall++;
+          rx_fallback(K.k, D.reaction_substep, D.dt, c, b, dc, db);
+        }
+        rx_correct<FQ>(K, D, W.un, cu.v, fqs, dev, c, db, dc);
+      }
+    }
+    um_tmem_free(tmem);
     if (n_net) atomicAdd(&s_net, n_net);
     if (n_fall) atomicAdd(&s_fall, n_fall);
     __syncthreads();

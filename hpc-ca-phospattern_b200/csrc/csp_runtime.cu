@@ -178,6 +178,7 @@ struct csp_handle {
   int graph_plan = -1;
   int plan_epoch = 0;                       // bumped when the autotuner replaces the plan
   int graph_surrogate = 0;
+  int graph_sur_tc = 0;
   // learned reaction surrogate (csp_set_surrogate)
   int surrogate = 0;
   float surrogate_tol = 1e-4f;
@@ -192,6 +193,8 @@ struct csp_handle {
   unsigned char* d_rx_class = nullptr;      // surrogate class bytes (RealDesc::rx_class), layout of d_dom
   int sur_network_ctas = 0;                 // persistent CTAs of k_react_network
   int sur_plain_ctas = 0;                   // persistent CTAs of k_react_plain
+  int sur_umma_ctas = 0;                    // persistent CTAs of k_react_network_umma
+  int sur_tc = 1;                           // network tiles: 1 warp mma.sync, 2 tcgen05 (csp_set_surrogate_tensor_cores)
   // training pairs harvested from the fields (csp_mlp_harvest): features [cap][8], targets [cap][5]
   float* d_hx = nullptr;
   float* d_ht = nullptr;
@@ -1078,6 +1081,11 @@ using NetworkKernel = void (*)(const RealDesc*, const RealCtl*, const float*, fl
 static NetworkKernel network_kernel(unsigned fq) {
   return fq == 0u ? k_react_network<0u> : fq == 0x10u ? k_react_network<0x10u> : k_react_network<0x3Eu>;
 }
+using NetworkUmmaKernel = void (*)(const RealDesc*, const RealCtl*, const float*, float, const unsigned short*,
+                                   const unsigned*, const unsigned*, unsigned*, int, unsigned long long*, int*);
+static NetworkUmmaKernel network_kernel_umma(unsigned fq) {
+  return fq == 0u ? k_react_network_umma<0u> : fq == 0x10u ? k_react_network_umma<0x10u> : k_react_network_umma<0x3Eu>;
+}
 using PlainKernel = void (*)(const RealDesc*, const RealCtl*, const unsigned short*, const unsigned*,
                              const unsigned*, unsigned*, int, unsigned long long*);
 static PlainKernel plain_kernel(unsigned fq) {
@@ -1096,9 +1104,14 @@ static void launch_surrogate(csp_handle* h, int r0, int r1) {
   plain_kernel(h->surrogate_fq)<<<h->sur_plain_ctas, MLP_DEPLOY_T, 0, h->stream>>>(
       h->d_desc + r0, h->d_ctl + r0, h->d_sur_list, h->d_sur_counts, tiles_plain, h->d_sur_queue + 2, chunks,
       h->d_mlp_cnt);
-  network_kernel(h->surrogate_fq)<<<h->sur_network_ctas, MLP_DEPLOY_T, MLP_NETWORK_SMEM, h->stream>>>(
-      h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
-      h->d_sur_queue, chunks, h->d_mlp_cnt);
+  if (h->sur_tc == 2)
+    network_kernel_umma(h->surrogate_fq)<<<h->sur_umma_ctas, UM_T, UM_SMEM, h->stream>>>(
+        h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
+        h->d_sur_queue, chunks, h->d_mlp_cnt, h->d_err);
+  else
+    network_kernel(h->surrogate_fq)<<<h->sur_network_ctas, MLP_DEPLOY_T, MLP_NETWORK_SMEM, h->stream>>>(
+        h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
+        h->d_sur_queue, chunks, h->d_mlp_cnt);
 }
 
 static void launch_epilogue(csp_handle* h, int r0, int r1, int* step_flags) {
@@ -1136,7 +1149,8 @@ static cudaError_t launch_step(csp_handle* h, int r0 = 0, int r1 = -1, int* step
 }
 
 static int ensure_graph(csp_handle* h) {
-  if (h->graph && h->graph_kernel == h->kernel && h->graph_surrogate == h->surrogate && h->graph_plan == h->plan_epoch)
+  if (h->graph && h->graph_kernel == h->kernel && h->graph_surrogate == h->surrogate && h->graph_sur_tc == h->sur_tc &&
+      h->graph_plan == h->plan_epoch)
     return CSP_OK;
   if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
   cudaGraph_t g;
@@ -1155,6 +1169,7 @@ static int ensure_graph(csp_handle* h) {
   h->graph_kernel = h->kernel;
   h->graph_plan = h->plan_epoch;
   h->graph_surrogate = h->surrogate;
+  h->graph_sur_tc = h->sur_tc;
   return CSP_OK;
 }
 
@@ -1894,6 +1909,7 @@ extern "C" int csp_test_wait_timeout(csp_handle* h, int32_t on) {
 
 extern "C" int csp_set_kernel(csp_handle* h, int32_t which) {
   if (!h || which < 0 || which > 1) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   if (which == 0 && !h->plan.ok) return fail(h, CSP_ENOTSUP, "staged kernel unavailable for this batch");
   h->kernel = which;
   return CSP_OK;
@@ -2056,6 +2072,7 @@ static int surrogate_supported(csp_handle* h) {
 
 extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol) {
   if (!h) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   const int on = params != nullptr;
   if (on) {
     int rc = surrogate_supported(h);
@@ -2090,6 +2107,11 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
       CUDA_TRY(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
       CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plain_kernel(h->surrogate_fq), MLP_DEPLOY_T, 0));
       h->sur_plain_ctas = std::max(per_sm, 1) * std::max(sms, 1);
+      CUDA_TRY(h, cudaFuncSetAttribute(network_kernel_umma(h->surrogate_fq), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       UM_SMEM));
+      CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, network_kernel_umma(h->surrogate_fq), UM_T,
+                                                                UM_SMEM));
+      h->sur_umma_ctas = std::max(per_sm, 1) * std::max(sms, 1);
     }
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     h->surrogate_tol = (float)tol;
@@ -2128,9 +2150,17 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
   return CSP_OK;
 }
 
+extern "C" int csp_set_surrogate_tensor_cores(csp_handle* h, int32_t kind) {
+  if (!h || (kind != 1 && kind != 2)) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
+  h->sur_tc = kind;
+  return CSP_OK;
+}
+
 extern "C" int csp_surrogate_counts(const csp_handle* hc, int64_t* voxels, int64_t* network, int64_t* fallbacks) {
   csp_handle* h = const_cast<csp_handle*>(hc);
   if (!h || !voxels || !network || !fallbacks) return CSP_EINVAL;
+  CSP_NOT_PENDING(h);
   unsigned long long c[3] = {0, 0, 0};
   if (h->d_mlp_cnt) {
     CUDA_TRY(h, cudaMemcpyAsync(c, h->d_mlp_cnt, sizeof c, cudaMemcpyDeviceToHost, h->stream));
@@ -2177,23 +2207,36 @@ extern "C" int csp_mlp_gradient(const float* params, const float* x, const float
 }
 
 extern "C" int csp_mlp_forward(const float* params, const float* x, int64_t n, int32_t tensor_cores, float* y) {
-  if (!params || !x || !y || n <= 0) return fail(nullptr, CSP_EINVAL, "bad argument");
+  if (!params || !x || !y || n <= 0 || tensor_cores < 0 || tensor_cores > 2) return fail(nullptr, CSP_EINVAL, "bad argument");
   float *dp = nullptr, *dx = nullptr, *dy = nullptr;
-  cudaError_t e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)MLP_FORWARD_SMEM);
+  int* derr = nullptr;
+  cudaError_t e = tensor_cores == 2
+                      ? cudaFuncSetAttribute(k_mlp_forward_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, UM_SMEM)
+                      : cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)MLP_FORWARD_SMEM);
   if (e == cudaSuccess) e = cudaMalloc(&dp, MLP_NPARAM * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&dx, n * MLP_IN * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&dy, n * MLP_OUT * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&derr, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemcpy(dp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dx, x, n * MLP_IN * sizeof(float), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    k_mlp_forward<<<(unsigned)((n + MLP_DEPLOY_T - 1) / MLP_DEPLOY_T), MLP_DEPLOY_T, MLP_FORWARD_SMEM>>>(
-        dp, dx, n, tensor_cores ? 1 : 0, dy);
+    if (tensor_cores == 2) {
+      const long long tiles = (n + UM_T - 1) / UM_T;
+      k_mlp_forward_umma<<<(unsigned)std::min<long long>(tiles, 592), UM_T, UM_SMEM>>>(dp, dx, n, dy, derr);
+    } else {
+      k_mlp_forward<<<(unsigned)((n + MLP_DEPLOY_T - 1) / MLP_DEPLOY_T), MLP_DEPLOY_T, MLP_FORWARD_SMEM>>>(
+          dp, dx, n, tensor_cores, dy);
+    }
     e = cudaGetLastError();
   }
+  int herr = 0;
   if (e == cudaSuccess) e = cudaMemcpy(y, dy, n * MLP_OUT * sizeof(float), cudaMemcpyDeviceToHost);
-  cudaFree(dp); cudaFree(dx); cudaFree(dy);
+  if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(dp); cudaFree(dx); cudaFree(dy); cudaFree(derr);
   if (e != cudaSuccess) return fail(nullptr, CSP_ECUDA, "mlp forward: %s", cudaGetErrorString(e));
+  if (herr) return fail(nullptr, CSP_EDEVICE, "mlp forward: bounded wait timed out");
   return CSP_OK;
 }
 

@@ -377,8 +377,10 @@ int csp_mlp_harvested(const csp_handle* h, int64_t first, int64_t n, float* x, f
 /* Loss and gradient of the mean squared error of params on n host pairs x[n][8], t[n][5]
  * with the device kernels used in training (for checks against a CPU implementation). */
 int csp_mlp_gradient(const float* params, const float* x, const float* t, int64_t n, float* grad, float* loss);
-/* Network outputs y[n][5] of inputs x[n][8]: the FP32 pass of training (tensor_cores = 0)
- * or the TF32 tensor-core pass the simulation uses (tensor_cores = 1). */
+/* Network outputs y[n][5] of inputs x[n][8]: the FP32 pass of training (tensor_cores = 0),
+ * the TF32 tensor-core pass the simulation uses (tensor_cores = 1: warp mma.sync tiles of
+ * 32 samples) or the same on the 5th-generation tensor cores (tensor_cores = 2: tcgen05
+ * MMAs on tiles of 128 samples with the accumulators in tensor memory). */
 int csp_mlp_forward(const float* params, const float* x, int64_t n, int32_t tensor_cores, float* y);
 /* Use params (NULL: switch off) for the reaction steps of every realisation. */
 int csp_set_surrogate(csp_handle* h, const float* params, double tol);
@@ -386,6 +388,11 @@ int csp_set_surrogate(csp_handle* h, const float* params, double tol);
  * evaluated for (the others were at equilibrium to within 1e-8 of their buffer totals, or
  * in a stiff domain), and those that took the plain integrator. */
 int csp_surrogate_counts(const csp_handle* h, int64_t* voxels, int64_t* network, int64_t* fallbacks);
+/* The tensor cores the surrogate's network tiles use: kind = 1 (the default) warp mma.sync
+ * tiles of 32 voxels; kind = 2 tcgen05 MMAs on tiles of 128 voxels with the accumulators in
+ * tensor memory (the same TF32 operands; at the surrogate's tile counts the serial
+ * per-layer MMA waits make it slower than kind 1).  No counterpart in the reference. */
+int csp_set_surrogate_tensor_cores(csp_handle* h, int32_t kind);
 
 /* ---- autotuner ----
  * Times candidate tile shapes of the staged voxel kernel (threads per CTA, x planes per
