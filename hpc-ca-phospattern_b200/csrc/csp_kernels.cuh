@@ -505,9 +505,12 @@ __global__ void __launch_bounds__(256, 8) k_density_rows(const RealDesc* __restr
 // step counter, apply the abort rule (species.c:3476-3486) on the openness counted by
 // the boundary kernel, stop at the last step.  flags (nullable): the stop flag of every
 // realisation after this step.
+// sur_queue (with the surrogate on): its tile queues, emptied for the next step once this
+// step's correction kernels have taken their tiles.
 __global__ void k_epilogue(const RealDesc* __restrict__ descs, RealCtl* __restrict__ ctl, StepRec* __restrict__ rec,
-                           int nreal, int* __restrict__ flags) {
+                           int nreal, int* __restrict__ flags, unsigned* __restrict__ sur_queue) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sur_queue && r == 0) sur_queue[0] = sur_queue[1] = sur_queue[2] = sur_queue[3] = 0u;
   if (r >= nreal) return;
   RealCtl& C = ctl[r];
   if (C.stopped) {

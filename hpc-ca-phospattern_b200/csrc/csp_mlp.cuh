@@ -721,7 +721,7 @@ __device__ __forceinline__ bool rx_active(const RealDesc& D, const RealCtl& C) {
 // counts[2 seg] / counts[2 seg + 1] their numbers, written on reaction steps.  tiles /
 // queue[0]: the network tiles of 32 listed voxels (seg << MLP_TILE_BITS | tile within
 // the list) and their number; tiles + MLP_PLAIN_TILES / queue[2]: the same for the plain
-// integrator.  queue[1] / queue[3]: CTAs of k_react_network / k_react_plain done.
+// integrator.  k_epilogue empties the queues for the next step.
 constexpr int MLP_TILE_BITS = 9;
 static_assert(MLP_DEPLOY_SPAN / 32 <= (1 << MLP_TILE_BITS), "tile index field");
 
@@ -856,17 +856,6 @@ __device__ __forceinline__ RxTile rx_fetch_tile(const RealDesc* __restrict__ des
   return f;
 }
 
-// Empties a queue for the next step once every CTA of the grid has read it (the last one
-// to finish resets it): q[0] tiles, q[1] CTAs done.
-__device__ __forceinline__ void rx_queue_done(unsigned* q) {
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(&q[1], 1u) == gridDim.x - 1) {
-      q[0] = 0;
-      q[1] = 0;
-    }
-  }
-}
 
 // The network voxels that k_react_surrogate listed, in tiles of 32 on the tensor cores (a
 // rejected output takes the plain integrator), each corrected from the old state
@@ -941,7 +930,6 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
       if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
     }
   }
-  rx_queue_done(queue);
 }
 
 // k_react_network on the 5th-generation tensor cores: a CTA of 128 threads takes groups of
@@ -1033,14 +1021,13 @@ __global__ void __launch_bounds__(UM_T) k_react_network_umma(const RealDesc* __r
       if (s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
     }
   }
-  rx_queue_done(queue);
 }
 
 // The plain-integrator voxels that k_react_surrogate listed (stiff domains), one per lane
 // (FP64), each corrected from the old state.  No weights and no activation tiles: the
 // CTAs hold a few KB of shared memory, so many more warps per SM hide the latency of
 // the voxels' dependent loads than the network kernel can.  Same tile distribution as
-// k_react_network, over the queue q (q[0] tiles, q[1] CTAs done).
+// k_react_network, over the queue q (q[0] tiles).
 template <unsigned FQ>
 __global__ void __launch_bounds__(MLP_DEPLOY_T, 4) k_react_plain(const RealDesc* __restrict__ descs,
                                                               const RealCtl* __restrict__ ctl,
@@ -1085,7 +1072,6 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 4) k_react_plain(const RealDesc*
     __syncthreads();
     if (threadIdx.x == 0 && s_fall) atomicAdd(&counters[2], (unsigned long long)s_fall);
   }
-  rx_queue_done(q);
 }
 
 // Forward passes for checks: y[n][5] of x[n][8], FP32 (tc = 0) or tensor cores (tc = 1,

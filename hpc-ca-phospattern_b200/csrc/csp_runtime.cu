@@ -1116,7 +1116,7 @@ static void launch_surrogate(csp_handle* h, int r0, int r1) {
 
 static void launch_epilogue(csp_handle* h, int r0, int r1, int* step_flags) {
   k_epilogue<<<(r1 - r0 + 127) / 128, 128, 0, h->stream>>>(h->d_desc + r0, h->d_ctl + r0, h->d_rec + r0, r1 - r0,
-                                                           step_flags);
+                                                           step_flags, h->surrogate ? h->d_sur_queue : nullptr);
 }
 
 static void launch_boundaries(csp_handle* h, int r0 = 0, int r1 = -1, int* step_flags = nullptr) {
@@ -2109,9 +2109,21 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
       h->sur_plain_ctas = std::max(per_sm, 1) * std::max(sms, 1);
       CUDA_TRY(h, cudaFuncSetAttribute(network_kernel_umma(h->surrogate_fq), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        UM_SMEM));
-      CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, network_kernel_umma(h->surrogate_fq), UM_T,
-                                                                UM_SMEM));
-      h->sur_umma_ctas = std::max(per_sm, 1) * std::max(sms, 1);
+      CUDA_TRY(h, cudaFuncSetAttribute(network_kernel_umma(h->surrogate_fq),
+                                       cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+      // resident CTAs per SM from the kernel's shared memory and registers (the occupancy
+      // query reports one for this kernel, which holds a third of the SM's shared memory):
+      // static + dynamic + the driver's reserve per CTA, and up to 1 KB of alignment
+      cudaFuncAttributes fa;
+      int smem_sm = 0, reserved = 0, regs_sm = 0;
+      CUDA_TRY(h, cudaFuncGetAttributes(&fa, network_kernel_umma(h->surrogate_fq)));
+      CUDA_TRY(h, cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+      CUDA_TRY(h, cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+      CUDA_TRY(h, cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+      const int per_block = (int)fa.sharedSizeBytes + UM_SMEM + reserved + 1024;
+      const int by_regs = regs_sm / std::max(1, fa.numRegs * UM_T);
+      per_sm = std::max(1, std::min({smem_sm / per_block, by_regs, 512 / UM_TMEM_COLS}));
+      h->sur_umma_ctas = per_sm * std::max(sms, 1);
     }
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
     h->surrogate_tol = (float)tol;
