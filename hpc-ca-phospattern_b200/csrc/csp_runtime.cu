@@ -1903,6 +1903,8 @@ extern "C" int csp_test_wait_timeout(csp_handle* h, int32_t on) {
   if (!h) return CSP_EINVAL;
   if (on && (h->kernel != 0 || !h->plan.ok || !h->plan.launch_inject))
     return fail(h, CSP_EINVAL, "the staged voxel kernel with the test hook is not in use");
+  // the hook's variant does not classify voxels for the surrogate
+  if (on && h->surrogate) return fail(h, CSP_EINVAL, "the test hook does not run with the surrogate on");
   h->inject_wait = on ? 1 : 0;
   return CSP_OK;
 }
@@ -2074,6 +2076,7 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
   if (!h) return CSP_EINVAL;
   CSP_NOT_PENDING(h);
   const int on = params != nullptr;
+  if (on && h->inject_wait) return fail(h, CSP_EINVAL, "the surrogate does not run with the wait-timeout test hook on");
   if (on) {
     int rc = surrogate_supported(h);
     if (rc) return rc;
