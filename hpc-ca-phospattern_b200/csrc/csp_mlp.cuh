@@ -657,11 +657,53 @@ __device__ __forceinline__ float rx_add(const RxDom& K, int s, float stored, flo
 }
 
 // The plain integrator's increments (the fallback), FP64, rounded to FP32.
+// rx_plain for the slots of MASK only (known at compile time, so the slots a domain lacks
+// issue no instructions); the same operations in the same order as rx_plain.
+template <unsigned MASK>
+__device__ __forceinline__ void rx_plain_mask(const RxConst& k, int n, double h, double c, const double* b0, double& dc,
+                                              double* db) {
+  double b[MLP_SLOTS];
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) b[q] = b0[q];
+  double cc = c;
+  for (int i = 0; i < n; i++) {
+    double g[MLP_SLOTS], sg = 0.0;
+#pragma unroll
+    for (int q = 0; q < MLP_SLOTS; q++) {
+      g[q] = 0.0;
+      if (!(MASK >> q & 1u)) continue;
+      g[q] = rx_g<double>(k, q, cc, b[q]);
+      sg += g[q];
+    }
+#pragma unroll
+    for (int q = 0; q < MLP_SLOTS; q++)
+      if (MASK >> q & 1u) b[q] += h * g[q];
+    cc -= h * sg;
+  }
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) db[q] = b[q] - b0[q];
+  dc = cc - c;
+}
+
+// The plain integrator's increments (the fallback), FP64, rounded to FP32: the slot sets of
+// the reference model's domains (the jSR's two buffers, the cytosol's four, the nSR's one)
+// take compiled forms, others the general loop.
 __device__ __forceinline__ void rx_fallback(const RxConst& kc, int n, double dt, float c, const float* b, float& dc,
                                             float* db) {
   double bd[MLP_SLOTS], dbd[MLP_SLOTS], dcd;
-  for (int q = 0; q < MLP_SLOTS; q++) bd[q] = b[q];
-  rx_plain(kc, n, dt, (double)c, bd, dcd, dbd);
+  unsigned mask = 0;
+#pragma unroll
+  for (int q = 0; q < MLP_SLOTS; q++) {
+    bd[q] = b[q];
+    if (kc.tot[q] > 0.f) mask |= 1u << q;
+  }
+  switch (mask) {
+    case 0x03u: rx_plain_mask<0x03u>(kc, n, dt, (double)c, bd, dcd, dbd); break;
+    case 0x0Fu: rx_plain_mask<0x0Fu>(kc, n, dt, (double)c, bd, dcd, dbd); break;
+    case 0x01u: rx_plain_mask<0x01u>(kc, n, dt, (double)c, bd, dcd, dbd); break;
+    default: rx_plain(kc, n, dt, (double)c, bd, dcd, dbd);
+  }
+#pragma unroll
   for (int q = 0; q < MLP_SLOTS; q++) db[q] = (float)dbd[q];
   dc = (float)dcd;
 }
