@@ -338,27 +338,35 @@ __device__ __forceinline__ void mlp_forward_tc(const MlpTC& T, float* stage, con
   __syncwarp();
 }
 
-// ---- tcgen05 forward pass: 128 samples per CTA of 128 threads (one warpgroup).  One
-// thread issues tcgen05.mma (kind::tf32, FP32 accumulation in 64 columns of tensor
-// memory) for a layer; the MMAs' completion arrives on an mbarrier (tcgen05.commit); each
-// warp then reads its 32 TMEM lanes (rows: one sample per thread) with tcgen05.ld, adds
-// the bias, applies the ReLU and writes the row back to shared memory as the next layer's
-// A operand.  Operands sit in shared memory in the canonical K-major layout without
-// swizzle: element (row, k) of a matrix of R rows at byte
+// ---- tcgen05 forward pass: 128 samples per warpgroup (4 warps, one sample per thread).
+// One thread of the warpgroup issues tcgen05.mma (kind::tf32, FP32 accumulation in the
+// warpgroup's 64 columns of tensor memory) for a layer; the MMAs' completion arrives on
+// the warpgroup's mbarrier (tcgen05.commit); each warp then reads its 32 TMEM lanes (rows:
+// one sample per thread) with tcgen05.ld, adds the bias, applies the ReLU and writes the
+// row back to shared memory as the next layer's A operand.  The warpgroups of a CTA share
+// the weights and synchronise only among themselves (named barrier 1 + wg), so one
+// warpgroup's MMAs overlap the other's epilogue.  Operands sit in shared memory in the
+// canonical K-major layout without swizzle: element (row, k) of a matrix of R rows at byte
 //   (k / 4) * 16 R + (row / 8) * 128 + (row % 8) * 16 + (k % 4) * 4,
 // i.e. core matrices of 8 rows x 16 bytes, 128 bytes apart along the rows (the stride
 // byte offset) and 16 R bytes apart along K (the leading byte offset); one MMA takes
 // K = 8 (two core matrices along K).  Layers: [128 x 8] [8 x 64], [128 x 64] [64 x 64],
 // [128 x 64] [64 x 16] (outputs 5..15 zero).
-constexpr int UM_T = 128;                          // threads (and samples) per CTA
+constexpr int UM_T = 128;                          // threads (and samples) per warpgroup
 constexpr int UM_B1 = 0;                           // B of layer 1: 64 x 8 tf32, 2 KB
 constexpr int UM_B2 = UM_B1 + 64 * 8 * 4;          // B of layer 2: 64 x 64, 16 KB
 constexpr int UM_B3 = UM_B2 + 64 * 64 * 4;         // B of layer 3: 16 x 64, 4 KB
-constexpr int UM_ACT = UM_B3 + 16 * 64 * 4;        // A: 128 x 64 activations, 32 KB
-constexpr int UM_BIAS = UM_ACT + 128 * 64 * 4;     // b1[64], b2[64], b3[16] (FP32)
-constexpr int UM_BAR = UM_BIAS + 1024;             // mbarrier, then the TMEM base address
-constexpr int UM_SMEM = UM_BAR + 128;
-constexpr int UM_TMEM_COLS = 64;
+constexpr int UM_BIAS = UM_B3 + 16 * 64 * 4;       // b1[64], b2[64], b3[16] (FP32)
+constexpr int UM_BAR = UM_BIAS + 1024;             // an mbarrier per warpgroup, then the TMEM base address
+constexpr int UM_TMEM_SLOT = UM_BAR + 64;
+constexpr int UM_ACT = UM_BAR + 1024;              // A: 128 x 64 activations per warpgroup, 32 KB each
+constexpr int UM_ACT_BYTES = 128 * 64 * 4;
+constexpr int UM_TMEM_COLS = 64;                   // per warpgroup
+__host__ __device__ constexpr int um_smem(int wgs) { return UM_ACT + wgs * UM_ACT_BYTES; }
+constexpr int UM_SMEM = um_smem(1);                // k_mlp_forward_umma: one warpgroup
+constexpr int UM_NET_WGS = 2;                      // warpgroups per CTA of k_react_network_umma
+constexpr int UM_NET_SMEM = um_smem(UM_NET_WGS);
+static_assert(UM_ACT % 16 == 0 && UM_ACT_BYTES % 16 == 0, "matrix descriptors address 16-byte units");
 
 __host__ __device__ constexpr unsigned um_off(int row, int k, int rows) {
   return (unsigned)((k >> 2) * (rows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (k & 3) * 4);
@@ -380,11 +388,30 @@ __device__ __forceinline__ void um_mma(unsigned tmem_d, unsigned long long da, u
       " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
       ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate) : "memory");
 }
+// the mbarrier tracks the completion of the MMAs this thread issued before it
 __device__ __forceinline__ void um_commit(unsigned bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void um_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void um_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+// barrier of warpgroup wg's 128 threads (named barrier 1 + wg, an immediate so that ptxas
+// reserves only the barriers used; 0 is __syncthreads); wg is uniform over the warpgroup
+static_assert(UM_NET_WGS <= 2, "named barriers 1 and 2");
+__device__ __forceinline__ void um_wg_sync(int wg) {
+  if (wg == 0) asm volatile("bar.sync 1, 128;" ::: "memory");
+  else asm volatile("bar.sync 2, 128;" ::: "memory");
+}
+// the same, true when p holds on every thread of the warpgroup
+__device__ __forceinline__ bool um_wg_and(int wg, bool p) {
+  unsigned r;
+  if (wg == 0)
+    asm volatile("{\n .reg .pred a, b;\n setp.ne.b32 a, %1, 0;\n bar.red.and.pred b, 1, 128, a;\n selp.u32 %0, 1, 0, b;\n}\n"
+                 : "=r"(r) : "r"((unsigned)p) : "memory");
+  else
+    asm volatile("{\n .reg .pred a, b;\n setp.ne.b32 a, %1, 0;\n bar.red.and.pred b, 2, 128, a;\n selp.u32 %0, 1, 0, b;\n}\n"
+                 : "=r"(r) : "r"((unsigned)p) : "memory");
+  return r != 0u;
+}
 // 16 consecutive columns of this thread's TMEM lane, waited for
 __device__ __forceinline__ void um_ld16(unsigned taddr, float (&v)[16]) {
   unsigned r[16];
@@ -422,31 +449,44 @@ __device__ __forceinline__ void um_load_weights(unsigned char* sm, const float* 
   for (int i = threadIdx.x; i < 16; i += blockDim.x) bias[128 + i] = i < MLP_OUT ? W.b3[i] : 0.f;
 }
 
-// One layer: D = A[:, :K] B^T over K / 8 MMAs, issued by thread 0; true once they completed
-// (bounded wait: false after WAIT_NS, the caller gives up).  phase: the mbarrier's parity.
-template <int K, int N, int BROWS>
-__device__ __forceinline__ bool um_layer(unsigned char* sm, unsigned tmem, unsigned& phase, int b_off) {
+// Warpgroup wg's part of a CTA: its activation tile, its mbarrier, its TMEM columns.
+struct UmWg {
+  int wg;
+  unsigned act, bar, tmem;    // shared-memory addresses of the A tile and the mbarrier; TMEM column base
+};
+__device__ __forceinline__ UmWg um_wg(unsigned char* sm, int wg, unsigned tmem_base) {
   const unsigned base = smem_u32(sm);
-  if (threadIdx.x == 0) {
+  return UmWg{wg, base + UM_ACT + (unsigned)(wg * UM_ACT_BYTES), base + UM_BAR + 8u * (unsigned)wg,
+              tmem_base + (unsigned)(wg * UM_TMEM_COLS)};
+}
+
+// One layer: D = A[:, :K] B^T over K / 8 MMAs, issued by the warpgroup's first thread;
+// true once they completed (bounded wait: false after WAIT_NS, the caller gives up).
+// phase: the mbarrier's parity.
+template <int K, int N, int BROWS>
+__device__ __forceinline__ bool um_layer(unsigned char* sm, const UmWg& g, unsigned& phase, int b_off) {
+  if ((threadIdx.x & 127) == 0) {
+    const unsigned base = smem_u32(sm);
     um_fence_after();
 #pragma unroll
     for (int ks = 0; ks < K / 8; ks++) {
-      const unsigned long long da = um_desc(base + UM_ACT + (unsigned)(2 * ks) * (128 * 16), 128 * 16, 128);
+      const unsigned long long da = um_desc(g.act + (unsigned)(2 * ks) * (128 * 16), 128 * 16, 128);
       const unsigned long long db = um_desc(base + b_off + (unsigned)(2 * ks) * (BROWS * 16), BROWS * 16, 128);
-      um_mma(tmem, da, db, um_idesc(128, N), ks > 0 ? 1u : 0u);
+      um_mma(g.tmem, da, db, um_idesc(128, N), ks > 0 ? 1u : 0u);
     }
-    um_commit(base + UM_BAR);
+    um_commit(g.bar);
   }
-  const bool ok = mbar_wait_bounded(base + UM_BAR, phase, WAIT_NS);
+  const bool ok = mbar_wait_bounded(g.bar, phase, WAIT_NS);
   phase ^= 1u;
   um_fence_after();
   return ok;
 }
 
 // ReLU(D + bias) of this thread's row back into the A operand as TF32 (64 columns).
-__device__ __forceinline__ void um_hidden(unsigned char* sm, unsigned tmem, const float* bias) {
-  const int row = threadIdx.x;
-  const unsigned taddr = tmem + ((unsigned)(row & ~31) << 16);
+__device__ __forceinline__ void um_hidden(unsigned char* sm, const UmWg& g, const float* bias) {
+  const int row = threadIdx.x & 127;
+  const unsigned taddr = g.tmem + ((unsigned)(row & ~31) << 16);
+  unsigned char* act = sm + (g.act - smem_u32(sm));
 #pragma unroll
   for (int c0 = 0; c0 < 64; c0 += 16) {
     float v[16];
@@ -458,73 +498,75 @@ __device__ __forceinline__ void um_hidden(unsigned char* sm, unsigned tmem, cons
       q.y = tf32_bits(fmaxf(v[c + 1] + bias[c0 + c + 1], 0.f));
       q.z = tf32_bits(fmaxf(v[c + 2] + bias[c0 + c + 2], 0.f));
       q.w = tf32_bits(fmaxf(v[c + 3] + bias[c0 + c + 3], 0.f));
-      *reinterpret_cast<uint4*>(sm + UM_ACT + um_off(row, c0 + c, 128)) = q;
+      *reinterpret_cast<uint4*>(act + um_off(row, c0 + c, 128)) = q;
     }
   }
 }
 
-// Forward pass of the CTA's 128 samples (thread t: sample t, inputs x, outputs y); every
-// thread of the CTA calls it.  false: an MMA did not complete within WAIT_NS.
-__device__ __forceinline__ bool mlp_forward_umma(unsigned char* sm, unsigned tmem, unsigned& phase, const float* x,
+// Forward pass of the warpgroup's 128 samples (its thread t: sample t, inputs x, outputs
+// y); every thread of the warpgroup calls it.  false: an MMA did not complete within WAIT_NS.
+__device__ __forceinline__ bool mlp_forward_umma(unsigned char* sm, const UmWg& g, unsigned& phase, const float* x,
                                                  float* y) {
-  const int row = threadIdx.x;
+  const int row = threadIdx.x & 127;
   const float* bias = reinterpret_cast<const float*>(sm + UM_BIAS);
+  unsigned char* act = sm + (g.act - smem_u32(sm));
   {
     uint4 a, b;
     a.x = tf32_bits(x[0]); a.y = tf32_bits(x[1]); a.z = tf32_bits(x[2]); a.w = tf32_bits(x[3]);
     b.x = tf32_bits(x[4]); b.y = tf32_bits(x[5]); b.z = tf32_bits(x[6]); b.w = tf32_bits(x[7]);
-    *reinterpret_cast<uint4*>(sm + UM_ACT + um_off(row, 0, 128)) = a;
-    *reinterpret_cast<uint4*>(sm + UM_ACT + um_off(row, 4, 128)) = b;
+    *reinterpret_cast<uint4*>(act + um_off(row, 0, 128)) = a;
+    *reinterpret_cast<uint4*>(act + um_off(row, 4, 128)) = b;
   }
   bool ok = true;
   // before each layer: every thread's rows written (generic proxy -> async proxy) and its
   // TMEM reads of the previous layer done
   um_fence_before();
   fence_proxy_async();
-  __syncthreads();
-  ok = um_layer<MLP_IN, 64, 64>(sm, tmem, phase, UM_B1) && ok;
-  if (ok) um_hidden(sm, tmem, bias);
+  um_wg_sync(g.wg);
+  ok = um_layer<MLP_IN, 64, 64>(sm, g, phase, UM_B1) && ok;
+  if (ok) um_hidden(sm, g, bias);
   um_fence_before();
   fence_proxy_async();
-  ok = __syncthreads_and(ok);
-  if (ok) ok = um_layer<MLP_H, 64, 64>(sm, tmem, phase, UM_B2);
-  if (ok) um_hidden(sm, tmem, bias + 64);
+  ok = um_wg_and(g.wg, ok);
+  if (ok) ok = um_layer<MLP_H, 64, 64>(sm, g, phase, UM_B2);
+  if (ok) um_hidden(sm, g, bias + 64);
   um_fence_before();
   fence_proxy_async();
-  ok = __syncthreads_and(ok);
-  if (ok) ok = um_layer<MLP_H, 16, 16>(sm, tmem, phase, UM_B3);
+  ok = um_wg_and(g.wg, ok);
+  if (ok) ok = um_layer<MLP_H, 16, 16>(sm, g, phase, UM_B3);
   if (ok) {
     float v[16];
-    um_ld16(tmem + ((unsigned)(row & ~31) << 16), v);
+    um_ld16(g.tmem + ((unsigned)(row & ~31) << 16), v);
 #pragma unroll
     for (int q = 0; q < MLP_OUT; q++) y[q] = v[q] + bias[128 + q];
   }
-  return __syncthreads_and(ok);
+  return um_wg_and(g.wg, ok);
 }
 
-// TMEM for the CTA (warp 0 allocates and, at the end, frees UM_TMEM_COLS columns).
-__device__ __forceinline__ unsigned um_tmem_alloc(unsigned char* sm) {
+// TMEM for the CTA (warp 0 allocates and, at the end, frees cols columns: a power of two
+// from 32 to 512).
+__device__ __forceinline__ unsigned um_tmem_alloc(unsigned char* sm, unsigned cols) {
   if (threadIdx.x < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                 ::"r"(smem_u32(sm + UM_BAR + 8)), "r"(UM_TMEM_COLS) : "memory");
+                 ::"r"(smem_u32(sm + UM_TMEM_SLOT)), "r"(cols) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   um_fence_before();
   __syncthreads();
   um_fence_after();
-  return *reinterpret_cast<volatile unsigned*>(sm + UM_BAR + 8);
+  return *reinterpret_cast<volatile unsigned*>(sm + UM_TMEM_SLOT);
 }
-__device__ __forceinline__ void um_tmem_free(unsigned tmem) {
+__device__ __forceinline__ void um_tmem_free(unsigned tmem, unsigned cols) {
   um_fence_before();
   __syncthreads();
   um_fence_after();
   if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
 }
 
-// Forward passes for checks on the tcgen05 path: y[n][5] of x[n][8]; err[0] |= 1 when an
-// MMA did not complete in time (the CTA then waits once more for it, frees its TMEM and
-// stops).
+// Forward passes for checks on the tcgen05 path (one warpgroup per CTA): y[n][5] of
+// x[n][8]; err[0] |= 1 when an MMA did not complete in time (the CTA then waits once more
+// for it, frees its TMEM and stops).
 __global__ void __launch_bounds__(UM_T) k_mlp_forward_umma(const float* __restrict__ params,
                                                            const float* __restrict__ x, long long n,
                                                            float* __restrict__ y, int* __restrict__ err) {
@@ -536,17 +578,18 @@ __global__ void __launch_bounds__(UM_T) k_mlp_forward_umma(const float* __restri
   }
   fence_proxy_async();
   __syncthreads();
-  const unsigned tmem = um_tmem_alloc(um_sm);
+  const unsigned tmem = um_tmem_alloc(um_sm, UM_TMEM_COLS);
+  const UmWg g = um_wg(um_sm, 0, tmem);
   unsigned phase = 0;
   for (long long t0 = (long long)blockIdx.x * UM_T; t0 < n; t0 += (long long)gridDim.x * UM_T) {
     const long long i = t0 + threadIdx.x;
     float xi[MLP_IN], yi[MLP_OUT];
 #pragma unroll
     for (int j = 0; j < MLP_IN; j++) xi[j] = i < n ? x[i * MLP_IN + j] : 0.f;
-    if (!mlp_forward_umma(um_sm, tmem, phase, xi, yi)) {
+    if (!mlp_forward_umma(um_sm, g, phase, xi, yi)) {
       // a late MMA may still write TMEM: wait for it once more (bounded) before freeing
       if (threadIdx.x == 0) {
-        mbar_wait_bounded(smem_u32(um_sm + UM_BAR), phase ^ 1u, WAIT_NS);
+        mbar_wait_bounded(g.bar, phase ^ 1u, WAIT_NS);
         atomicOr(err, 1);
       }
       break;
@@ -555,7 +598,7 @@ __global__ void __launch_bounds__(UM_T) k_mlp_forward_umma(const float* __restri
 #pragma unroll
       for (int j = 0; j < MLP_OUT; j++) y[i * MLP_OUT + j] = yi[j];
   }
-  um_tmem_free(tmem);
+  um_tmem_free(tmem, UM_TMEM_COLS);
 }
 
 // Increment of the network output t, with the acceptance test (see the header comment).
@@ -974,27 +1017,29 @@ __global__ void __launch_bounds__(MLP_DEPLOY_T, 2) k_react_network(const RealDes
   }
 }
 
-// k_react_network on the 5th-generation tensor cores: a CTA of 128 threads takes groups of
-// four queued tiles, one per warp (each warp fetches its tile's voxels and caches its
-// realisation's constants as in k_react_network), and runs the network for the group's
-// 128 voxels as one tcgen05 MMA chain per layer (mlp_forward_umma); rejected outputs take
-// the plain integrator.  Persistent CTAs: CTA b takes a contiguous range of the groups.
-// An MMA that does not complete within WAIT_NS sets ERR_TIMEOUT in err and stops the CTA
-// (after a second bounded wait for it and with its TMEM freed).
+// k_react_network on the 5th-generation tensor cores: a CTA of UM_NET_WGS warpgroups
+// (4 warps each) shares one copy of the weights; a warpgroup takes groups of four queued
+// tiles, one per warp (each warp fetches its tile's voxels and caches its realisation's
+// constants as in k_react_network), and runs the network for the group's 128 voxels as one
+// tcgen05 MMA chain per layer (mlp_forward_umma, synchronised within the warpgroup only);
+// rejected outputs take the plain integrator.  Persistent CTAs: CTA b takes a contiguous
+// range of the groups, dealt to its warpgroups in turn.  An MMA that does not complete
+// within WAIT_NS sets ERR_TIMEOUT in err and stops the warpgroup (after a second bounded
+// wait for it); the CTA then frees its TMEM.
 template <unsigned FQ>
-__global__ void __launch_bounds__(UM_T) k_react_network_umma(const RealDesc* __restrict__ descs,
-                                                             const RealCtl* __restrict__ ctl,
-                                                             const float* __restrict__ params, float tol,
-                                                             const unsigned short* __restrict__ list,
-                                                             const unsigned* __restrict__ counts,
-                                                             const unsigned* __restrict__ tiles,
-                                                             unsigned* __restrict__ queue, int chunks,
-                                                             unsigned long long* __restrict__ counters,
-                                                             int* __restrict__ err) {
+__global__ void __launch_bounds__(UM_T * UM_NET_WGS, 2) k_react_network_umma(const RealDesc* __restrict__ descs,
+                                                                          const RealCtl* __restrict__ ctl,
+                                                                          const float* __restrict__ params, float tol,
+                                                                          const unsigned short* __restrict__ list,
+                                                                          const unsigned* __restrict__ counts,
+                                                                          const unsigned* __restrict__ tiles,
+                                                                          unsigned* __restrict__ queue, int chunks,
+                                                                          unsigned long long* __restrict__ counters,
+                                                                          int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char um_sm[];
-  __shared__ RxWarpCache s_wc[UM_T / 32];
+  __shared__ RxWarpCache s_wc[UM_NET_WGS * UM_T / 32];
   __shared__ unsigned s_net, s_fall, s_total;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wi = warp & 3, wg = warp >> 2;
   if (threadIdx.x == 0) { s_total = queue[0]; s_net = 0; s_fall = 0; }
   __syncthreads();
   const unsigned total = s_total, groups = (total + 3u) / 4u;
@@ -1003,23 +1048,26 @@ __global__ void __launch_bounds__(UM_T) k_react_network_umma(const RealDesc* __r
   if (g_lo < g_hi) {                                     // uniform over the block
     um_load_weights(um_sm, params);
     if (threadIdx.x == 0) {
-      mbar_init(smem_u32(um_sm + UM_BAR), 1);
+      for (int w = 0; w < UM_NET_WGS; w++) mbar_init(smem_u32(um_sm + UM_BAR + 8 * w), 1);
       fence_mbar_init();
     }
     fence_proxy_async();
     __syncthreads();
-    const unsigned tmem = um_tmem_alloc(um_sm);
+    const unsigned tmem = um_tmem_alloc(um_sm, UM_NET_WGS * UM_TMEM_COLS);
+    const UmWg G = um_wg(um_sm, wg, tmem);
     unsigned phase = 0, n_net = 0, n_fall = 0;
     RxWarpCache& W = s_wc[warp];
     int rc = -1;                                         // realisation whose constants this warp caches
     RxTile nx{};
-    if (4 * g_lo + warp < total) nx = rx_fetch_tile(descs, list, counts, tiles[4 * g_lo + warp], chunks, 0, lane);
-    for (unsigned g = g_lo; g < g_hi; g++) {
-      const bool tile = 4 * g + warp < total;            // warp-uniform
+    const unsigned g0 = g_lo + (unsigned)wg;
+    if (g0 < g_hi && 4 * g0 + wi < total) nx = rx_fetch_tile(descs, list, counts, tiles[4 * g0 + wi], chunks, 0, lane);
+    for (unsigned g = g0; g < g_hi; g += UM_NET_WGS) {  // uniform over the warpgroup
+      const bool tile = 4 * g + wi < total;              // warp-uniform
       RxTile cu = nx;
       if (!tile) cu.have = false;
-      if (g + 1 < g_hi && 4 * (g + 1) + warp < total)
-        nx = rx_fetch_tile(descs, list, counts, tiles[4 * (g + 1) + warp], chunks, 0, lane);
+      const unsigned gn = g + UM_NET_WGS;
+      if (gn < g_hi && 4 * gn + wi < total)
+        nx = rx_fetch_tile(descs, list, counts, tiles[4 * gn + wi], chunks, 0, lane);
       float dev[MLP_RX_NS], c = 0.f, b[MLP_SLOTS], x[MLP_IN], t[MLP_OUT];
 #pragma unroll
       for (int i = 0; i < MLP_IN; i++) x[i] = 0.f;
@@ -1037,9 +1085,9 @@ __global__ void __launch_bounds__(UM_T) k_react_network_umma(const RealDesc* __r
         rx_load_old<FQ>(K, W.uo, cu.v, fqs, dev, c, b);
         rx_features(K.k, cu.d, dtr, c, b, x);
       }
-      if (!mlp_forward_umma(um_sm, tmem, phase, x, t)) {
-        if (threadIdx.x == 0) {
-          mbar_wait_bounded(smem_u32(um_sm + UM_BAR), phase ^ 1u, WAIT_NS);
+      if (!mlp_forward_umma(um_sm, G, phase, x, t)) {
+        if ((threadIdx.x & 127) == 0) {
+          mbar_wait_bounded(G.bar, phase ^ 1u, WAIT_NS);
           atomicOr(err, ERR_TIMEOUT);
         }
         break;
@@ -1054,7 +1102,7 @@ __global__ void __launch_bounds__(UM_T) k_react_network_umma(const RealDesc* __r
         rx_correct<FQ>(K, D, W.un, cu.v, fqs, dev, c, db, dc);
       }
     }
-    um_tmem_free(tmem);
+    um_tmem_free(tmem, UM_NET_WGS * UM_TMEM_COLS);
     if (n_net) atomicAdd(&s_net, n_net);
     if (n_fall) atomicAdd(&s_fall, n_fall);
     __syncthreads();

@@ -1105,7 +1105,7 @@ static void launch_surrogate(csp_handle* h, int r0, int r1) {
       h->d_desc + r0, h->d_ctl + r0, h->d_sur_list, h->d_sur_counts, tiles_plain, h->d_sur_queue + 2, chunks,
       h->d_mlp_cnt);
   if (h->sur_tc == 2)
-    network_kernel_umma(h->surrogate_fq)<<<h->sur_umma_ctas, UM_T, UM_SMEM, h->stream>>>(
+    network_kernel_umma(h->surrogate_fq)<<<h->sur_umma_ctas, UM_T * UM_NET_WGS, UM_NET_SMEM, h->stream>>>(
         h->d_desc + r0, h->d_ctl + r0, h->d_mlp, h->surrogate_tol, h->d_sur_list, h->d_sur_counts, h->d_sur_tiles,
         h->d_sur_queue, chunks, h->d_mlp_cnt, h->d_err);
   else
@@ -2111,11 +2111,11 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
       CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, plain_kernel(h->surrogate_fq), MLP_DEPLOY_T, 0));
       h->sur_plain_ctas = std::max(per_sm, 1) * std::max(sms, 1);
       CUDA_TRY(h, cudaFuncSetAttribute(network_kernel_umma(h->surrogate_fq), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       UM_SMEM));
+                                       UM_NET_SMEM));
       CUDA_TRY(h, cudaFuncSetAttribute(network_kernel_umma(h->surrogate_fq),
                                        cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
       // resident CTAs per SM from the kernel's shared memory and registers (the occupancy
-      // query reports one for this kernel, which holds a third of the SM's shared memory):
+      // query reports one for this kernel, which holds nearly half of the SM's shared memory):
       // static + dynamic + the driver's reserve per CTA, and up to 1 KB of alignment
       cudaFuncAttributes fa;
       int smem_sm = 0, reserved = 0, regs_sm = 0;
@@ -2123,9 +2123,9 @@ extern "C" int csp_set_surrogate(csp_handle* h, const float* params, double tol)
       CUDA_TRY(h, cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
       CUDA_TRY(h, cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
       CUDA_TRY(h, cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
-      const int per_block = (int)fa.sharedSizeBytes + UM_SMEM + reserved + 1024;
-      const int by_regs = regs_sm / std::max(1, fa.numRegs * UM_T);
-      per_sm = std::max(1, std::min({smem_sm / per_block, by_regs, 512 / UM_TMEM_COLS}));
+      const int per_block = (int)fa.sharedSizeBytes + UM_NET_SMEM + reserved + 1024;
+      const int by_regs = regs_sm / std::max(1, fa.numRegs * UM_T * UM_NET_WGS);
+      per_sm = std::max(1, std::min({smem_sm / per_block, by_regs, 512 / (UM_TMEM_COLS * UM_NET_WGS)}));
       h->sur_umma_ctas = per_sm * std::max(sms, 1);
     }
     CUDA_TRY(h, cudaMemcpyAsync(h->d_mlp, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->stream));
