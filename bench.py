@@ -251,13 +251,14 @@ def run_reference(args, rank, world):
     return 0
 
 
-def surrogate_run(pkg, specs, opts, W, K):
+def surrogate_run(pkg, specs, opts, W, K, tc=1):
     """The workload with dt_update_react = 10 dt, with and without the learned reaction
     surrogate.  Training pairs are harvested from a run of the workload itself (32 of its
     realisations stepped 0.2 ms, about 1e6 pairs taken every 0.02 ms, log-uniform in Ca as
     far as the states allow), the network trained on them on device; then both ensembles
     are timed like the main run, and both are compared on 8 realisations over 400 steps
-    with the run that reacts every step (max relative error per species)."""
+    with the run that reacts every step (max relative error per species).  tc: the network
+    tiles on warp mma.sync (1) or tcgen05 (2)."""
     dt = 0.95 * 36 / (6 * 220000.0)
     o10 = [dict(o, dt_update_react=10 * dt) for o in opts]
     harv = pkg.Simulation(specs[:32], o10[:32])
@@ -275,6 +276,7 @@ def surrogate_run(pkg, specs, opts, W, K):
         sim = pkg.Simulation(specs, o10)
         if use:
             sim.set_surrogate(params, 1e-4)
+            sim.set_surrogate_tensor_cores(tc)
         sim.advance(W)
         sim.advance(K)
         out[name] = nvox * K / (sim.last_ms() / 1e3)
@@ -292,6 +294,7 @@ def surrogate_run(pkg, specs, opts, W, K):
         sim = pkg.Simulation(specs[:n8], o10[:n8])
         if use:
             sim.set_surrogate(params, 1e-4)
+            sim.set_surrogate_tensor_cores(tc)
         sim.advance(steps)
         e = np.zeros(len(specs[0]["species"]))
         for r in range(n8):
@@ -301,6 +304,7 @@ def surrogate_run(pkg, specs, opts, W, K):
         errs[name] = e
         sim.close()
     return {"value": out["surrogate"], "unit": "voxel-steps/s", "dt_update_react": "10 dt",
+            "network_tiles": "tcgen05" if tc == 2 else "mma.sync",
             "without_network": {"value": out["plain_T10"], "unit": "voxel-steps/s",
                                 "max_rel_err_vs_every_step": float(errs["plain_T10"].max()),
                                 "per_species": [float(v) for v in errs["plain_T10"]]},
@@ -370,6 +374,8 @@ def main():
     ap.add_argument("--realisations", type=int, default=N_REAL)
     ap.add_argument("--extras", type=int, default=1,
                     help="also time the plain single-realisation path and the surrogate run (0: skip)")
+    ap.add_argument("--surrogate-tc", type=int, default=1, choices=[1, 2],
+                    help="network tiles of the surrogate run: warp mma.sync (1) or tcgen05 (2)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="length of the CPU baseline sample (0: skip)")
     args = ap.parse_args()
@@ -444,7 +450,7 @@ def main():
         plain_single = int(np.prod(specs[0]["voxels"].shape)) * K / (single.last_ms() / 1e3)
         single.close()
         # ---- learned reaction surrogate (dt_update_react = 10 dt): train, deploy, time ----
-        sur = surrogate_run(pkg, specs, opts, W, K)
+        sur = surrogate_run(pkg, specs, opts, W, K, args.surrogate_tc)
         # ---- configs 2 and 4 on the same kernels ----
         s2, o2 = synth.config2()
         s4, o4 = synth.config4()
