@@ -315,6 +315,35 @@ def test_surrogate_tcgen05_tiles_match_mma_sync(pkg, synth):
 
 
 @pytest.mark.gpu
+def test_surrogate_tcgen05_both_warpgroups(pkg, synth):
+    """The tcgen05 network kernel's second warpgroup (its own named barrier, mbarrier,
+    activation tile and TMEM columns) only gets work when a CTA holds two or more groups of
+    128 voxels: an ensemble of config-3 grids late enough in its sparks that a reaction
+    step lists more network voxels than 296 CTAs (2 per SM x 148 SMs) x 128 take in one
+    round.  The fields must equal those of the warp mma.sync tiles as in the single-grid
+    case."""
+    p, _ = trained(pkg, synth)
+    specs, opts = synth.config3(n=8)
+    opts = [dict(o, dt_update_react=10 * DT) for o in opts]
+    steps, every = 425, 10
+    out = []
+    for kind in (1, 2):
+        sim = pkg.Simulation(specs, opts)
+        sim.set_surrogate(p, 1e-4)
+        sim.set_surrogate_tensor_cores(kind)
+        sim.advance(steps)
+        out.append(([sim.state(r) for r in range(len(specs))], sim.surrogate_counts()))
+        sim.close()
+    (u1, c1), (u2, c2) = out
+    per_step = c1[1] / (steps // every)
+    print("network voxels per reaction step", per_step, c1, c2)
+    assert per_step > 296 * 128, per_step
+    assert c1[0] == c2[0] and abs(c1[1] - c2[1]) <= 0.01 * c1[1]
+    err = max(float(np.max(np.abs(a - b)) / np.max(np.abs(a))) for a, b in zip(u1, u2))
+    assert err <= 1e-5, err
+
+
+@pytest.mark.gpu
 def test_forward_passes_match_oracle(pkg):
     """The FP32 pass (training) and the TF32 tensor-core passes (warp mma.sync, used in
     deployment; tcgen05 with tensor-memory accumulators) against FP64."""
